@@ -1,0 +1,406 @@
+"""Benchmark of the per-step hot path: one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload impact|fluid|plummer]
+                    [--accum plain|compensated] [--no-cpu-baseline]
+
+Workload (default): the elastic-plastic two-sphere impact at N = 65,536 (R = 1 with 58,254 particles and
+R = 0.5 with 7,282, relative velocity 0.5 along x, y-offset 0.3, rho0 = 1, Murnaghan K = 10, shear 5,
+von Mises Y = 0.5, AV alpha = 1 beta = 2, h = 2.5 x mean spacing, G = 1, eps = 0.01, dt = 1e-4), seeded
+synthetic initial conditions. A step is computeDerivatives + integrate (the captured step graph).
+
+Timing: W untimed steps, then K steps, each bracketed by CUDA events on the launching stream, with a
+256 MiB write between steps (outside the events) to flush the 126 MB L2; barrier + synchronize on both
+sides; the max over ranks. N > 1 runs independent replicas (the path is not sharded across GPUs) and
+reports the whole-job rate.
+
+--impl reference times GraSPH2's own CPU hot path (its job headers compiled for the host with OpenMP,
+oracle/_ref) on this machine's cores, on bounded row samples of the same workload, extrapolated.
+"""
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/s & pair-interactions/s, chosen vs plain form at ≤1e-4 energy drift"
+
+# Algorithmic flop model (frozen; derivation in DESIGN.md): per pair of the N^2 sweep and per
+# neighbour pair (0 < r <= h) of the SPH passes.
+FLOP_GRAV_PAIR = 20        # softened gravity, the GPU Gems 3 ch. 31 convention
+FLOP_DENS_PAIR = 8         # distance test of the density sum
+FLOP_DENS_NB = 10          # W(r) and the accumulation per neighbour
+FLOP_FUSED_NB = 160        # strain/rotation rates, div v, stress acceleration, AV per neighbour (solids)
+FLOP_ACC_NB = 60           # pressure acceleration + AV per neighbour (fluid, acceleration pass only)
+
+FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["impact", "fluid", "plummer"], default="impact")
+    ap.add_argument("--accum", choices=["plain", "compensated"], default="plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU work for the CPU baseline")
+    return ap.parse_args()
+
+
+# ---- workloads ------------------------------------------------------------------------------------
+def workload(name):
+    from grasph2_b200 import ics
+    from grasph2_b200.params import config0_params, config1_params, config2_params
+    if name == "impact":
+        st = ics.two_sphere_impact(seed=20261203)
+        desc = ("elastic-plastic two-sphere impact, N=65536 (R=1: 58254, R=0.5: 7282), rho0=1, Murnaghan K=10, "
+                "shear=5, von Mises Y=0.5, AV alpha=1 beta=2, h=2.5x mean spacing, G=1 eps=0.01, dt=1e-4")
+        return config1_params(), st, desc, "impact"
+    if name == "fluid":
+        st = ics.uniform_sphere(4096, radius=1.0, rho0=0.239, omega=(0, 0, 0.1), seed=20261203)
+        return config0_params(), st, "SPH + self-gravity fluid sphere, N=4096, h=0.15, eps=0.02", "fluid"
+    st = ics.plummer_sphere(1 << 20, seed=20261203)
+    return config2_params(), st, "Plummer sphere N-body, N=1048576, a=1, eps=0.01, dt=1e-3", "nbody"
+
+
+def flops_per_step(params, st, counts):
+    from grasph2_b200._abi import FLAG_BITS as F
+    n = st["mass"].shape[0]
+    n2 = float(n) * n
+    nb = counts
+    out = {}
+    if params.flags & F["SPH"]:
+        if not params.flags & F["INTEGRATE_DENSITY"]:
+            out["density"] = FLOP_DENS_PAIR * n2 + FLOP_DENS_NB * nb
+        solids = params.flags & F["SOLIDS"]
+        out["pairs"] = FLOP_GRAV_PAIR * n2 + (FLOP_FUSED_NB if solids else FLOP_ACC_NB) * nb
+    else:
+        out["gravity"] = FLOP_GRAV_PAIR * n2
+    return out
+
+
+def neighbour_pairs(pos, h, device):
+    """Number of ordered pairs with 0 < r <= h (for the flop model), counted on the GPU with torch."""
+    import torch
+    x = torch.as_tensor(np.asarray(pos, dtype=np.float32), device=device)
+    n = x.shape[0]
+    total = 0
+    chunk = 4096
+    for i0 in range(0, n, chunk):
+        d2 = torch.cdist(x[i0:i0 + chunk], x).pow_(2)
+        total += int(((d2 > 0) & (d2 <= h * h)).sum().item())
+    return total
+
+
+# ---- clocks ---------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        sel = self._selector(device_index)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", sel, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    @staticmethod
+    def _selector(device_index):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        if vis:
+            parts = [p.strip() for p in vis.split(",") if p.strip()]
+            if device_index < len(parts):
+                return parts[device_index]
+        return str(device_index)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                rows.append((float(f[0]), float(f[1]), float(f[2]), f[3], f[4], f[5], f[6], f[7]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in loaded:
+            for nm, val in zip(names, r[4:8]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(loaded), "power_w_max": max(r[2] for r in rows), "reasons": sorted(reasons)}
+
+
+# ---- CPU reference timing ------------------------------------------------------------------------
+def cpu_reference_sample(variant, st, budget_s, rows_hint=None):
+    """Time the reference's own hot path (oracle/_ref, FP32 as shipped, OpenMP on all host cores) on
+    target-row samples of the workload; return (steps/s extrapolated, description, cores, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from grasph2_b200.state import as_dtype
+    n = st["mass"].shape[0]
+    cores = os.cpu_count() or 1
+    if pyoracle.ref_available(variant):
+        R = pyoracle.RefBuild(variant, double=False)
+        s32 = as_dtype(st, np.float32)
+        kind = "reference"
+
+        def sample(m):
+            t0 = time.perf_counter()
+            R.compute_derivatives_rows(s32, 0, m)
+            return time.perf_counter() - t0
+
+        t0 = time.perf_counter()
+        R.integrate(as_dtype(st, np.float32), True)
+        t_int = time.perf_counter() - t0
+    else:
+        O = pyoracle.Oracle()
+        kind = "port"
+        from grasph2_b200.params import config1_params
+        p = config1_params()
+        s64 = as_dtype(st, np.float64)
+
+        def sample(m):
+            t0 = time.perf_counter()
+            O.compute_derivatives(p, s64, 0, m)
+            return time.perf_counter() - t0
+
+        t_int = 0.0
+    m = rows_hint or 64
+    t = sample(m)
+    while t < 0.2 * budget_s and m < n:
+        m = min(n, int(m * max(2.0, 0.5 * budget_s / max(t, 1e-3))))
+        t = sample(m)
+    per_step = t * n / m + t_int
+    desc = ("computeDerivatives on target rows [0, %d) of N=%d (all passes), %.2f s, plus integrate of all N; "
+            "extrapolated x N/rows" % (m, n, t))
+    return 1.0 / per_step, desc, cores, kind, m
+
+
+def run_reference_arm(args, rank, world):
+    if world > 1 and rank != 0:
+        return
+    params, st, desc, variant = workload(args.workload)
+    n = st["mass"].shape[0]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    if not pyoracle.ref_available(variant) and not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
+        print(json.dumps({"impl": "reference", "unavailable": "neither oracle/_ref nor oracle/liboracle.so is built"}))
+        return
+    total_budget = 150.0
+    per = max(0.05, total_budget / float(args.steps + args.warmup + 2))
+    rate0, _, cores, kind, m = cpu_reference_sample(variant, st, per)
+    times = []
+    from grasph2_b200.state import as_dtype
+    if kind == "reference":
+        R = pyoracle.RefBuild(variant, double=False)
+        s32 = as_dtype(st, np.float32)
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            R.compute_derivatives_rows(s32, 0, m)
+            dt = time.perf_counter() - t0
+            if k >= args.warmup:
+                times.append(dt)
+    else:
+        times = [1.0 / rate0] * args.steps
+    t_step = (sum(times) / len(times)) * n / m
+    value = 1.0 / t_step
+    pairs = flops_pairs(params, n)
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": desc, "n": n, "sample": "rows [0,%d) per step, extrapolated x N/rows" % m},
+        "pair_interactions_per_s": pairs * value,
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
+                         "sample": "GraSPH2 host jobs (FP32, OpenMP) on rows [0,%d) of N=%d per step" % (m, n)},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def flops_pairs(params, n):
+    from grasph2_b200._abi import FLAG_BITS as F
+    passes = 1
+    if params.flags & F["SPH"]:
+        passes = 2 if not params.flags & F["INTEGRATE_DENSITY"] else 1
+        if params.flags & F["BALSARA_SWITCH"]:
+            passes += 1
+    return float(n) * n * passes
+
+
+# ---- our arm ----------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from grasph2_b200.params import make_options
+    from grasph2_b200.sim import DeviceParticleBuffer, measure_fp32_peak
+
+    params, st, desc, variant = workload(args.workload)
+    n = st["mass"].shape[0]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    peak_tflops = measure_fp32_peak(0.5)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    pb = DeviceParticleBuffer(params, n, make_options(accum=args.accum))
+    pb.upload(st, stream=stream)
+    pb.profile_enable(True)
+    for _ in range(args.warmup):
+        flush.zero_()
+        pb.step(1, stream)
+        pb.profile_collect()
+    pb.profile_reset()
+
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = pb.launch_count()
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(args.steps):
+        flush.zero_()
+        ev0[k].record(stream)
+        pb.step(1, stream)
+        ev1[k].record(stream)
+        pb.profile_collect()
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    gpu_launches = pb.launch_count() - launches0
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    prof = pb.profile_read()
+
+    # e2e: the public API with host buffers (pinned): upload inputs, one step, download the result
+    up_names = ["pos", "mass", "vel", "density", "dstress"]
+    down_names = ["pos", "vel", "acc", "density", "dstress"]
+    from grasph2_b200.state import new_state
+    pinned_in = {k: torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float32)).pin_memory().numpy()
+                 for k in up_names}
+    host_out = new_state(n, np.float32)
+    pinned_out = {k: torch.empty(host_out[k].shape, dtype=torch.float32).pin_memory().numpy() for k in down_names}
+    h2d = sum(a.nbytes for a in pinned_in.values())
+    d2h = sum(a.nbytes for a in pinned_out.values())
+    e2e_steps = max(5, min(args.steps, 50))
+    pb.profile_enable(False)
+    pb2 = DeviceParticleBuffer(params, n, make_options(accum=args.accum))
+    e2e_ms = 0.0
+    for k in range(e2e_steps + 3):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        pb2.upload(pinned_in, stream=stream)
+        pb2.step(1, stream)
+        pb2.download(down_names, stream=stream, out=pinned_out)
+        b.record(stream)
+        b.synchronize()
+        if k >= 3:
+            e2e_ms += a.elapsed_time(b)
+    pb2.close()
+
+    if rank != 0:
+        pb.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    steps_total = args.steps * world
+    value = steps_total / (total_ms * 1e-3)
+    ms_per_step = total_ms / args.steps
+    nb = neighbour_pairs(st["pos"], params.H, dev) if (params.flags & 2) else 0
+    fl = flops_per_step(params, st, nb)
+    dominant = max(fl, key=lambda k: fl[k])
+    ms_dom, cnt_dom = prof[dominant]
+    achieved = fl[dominant] / (ms_dom / cnt_dom * 1e-3) / 1e12 if cnt_dom else None
+    pairs_per_step = flops_pairs(params, n)
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, sdesc, cores, kind, _ = cpu_reference_sample(variant, st, args.cpu_budget)
+        cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sdesc}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded initial conditions)",
+        "config": {"workload": desc, "n": n, "form": args.accum, "l2": "flushed between timed steps (256 MiB write)",
+                   "step": "computeDerivatives + integrate, one captured CUDA graph",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "pair_interactions_per_s": pairs_per_step * value,
+        "kernel_ms_per_step": {k: (v[0] / v[1] if v[1] else None) for k, v in prof.items()},
+        "roofline": {"bound": "fp32", "kernel": dominant, "achieved": achieved, "peak": peak_tflops,
+                     "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None,
+                     "traffic": None, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
+                     "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "e2e": {"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": gpu_launches,
+    }
+    print(json.dumps(line))
+    pb.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

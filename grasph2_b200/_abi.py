@@ -1,0 +1,168 @@
+"""ctypes mirror of include/grasph2_b200.h (structs, flags, status codes) and the library loader.
+
+The shared library is built in-tree by grasph2_b200/build.py into grasph2_b200/lib/libgrasph2_b200.so.
+Loading fails loudly when it is missing: there is no CPU fallback in this package.
+"""
+
+import ctypes
+import os
+
+c_double3 = ctypes.c_double * 3
+
+# ---- status codes -------------------------------------------------------------------------------
+GSPH_OK = 0
+GSPH_E_INVALID = -1
+GSPH_E_CUDA = -2
+GSPH_E_NOMEM = -3
+GSPH_E_STATE = -4
+GSPH_E_NUMERIC = -5
+GSPH_E_TIMEOUT = -6
+GSPH_E_UNSUPPORTED = -7
+STATUS_NAMES = {0: "GSPH_OK", -1: "GSPH_E_INVALID", -2: "GSPH_E_CUDA", -3: "GSPH_E_NOMEM", -4: "GSPH_E_STATE",
+                -5: "GSPH_E_NUMERIC", -6: "GSPH_E_TIMEOUT", -7: "GSPH_E_UNSUPPORTED"}
+
+# ---- physics switches (settings/settings.h #defines) --------------------------------------------
+FLAG_BITS = {
+    "SELF_GRAVITY": 1 << 0, "SPH": 1 << 1, "INTEGRATE_DENSITY": 1 << 2, "DEAL_WITH_NO_PARTNERS": 1 << 3,
+    "SOLIDS": 1 << 4, "VARIABLE_TIMESTEP": 1 << 5, "ACCELERATION_CRITERION": 1 << 6,
+    "VELOCITY_CRITERION": 1 << 7, "PLASTICITY_MIESE": 1 << 8, "PLASTICITY_MC": 1 << 9,
+    "CLOHESSY_WILTSHIRE": 1 << 10, "CONSTANT_ACCELERATION": 1 << 11, "SIMPLE_BOX_BOUNDARY": 1 << 12,
+    "ARTIFICIAL_VISCOSITY": 1 << 13, "BALSARA_SWITCH": 1 << 14, "ARTIFICIAL_STRESS": 1 << 15, "XSPH": 1 << 16,
+}
+ALL_FLAGS = (1 << 17) - 1
+
+# ---- particle attributes (particle_bases order) -------------------------------------------------
+ATTRIBUTES = [  # name, bit, components
+    ("pos", 1 << 0, 3), ("mass", 1 << 1, 1), ("vel", 1 << 2, 3), ("acc", 1 << 3, 3), ("balsara", 1 << 4, 1),
+    ("xvel", 1 << 5, 3), ("density", 1 << 6, 1), ("density_dt", 1 << 7, 1), ("dstress", 1 << 8, 9),
+    ("dstress_dt", 1 << 9, 9), ("maxvsig", 1 << 10, 1),
+]
+ATTR_BITS = {name: bit for name, bit, _ in ATTRIBUTES}
+ATTR_COMPONENTS = {name: k for name, _, k in ATTRIBUTES}
+ALL_ATTRIBS = (1 << 11) - 1
+
+ACCUM_PLAIN = 0
+ACCUM_COMPENSATED = 1
+
+
+class GsphParams(ctypes.Structure):
+    _fields_ = [
+        ("flags", ctypes.c_uint32), ("dimension", ctypes.c_int32),
+        ("H", ctypes.c_double), ("grav_eps", ctypes.c_double), ("grav_G", ctypes.c_double),
+        ("rho0", ctypes.c_double), ("bulk", ctypes.c_double), ("dbulk_dp", ctypes.c_double),
+        ("soundspeed", ctypes.c_double), ("shear", ctypes.c_double), ("Y", ctypes.c_double),
+        ("tanfr", ctypes.c_double), ("cohesion", ctypes.c_double), ("av_alpha", ctypes.c_double),
+        ("av_beta", ctypes.c_double), ("mateps", ctypes.c_double), ("matexp", ctypes.c_double),
+        ("normalsep", ctypes.c_double), ("xsph_factor", ctypes.c_double), ("fixed_dt", ctypes.c_double),
+        ("initial_dt", ctypes.c_double), ("min_dt", ctypes.c_double), ("max_dt", ctypes.c_double),
+        ("accel_accuracy", ctypes.c_double), ("velocity_accuracy", ctypes.c_double), ("cw_n", ctypes.c_double),
+        ("const_acc", c_double3), ("box_min", c_double3), ("box_max", c_double3),
+        ("box_reflectiveness", ctypes.c_double),
+    ]
+
+
+class GsphOptions(ctypes.Structure):
+    _fields_ = [
+        ("accum", ctypes.c_int32), ("j_split", ctypes.c_int32), ("j_tile", ctypes.c_int32),
+        ("i_per_thread", ctypes.c_int32), ("threads", ctypes.c_int32), ("check_finite", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 10),
+    ]
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+class GsphHostParticles(ctypes.Structure):
+    _fields_ = [(name, _fp) for name, _, _ in ATTRIBUTES]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class OracleParticles(ctypes.Structure):
+    """FP64 twin of GsphHostParticles, used by the oracle bindings."""
+    _fields_ = [(name, _dp) for name, _, _ in ATTRIBUTES]
+
+
+class GsphDiag(ctypes.Structure):
+    _fields_ = [
+        ("e_kin", ctypes.c_double), ("e_grav", ctypes.c_double), ("e_int", ctypes.c_double),
+        ("e_shear", ctypes.c_double), ("momentum", c_double3), ("ang_mom", c_double3), ("mass", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return dict(e_kin=self.e_kin, e_grav=self.e_grav, e_int=self.e_int, e_shear=self.e_shear,
+                    momentum=tuple(self.momentum), ang_mom=tuple(self.ang_mom), mass=self.mass,
+                    e_total=self.e_kin + self.e_grav + self.e_int + self.e_shear)
+
+
+KSLOTS = 5
+KSLOT_NAMES = ("density", "vgrad", "pairs", "gravity", "step")
+
+
+class GsphProfile(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double * KSLOTS), ("launches", ctypes.c_int64 * KSLOTS)]
+
+
+class GsphDeviceView(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("posm", ctypes.c_void_p), ("velrho", ctypes.c_void_p),
+                ("acc", ctypes.c_void_p), ("pos64", ctypes.c_void_p)]
+
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PACKAGE_DIR, "lib", "libgrasph2_b200.so")
+
+_lib = None
+
+_SIGNATURES = {
+    "gsph_params_reference_defaults": (ctypes.c_int, [ctypes.POINTER(GsphParams)]),
+    "gsph_params_validate": (ctypes.c_int, [ctypes.POINTER(GsphParams), ctypes.c_char_p, ctypes.c_size_t]),
+    "gsph_options_defaults": (ctypes.c_int, [ctypes.POINTER(GsphOptions)]),
+    "gsph_create": (ctypes.c_int, [ctypes.POINTER(GsphParams), ctypes.POINTER(GsphOptions), ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_void_p)]),
+    "gsph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
+                                   ctypes.c_void_p]),
+    "gsph_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
+                                     ctypes.c_void_p]),
+    "gsph_upload_pos64": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_void_p]),
+    "gsph_download_pos64": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_void_p]),
+    "gsph_compute_derivatives": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_integrate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "gsph_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "gsph_current_timestep": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_void_p]),
+    "gsph_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
+                                        ctypes.c_void_p]),
+    "gsph_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gsph_device_view_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GsphDeviceView)]),
+    "gsph_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_profile_enable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "gsph_profile_collect": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GsphProfile)]),
+    "gsph_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_measure_fp32_peak": (ctypes.c_int, [ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+}
+
+
+def load_library(path=None):
+    """Load libgrasph2_b200.so (once) and declare its signatures. Raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError("grasph2_b200: CUDA library not built (%s missing); run "
+                           "`python -c 'import __graft_entry__ as g; g.build()'` or grasph2_b200/build.py" % p)
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in _SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def exported_symbols():
+    return sorted(_SIGNATURES)

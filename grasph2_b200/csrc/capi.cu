@@ -1,0 +1,675 @@
+// capi.cu -- the C-ABI of include/grasph2_b200.h: context (the DeviceParticleBuffer analogue),
+// upload/download in the reference's attribute layout, computeDerivatives / integrate dispatch,
+// the CUDA-graph step loop and the FP64 diagnostics.
+#include <cmath>
+#include <cstdio>
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "integrate.cuh"
+#include "pairs.cuh"
+
+using namespace gsph;
+
+struct gsph_ctx {
+    gsph_params params;
+    gsph_options opt;
+    DevParams dp;
+    Launch L;
+    DevArrays a;
+    int device = 0;
+    int sm_count = 148;
+    std::vector<void*> allocations;
+    float* staging = nullptr;     // 9 * n floats
+    double* staging64 = nullptr;  // 3 * n doubles
+    double* diag_out = nullptr;   // device, 12 doubles
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int64_t graph_kernels = 0;
+    int64_t launches = 0;
+    // per-kernel timing (gsph_profile_*)
+    bool profiling = false;
+    KTimer timers[GSPH_KSLOTS];
+    bool pending[GSPH_KSLOTS] = {};
+    uint32_t graph_slots = 0;      // slots recorded inside the captured step graph
+    double prof_ms[GSPH_KSLOTS] = {};
+    int64_t prof_launches[GSPH_KSLOTS] = {};
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(gsph_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+int cuda_fail(gsph_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, GSPH_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define GSPH_CK(ctx, call, what)                          \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+double spline_prefactor(int dim, double h) {  // src/sph/kernel.h:44-60
+    if (dim == 1) return 4.0 / (3.0 * h);
+    if (dim == 2) return 40.0 / (7.0 * M_PI * h * h);
+    return 8.0 / (M_PI * h * h * h);
+}
+double dspline_prefactor(int dim, double h) {  // src/sph/kernel.h:71-87
+    if (dim == 1) return 24.0 / (3.0 * h * h);
+    if (dim == 2) return 240.0 / (7.0 * M_PI * h * h * h);
+    return 48.0 / (M_PI * h * h * h * h);
+}
+
+DevParams make_dev_params(const gsph_params& p) {
+    DevParams d{};
+    d.flags = p.flags;
+    d.dim = p.dimension;
+    d.H = static_cast<float>(p.H);
+    d.H2 = static_cast<float>(p.H * p.H);
+    d.inv_h = static_cast<float>(1.0 / p.H);
+    d.eps2 = static_cast<float>(p.grav_eps * p.grav_eps);
+    d.G = static_cast<float>(p.grav_G);
+    d.w_pref = static_cast<float>(spline_prefactor(p.dimension, p.H));
+    d.dw_pref = static_cast<float>(dspline_prefactor(p.dimension, p.H));
+    d.rho0 = static_cast<float>(p.rho0);
+    d.bulk = static_cast<float>(p.bulk);
+    d.dbulk = static_cast<float>(p.dbulk_dp);
+    d.c = static_cast<float>(p.soundspeed);
+    d.c2 = static_cast<float>(p.soundspeed * p.soundspeed);
+    d.shear = static_cast<float>(p.shear);
+    d.Y = static_cast<float>(p.Y);
+    d.tanfr = static_cast<float>(p.tanfr);
+    d.cohesion = static_cast<float>(p.cohesion);
+    d.alpha = static_cast<float>(p.av_alpha);
+    d.beta = static_cast<float>(p.av_beta);
+    d.mateps = static_cast<float>(p.mateps);
+    d.matexp = static_cast<float>(p.matexp);
+    {  // 1 / W(normalsep) of the artificial stress (computeDerivatives.h:265)
+        const double q = p.normalsep / p.H;
+        double w = 0.0;
+        if (q <= 1.0) w = (q < 0.5) ? (6 * q * q * q - 6 * q * q + 1) : 2 * (1 - q) * (1 - q) * (1 - q);
+        w *= spline_prefactor(p.dimension, p.H);
+        d.inv_w_normalsep = static_cast<float>(w > 0 ? 1.0 / w : 0.0);
+    }
+    d.xsph = static_cast<float>(p.xsph_factor);
+    d.fixed_dt = static_cast<float>(p.fixed_dt);
+    d.initial_dt = static_cast<float>(p.initial_dt);
+    d.min_dt = static_cast<float>(p.min_dt);
+    d.max_dt = static_cast<float>(p.max_dt);
+    d.accel_acc = static_cast<float>(p.accel_accuracy);
+    d.vel_acc = static_cast<float>(p.velocity_accuracy);
+    d.cw_n = static_cast<float>(p.cw_n);
+    for (int k = 0; k < 3; ++k) {
+        d.const_acc[k] = static_cast<float>(p.const_acc[k]);
+        d.box_min[k] = static_cast<float>(p.box_min[k]);
+        d.box_max[k] = static_cast<float>(p.box_max[k]);
+    }
+    d.box_refl = static_cast<float>(p.box_reflectiveness);
+    d.balsara_floor = static_cast<float>(0.0001 * p.soundspeed / p.H);
+    return d;
+}
+
+// smallest j-split whose last wave is at least 95 % full (or the best one up to `cap`)
+int pick_split(int64_t iblocks, int slots, int cap) {
+    int best = 1;
+    double best_eff = 0.0;
+    for (int s = 1; s <= cap; ++s) {
+        const double w = static_cast<double>(iblocks) * s / slots;
+        const double eff = w / std::ceil(w);
+        if (eff >= 0.95 && w >= 1.0) return s;
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = s;
+        }
+    }
+    return best;
+}
+
+bool is_pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+void* dalloc(gsph_ctx* c, size_t bytes, cudaError_t& e) {
+    void* p = nullptr;
+    e = cudaMalloc(&p, bytes == 0 ? 16 : bytes);
+    if (e == cudaSuccess) c->allocations.push_back(p);
+    return p;
+}
+
+void drop_graph(gsph_ctx* c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    c->graph_slots = 0;
+}
+
+void release(gsph_ctx* c) {
+    drop_graph(c);
+    for (auto& t : c->timers) {
+        if (t.start) cudaEventDestroy(t.start);
+        if (t.stop) cudaEventDestroy(t.stop);
+        t.start = t.stop = nullptr;
+    }
+    if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
+    for (void* p : c->allocations) cudaFree(p);
+    c->allocations.clear();
+}
+
+int check_status(gsph_ctx* c, cudaStream_t s) {
+    int st = 0;
+    GSPH_CK(c, cudaMemcpyAsync(&st, c->a.status, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
+    GSPH_CK(c, cudaStreamSynchronize(s), "stream synchronize");
+    if (st & GSPH_DEV_ERR_TIMEOUT) return fail(c, GSPH_E_TIMEOUT, "a device-side wait gave up (j-tile pipeline)");
+    if (st & 2) {  // a host-requested scan: report once, then clear the flag
+        const int cleared = st & ~2;
+        cudaMemcpyAsync(c->a.status, &cleared, sizeof(int), cudaMemcpyHostToDevice, s);
+        cudaStreamSynchronize(s);
+        return fail(c, GSPH_E_NUMERIC, "non-finite particle state");
+    }
+    return GSPH_OK;
+}
+
+// timer of `slot` when profiling, and mark it pending (collected by gsph_profile_collect)
+const KTimer* slot_timer(gsph_ctx* c, int slot) {
+    if (!c->profiling) return nullptr;
+    c->pending[slot] = true;
+    return &c->timers[slot];
+}
+
+int derivatives(gsph_ctx* c, cudaStream_t s) {
+    const DevParams& p = c->dp;
+    cudaError_t e;
+    if (has(p, GSPH_SPH)) {
+        if (!has(p, GSPH_INTEGRATE_DENSITY)) {
+            e = launch_density(c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_DENSITY));
+            if (e != cudaSuccess) return cuda_fail(c, e, "density pass");
+            c->launches += 2;
+        } else {
+            e = launch_prepare(c->a, p, s);
+            if (e != cudaSuccess) return cuda_fail(c, e, "j-record pass");
+            c->launches += 1;
+        }
+        const bool vgrad = has(p, GSPH_SOLIDS) || has(p, GSPH_INTEGRATE_DENSITY) || has(p, GSPH_BALSARA_SWITCH);
+        if (vgrad && has(p, GSPH_BALSARA_SWITCH)) {
+            e = launch_pairs(PASS_VGRAD, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_VGRAD));
+            if (e != cudaSuccess) return cuda_fail(c, e, "velocity-gradient pass");
+            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS));
+            if (e != cudaSuccess) return cuda_fail(c, e, "acceleration pass");
+            c->launches += 4;
+        } else {
+            e = launch_pairs(vgrad ? PASS_FUSED : PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS));
+            if (e != cudaSuccess) return cuda_fail(c, e, "pair pass");
+            c->launches += 2;
+        }
+    } else {
+        e = launch_gravity(c->a, p, c->L, s,
+                           has(p, GSPH_SELF_GRAVITY) ? slot_timer(c, GSPH_KSLOT_GRAVITY) : nullptr);
+        if (e != cudaSuccess) return cuda_fail(c, e, "gravity pass");
+        c->launches += has(p, GSPH_SELF_GRAVITY) ? 2 : 1;
+    }
+    return GSPH_OK;
+}
+
+int integrate(gsph_ctx* c, int not_first_step, cudaStream_t s) {
+    cudaError_t e = launch_leapfrog(c->a, c->dp, not_first_step, s);
+    if (e != cudaSuccess) return cuda_fail(c, e, "leapfrog");
+    c->launches += has(c->dp, GSPH_VARIABLE_TIMESTEP) ? 3 : 1;
+    return GSPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsph_params_reference_defaults(gsph_params* p) {
+    if (!p) return GSPH_E_INVALID;
+    std::memset(p, 0, sizeof(*p));
+    const double pradius = 0.1 * std::pow(double(1 << 14), -1.0 / 3.0);  // settings.h:97-98
+    p->flags = GSPH_SELF_GRAVITY | GSPH_SPH | GSPH_INTEGRATE_DENSITY | GSPH_SOLIDS | GSPH_VARIABLE_TIMESTEP |
+               GSPH_ACCELERATION_CRITERION | GSPH_VELOCITY_CRITERION | GSPH_PLASTICITY_MC |
+               GSPH_ARTIFICIAL_VISCOSITY | GSPH_BALSARA_SWITCH;
+    p->dimension = 3;
+    p->H = pradius * 2.5;
+    p->grav_eps = p->H;
+    p->grav_G = 1.0;
+    p->rho0 = 1.0 / (1 << 14) / (4.0 / 3.0 * pradius * pradius * pradius * M_PI);
+    p->bulk = 1024;
+    p->dbulk_dp = 1;
+    p->soundspeed = std::sqrt(p->bulk / p->rho0);
+    p->shear = 128;
+    p->Y = 0.5;
+    p->tanfr = std::tan(45.0 * M_PI / 180.0);
+    p->cohesion = 0.0;
+    p->av_alpha = 1.0;
+    p->av_beta = 3.0;
+    p->mateps = 0.4;
+    p->matexp = 4.0;
+    p->normalsep = p->H * 0.3;
+    p->xsph_factor = 0.5;
+    p->fixed_dt = 0.002;
+    p->initial_dt = 0.002;
+    p->min_dt = 0.00002;
+    p->max_dt = 0.02;
+    p->accel_accuracy = 0.01;
+    p->velocity_accuracy = 0.09;
+    p->cw_n = std::sqrt(1.0 / 3.0);
+    p->const_acc[1] = -1.0;
+    for (int k = 0; k < 3; ++k) {
+        p->box_min[k] = -1.2;
+        p->box_max[k] = 1.2;
+    }
+    p->box_reflectiveness = 0.5;
+    return GSPH_OK;
+}
+
+int gsph_params_validate(const gsph_params* p, char* msg, size_t msg_len) {
+    auto bad = [&](int code, const char* why) {
+        if (msg && msg_len) std::snprintf(msg, msg_len, "%s", why);
+        return code;
+    };
+    if (!p) return bad(GSPH_E_INVALID, "params is NULL");
+    if (p->flags & ~GSPH_ALL_FLAGS) return bad(GSPH_E_INVALID, "unknown flag bits");
+    if (p->dimension < 1 || p->dimension > 3) return bad(GSPH_E_INVALID, "dimension must be 1, 2 or 3");
+    if (!(p->H > 0) || !std::isfinite(p->H)) return bad(GSPH_E_INVALID, "H must be positive and finite");
+    if (!(p->grav_eps >= 0) || !std::isfinite(p->grav_eps)) return bad(GSPH_E_INVALID, "grav_eps must be >= 0");
+    if ((p->flags & GSPH_PLASTICITY_MIESE) && (p->flags & GSPH_PLASTICITY_MC))
+        return bad(GSPH_E_INVALID, "choose up to one plasticity model (settings.h:203-205)");
+    if (p->flags & GSPH_SPH) {
+        if (!(p->rho0 > 0)) return bad(GSPH_E_INVALID, "rho0 must be positive");
+        if ((p->flags & GSPH_SOLIDS) && !(p->dbulk_dp != 0)) return bad(GSPH_E_INVALID, "dbulk_dp must be nonzero");
+    }
+    if (!(p->flags & GSPH_VARIABLE_TIMESTEP) && !(p->fixed_dt > 0)) return bad(GSPH_E_INVALID, "fixed_dt must be > 0");
+    if ((p->flags & GSPH_VARIABLE_TIMESTEP) && !(p->min_dt > 0 && p->max_dt >= p->min_dt && p->initial_dt > 0))
+        return bad(GSPH_E_INVALID, "variable step needs 0 < min_dt <= max_dt and initial_dt > 0");
+    if (msg && msg_len) msg[0] = 0;
+    return GSPH_OK;
+}
+
+int gsph_options_defaults(gsph_options* o) {
+    if (!o) return GSPH_E_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    o->accum = GSPH_ACCUM_PLAIN;
+    return GSPH_OK;
+}
+
+int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_ctx** out) {
+    if (!out) return fail(nullptr, GSPH_E_INVALID, "out is NULL");
+    *out = nullptr;
+    char why[160];
+    const int v = gsph_params_validate(p, why, sizeof why);
+    if (v != GSPH_OK) return fail(nullptr, v, why);
+    if (n < 1 || n > (int64_t(1) << 31)) return fail(nullptr, GSPH_E_INVALID, "n must be in [1, 2^31]");
+    gsph_options o;
+    if (opt) o = *opt;
+    else gsph_options_defaults(&o);
+    if (o.accum != GSPH_ACCUM_PLAIN && o.accum != GSPH_ACCUM_COMPENSATED)
+        return fail(nullptr, GSPH_E_INVALID, "options.accum must be GSPH_ACCUM_PLAIN or GSPH_ACCUM_COMPENSATED");
+    if (o.j_tile && !is_pow2_in(o.j_tile, 64, 1024)) return fail(nullptr, GSPH_E_INVALID, "j_tile: power of 2 in [64,1024]");
+    if (o.threads && o.threads != 64 && o.threads != 128 && o.threads != 256)
+        return fail(nullptr, GSPH_E_INVALID, "threads: 64, 128 or 256");
+    if (o.i_per_thread && o.i_per_thread != 1 && o.i_per_thread != 2 && o.i_per_thread != 4 && o.i_per_thread != 8)
+        return fail(nullptr, GSPH_E_INVALID, "i_per_thread: 1, 2, 4 or 8");
+    if (o.j_split < 0 || o.j_split > kMaxSplit) return fail(nullptr, GSPH_E_INVALID, "j_split out of range");
+
+    gsph_ctx* c = new (std::nothrow) gsph_ctx();
+    if (!c) return fail(nullptr, GSPH_E_NOMEM, "host allocation failed");
+    c->params = *p;
+    c->opt = o;
+    c->dp = make_dev_params(*p);
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(nullptr, GSPH_E_CUDA, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+    }
+    const int64_t n_pad = (n + kPad - 1) / kPad * kPad;
+    c->a.n = n;
+    c->a.n_pad = n_pad;
+
+    // launch shape
+    Launch& L = c->L;
+    L.accum = o.accum;
+    L.threads = o.threads ? o.threads : 128;
+    L.jt = o.j_tile ? o.j_tile : 256;
+    L.grav_threads = 128;
+    L.grav_ipt = o.i_per_thread ? o.i_per_thread : 4;
+    const int64_t ntiles = n_pad / L.jt;
+    const int cap = static_cast<int>(std::min<int64_t>(kMaxSplit, std::max<int64_t>(1, ntiles)));
+    L.nseg = o.j_split ? std::min(o.j_split, cap) : pick_split(n_pad / L.threads, c->sm_count * 4, cap);
+    L.grav_nseg = o.j_split ? std::min(o.j_split, cap)
+                            : pick_split(n_pad / (int64_t(L.grav_threads) * L.grav_ipt), c->sm_count * 4, cap);
+
+    cudaError_t ae = cudaSuccess;
+    auto F4 = [&](void) { return static_cast<float4*>(dalloc(c, n_pad * sizeof(float4), ae)); };
+    DevArrays& a = c->a;
+    a.posm = F4(); a.velrho = F4(); a.acc = F4(); a.xvel = F4();
+    a.sA = F4(); a.sB = F4(); a.dA = F4(); a.dB = F4(); a.jA = F4(); a.jB = F4();
+    a.pos64 = static_cast<double*>(dalloc(c, 3 * n_pad * sizeof(double), ae));
+    a.rhodot = static_cast<float*>(dalloc(c, n_pad * sizeof(float), ae));
+    a.balsara = static_cast<float*>(dalloc(c, n_pad * sizeof(float), ae));
+    a.part = static_cast<float*>(dalloc(c, partial_floats(c->dp, L, n_pad) * sizeof(float), ae));
+    a.dt_state = static_cast<float*>(dalloc(c, 4 * sizeof(float), ae));
+    a.diag = static_cast<double*>(dalloc(c, diag_scratch_doubles(n) * sizeof(double), ae));
+    a.status = static_cast<int*>(dalloc(c, sizeof(int) * 4, ae));
+    c->staging = static_cast<float*>(dalloc(c, 9 * n * sizeof(float), ae));
+    c->staging64 = static_cast<double*>(dalloc(c, 3 * n * sizeof(double), ae));
+    c->diag_out = static_cast<double*>(dalloc(c, 16 * sizeof(double), ae));
+    if (ae != cudaSuccess) {
+        release(c);
+        delete c;
+        return fail(nullptr, GSPH_E_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(ae));
+    }
+    e = cudaMemset(a.dt_state, 0, 4 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(a.status, 0, 4 * sizeof(int));
+    if (e == cudaSuccess) e = launch_init_padding(a, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        release(c);
+        delete c;
+        return fail(nullptr, GSPH_E_CUDA, std::string("context initialisation: ") + cudaGetErrorString(e));
+    }
+    c->launches = 1;
+    *out = c;
+    return GSPH_OK;
+}
+
+int gsph_destroy(gsph_ctx* c) {
+    if (!c) return GSPH_E_INVALID;
+    release(c);
+    delete c;
+    return GSPH_OK;
+}
+
+int gsph_upload(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!src) return fail(c, GSPH_E_INVALID, "src is NULL");
+    if (mask & ~GSPH_ALL_ATTRIBS) return fail(c, GSPH_E_INVALID, "unknown attribute bits in mask");
+    const float* ptrs[11] = {src->pos, src->mass, src->vel, src->acc, src->balsara, src->xvel,
+                             src->density, src->density_dt, src->dstress, src->dstress_dt, src->maxvsig};
+    static const int comps[11] = {3, 1, 3, 3, 1, 3, 1, 1, 9, 9, 1};
+    for (int k = 0; k < 11; ++k)
+        if ((mask >> k & 1u) && !ptrs[k]) return fail(c, GSPH_E_INVALID, "attribute pointer is NULL for a set mask bit");
+    cudaStream_t s = as_stream(stream);
+    for (int k = 0; k < 11; ++k) {
+        if (!(mask >> k & 1u)) continue;
+        GSPH_CK(c, cudaMemcpyAsync(c->staging, ptrs[k], comps[k] * c->a.n * sizeof(float), cudaMemcpyHostToDevice, s),
+                "upload copy");
+        GSPH_CK(c, launch_pack(c->a, k, c->staging, s), "upload pack");
+        c->launches += 1;
+    }
+    if (c->opt.check_finite) {
+        GSPH_CK(c, launch_check_finite(c->a, s), "finite check");
+        c->launches += 1;
+        return check_status(c, s);
+    }
+    return GSPH_OK;
+}
+
+int gsph_download(gsph_ctx* c, uint32_t mask, gsph_host_particles* dst, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!dst) return fail(c, GSPH_E_INVALID, "dst is NULL");
+    if (mask & ~GSPH_ALL_ATTRIBS) return fail(c, GSPH_E_INVALID, "unknown attribute bits in mask");
+    float* ptrs[11] = {dst->pos, dst->mass, dst->vel, dst->acc, dst->balsara, dst->xvel,
+                       dst->density, dst->density_dt, dst->dstress, dst->dstress_dt, dst->maxvsig};
+    static const int comps[11] = {3, 1, 3, 3, 1, 3, 1, 1, 9, 9, 1};
+    for (int k = 0; k < 11; ++k)
+        if ((mask >> k & 1u) && !ptrs[k]) return fail(c, GSPH_E_INVALID, "attribute pointer is NULL for a set mask bit");
+    cudaStream_t s = as_stream(stream);
+    for (int k = 0; k < 11; ++k) {
+        if (!(mask >> k & 1u)) continue;
+        GSPH_CK(c, launch_unpack(c->a, k, c->staging, s), "download unpack");
+        c->launches += 1;
+        GSPH_CK(c, cudaMemcpyAsync(ptrs[k], c->staging, comps[k] * c->a.n * sizeof(float), cudaMemcpyDeviceToHost, s),
+                "download copy");
+    }
+    return check_status(c, s);
+}
+
+int gsph_upload_pos64(gsph_ctx* c, const double* pos, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!pos) return fail(c, GSPH_E_INVALID, "pos is NULL");
+    cudaStream_t s = as_stream(stream);
+    GSPH_CK(c, cudaMemcpyAsync(c->staging64, pos, 3 * c->a.n * sizeof(double), cudaMemcpyHostToDevice, s), "upload copy");
+    GSPH_CK(c, launch_pack_pos64(c->a, c->staging64, s), "upload pack");
+    c->launches += 1;
+    return GSPH_OK;
+}
+
+int gsph_download_pos64(gsph_ctx* c, double* pos, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!pos) return fail(c, GSPH_E_INVALID, "pos is NULL");
+    cudaStream_t s = as_stream(stream);
+    GSPH_CK(c, launch_unpack_pos64(c->a, c->staging64, s), "download unpack");
+    c->launches += 1;
+    GSPH_CK(c, cudaMemcpyAsync(pos, c->staging64, 3 * c->a.n * sizeof(double), cudaMemcpyDeviceToHost, s), "download copy");
+    return check_status(c, s);
+}
+
+int gsph_compute_derivatives(gsph_ctx* c, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    return derivatives(c, as_stream(stream));
+}
+
+int gsph_integrate(gsph_ctx* c, int not_first_step, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    return integrate(c, not_first_step, as_stream(stream));
+}
+
+int gsph_step(gsph_ctx* c, int32_t nsteps, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (nsteps < 0) return fail(c, GSPH_E_INVALID, "nsteps < 0");
+    if (nsteps == 0) return GSPH_OK;
+    cudaStream_t s = as_stream(stream);
+    if (!c->graph_exec) {
+        if (!c->capture_stream) GSPH_CK(c, cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking), "stream");
+        const int64_t before = c->launches;
+        bool was_pending[GSPH_KSLOTS];
+        for (int k = 0; k < GSPH_KSLOTS; ++k) {
+            was_pending[k] = c->pending[k];
+            c->pending[k] = false;
+        }
+        GSPH_CK(c, cudaStreamBeginCapture(c->capture_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = GSPH_OK;
+        const KTimer* st = slot_timer(c, GSPH_KSLOT_STEP);
+        if (st) {
+            const cudaError_t te = timer_record(st->start, c->capture_stream);
+            if (te != cudaSuccess) rc = cuda_fail(c, te, "timer");
+        }
+        if (rc == GSPH_OK) rc = derivatives(c, c->capture_stream);
+        if (rc == GSPH_OK) rc = integrate(c, 1, c->capture_stream);
+        if (rc == GSPH_OK && st) {
+            const cudaError_t te = timer_record(st->stop, c->capture_stream);
+            if (te != cudaSuccess) rc = cuda_fail(c, te, "timer");
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(c->capture_stream, &g);
+        c->launches = before;
+        uint32_t slots = 0;
+        for (int k = 0; k < GSPH_KSLOTS; ++k) {
+            if (c->pending[k]) slots |= 1u << k;
+            c->pending[k] = was_pending[k];
+        }
+        if (rc != GSPH_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ee != cudaSuccess) return cuda_fail(c, ee, "end capture");
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+        if (ie != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return cuda_fail(c, ie, "graph instantiate");
+        }
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        int64_t kernels = 0;
+        if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (auto nd : nodes) {
+            cudaGraphNodeType ty;
+            if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        c->graph = g;
+        c->graph_exec = ex;
+        c->graph_kernels = kernels;
+        c->graph_slots = slots;
+    }
+    for (int32_t k = 0; k < nsteps; ++k) {
+        GSPH_CK(c, cudaGraphLaunch(c->graph_exec, s), "graph launch");
+        c->launches += c->graph_kernels;
+    }
+    for (int k = 0; k < GSPH_KSLOTS; ++k)
+        if (c->graph_slots >> k & 1u) c->pending[k] = true;
+    return GSPH_OK;
+}
+
+int gsph_current_timestep(gsph_ctx* c, double* dt, void* stream) {
+    if (!c || !dt) return c ? fail(c, GSPH_E_INVALID, "dt is NULL") : GSPH_E_INVALID;
+    if (!(c->params.flags & GSPH_VARIABLE_TIMESTEP)) {
+        *dt = static_cast<float>(c->params.fixed_dt);  // f1_t fixed_timestep
+        return GSPH_OK;
+    }
+    float v = 0.0f;
+    cudaStream_t s = as_stream(stream);
+    GSPH_CK(c, cudaMemcpyAsync(&v, c->a.dt_state, sizeof(float), cudaMemcpyDeviceToHost, s), "timestep read");
+    GSPH_CK(c, cudaStreamSynchronize(s), "stream synchronize");
+    *dt = v;
+    return GSPH_OK;
+}
+
+int gsph_diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!out) return fail(c, GSPH_E_INVALID, "out is NULL");
+    cudaStream_t s = as_stream(stream);
+    GSPH_CK(c, launch_diagnostics(c->a, c->dp, half_kick, c->diag_out, s), "diagnostics");
+    c->launches += 2;
+    double h[12];
+    GSPH_CK(c, cudaMemcpyAsync(h, c->diag_out, sizeof h, cudaMemcpyDeviceToHost, s), "diagnostics read");
+    const int rc = check_status(c, s);
+    if (rc != GSPH_OK) return rc;
+    out->e_kin = h[0];
+    out->e_grav = h[1];
+    out->e_int = h[2];
+    out->e_shear = h[3];
+    for (int k = 0; k < 3; ++k) {
+        out->momentum[k] = h[4 + k];
+        out->ang_mom[k] = h[7 + k];
+    }
+    out->mass = h[10];
+    return GSPH_OK;
+}
+
+int gsph_size(gsph_ctx* c, int64_t* n) {
+    if (!c || !n) return GSPH_E_INVALID;
+    *n = c->a.n;
+    return GSPH_OK;
+}
+
+const char* gsph_last_error(gsph_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int gsph_device_view_get(gsph_ctx* c, gsph_device_view* v) {
+    if (!c || !v) return GSPH_E_INVALID;
+    v->n = c->a.n;
+    v->posm = c->a.posm;
+    v->velrho = c->a.velrho;
+    v->acc = c->a.acc;
+    v->pos64 = c->a.pos64;
+    return GSPH_OK;
+}
+
+int gsph_launch_count(gsph_ctx* c, int64_t* count) {
+    if (!c || !count) return GSPH_E_INVALID;
+    *count = c->launches;
+    return GSPH_OK;
+}
+
+int gsph_profile_enable(gsph_ctx* c, int on) {
+    if (!c) return GSPH_E_INVALID;
+    if ((on != 0) == c->profiling) return GSPH_OK;
+    drop_graph(c);
+    if (on)
+        for (auto& t : c->timers) {
+            if (!t.start) GSPH_CK(c, cudaEventCreate(&t.start), "event create");
+            if (!t.stop) GSPH_CK(c, cudaEventCreate(&t.stop), "event create");
+        }
+    c->profiling = on != 0;
+    for (bool& b : c->pending) b = false;
+    return GSPH_OK;
+}
+
+int gsph_profile_collect(gsph_ctx* c) {
+    if (!c) return GSPH_E_INVALID;
+    for (int k = 0; k < GSPH_KSLOTS; ++k) {
+        if (!c->pending[k] || !c->timers[k].stop) continue;
+        GSPH_CK(c, cudaEventSynchronize(c->timers[k].stop), "event synchronize");
+        float ms = 0.0f;
+        GSPH_CK(c, cudaEventElapsedTime(&ms, c->timers[k].start, c->timers[k].stop), "event elapsed");
+        c->prof_ms[k] += ms;
+        c->prof_launches[k] += 1;
+        c->pending[k] = false;
+    }
+    return GSPH_OK;
+}
+
+int gsph_profile_read(gsph_ctx* c, gsph_profile* out) {
+    if (!c || !out) return GSPH_E_INVALID;
+    for (int k = 0; k < GSPH_KSLOTS; ++k) {
+        out->ms[k] = c->prof_ms[k];
+        out->launches[k] = c->prof_launches[k];
+    }
+    return GSPH_OK;
+}
+
+int gsph_profile_reset(gsph_ctx* c) {
+    if (!c) return GSPH_E_INVALID;
+    for (int k = 0; k < GSPH_KSLOTS; ++k) {
+        c->prof_ms[k] = 0.0;
+        c->prof_launches[k] = 0;
+    }
+    return GSPH_OK;
+}
+
+int gsph_measure_fp32_peak(double seconds, double* tflops) {
+    if (!tflops || !(seconds > 0)) return fail(nullptr, GSPH_E_INVALID, "bad arguments");
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    float* sink = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&sink, 4096 * sizeof(float));
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    int iters = 256;
+    double best = 0.0;
+    for (int round = 0; e == cudaSuccess && round < 12; ++round) {
+        e = cudaEventRecord(a, 0);
+        if (e == cudaSuccess) e = launch_fp32_peak(sms, iters, sink, 0);
+        if (e == cudaSuccess) e = cudaEventRecord(b, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e != cudaSuccess) break;
+        const double tf = static_cast<double>(fp32_peak_flops(sms, iters)) / (ms * 1e-3) / 1e12;
+        if (ms > 0.25 * seconds * 1e3) best = std::max(best, tf);
+        if (ms < 0.25 * seconds * 1e3) iters = static_cast<int>(std::min<double>(iters * 4.0, 1 << 28));
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (sink) cudaFree(sink);
+    if (e != cudaSuccess) return fail(nullptr, GSPH_E_CUDA, std::string("fp32 peak: ") + cudaGetErrorString(e));
+    *tflops = best;
+    return GSPH_OK;
+}
+
+}  // extern "C"

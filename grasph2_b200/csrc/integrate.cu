@@ -1,0 +1,421 @@
+// integrate.cu -- per-particle kernels: the leapfrog (src/integration.h), the variable-step
+// reduction, FP64 diagnostics, and the host-layout pack/unpack used by upload/download.
+//
+// HBM-bound: each kernel touches each particle once with coalesced float4 / double streams.
+#include "integrate.cuh"
+
+namespace gsph {
+
+namespace {
+
+inline unsigned blocks_for(int64_t n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
+
+__device__ __forceinline__ float murnaghan(const DevParams& p, float rho) {
+    return p.bulk / p.dbulk * (powf(rho / p.rho0, p.dbulk) - 1.0f);
+}
+
+// plasticity (src/sph/models.h:194-205) on the six stored components of the symmetric S:
+// J2 = 1/2 sum_de S_de^2 counts each off-diagonal twice; S *= Y^2/(3 J2) when that is < 1
+__device__ __forceinline__ void plasticity(float4& a, float4& b, float Y) {
+    const float J2 = 0.5f * (a.x * a.x + a.y * a.y + a.z * a.z + 2.0f * (a.w * a.w + b.x * b.x + b.y * b.y));
+    const float f = Y * Y / (3.0f * J2);
+    if (f < 1.0f) {
+        a.x *= f; a.y *= f; a.z *= f; a.w *= f;
+        b.x *= f; b.y *= f;
+    }
+}
+
+// the per-particle update shared by fixedTsLeapfrog (integration.h:90-124) and
+// variableTsLeapfrog_useNewTimestep (:171-217): kick, drift (FP64 master position), density and
+// stress update, plasticity, box boundary
+__device__ __forceinline__ void kick_drift(const DevArrays& a, const DevParams& p, int64_t i, float kick_dt, float dt) {
+    float4 vr = a.velrho[i];
+    const float4 ac = a.acc[i];
+    vr.x = fmaf(ac.x, kick_dt, vr.x);
+    vr.y = fmaf(ac.y, kick_dt, vr.y);
+    vr.z = fmaf(ac.z, kick_dt, vr.z);
+    float ux = vr.x, uy = vr.y, uz = vr.z;
+    const bool sph = has(p, GSPH_SPH);
+    if (sph && has(p, GSPH_XSPH)) {
+        const float4 xv = a.xvel[i];
+        ux = fmaf(p.xsph, xv.x, ux);
+        uy = fmaf(p.xsph, xv.y, uy);
+        uz = fmaf(p.xsph, xv.z, uz);
+    }
+    const int64_t np = a.n_pad;
+    double x = a.pos64[i], y = a.pos64[np + i], z = a.pos64[2 * np + i];
+    x += static_cast<double>(ux) * static_cast<double>(dt);
+    y += static_cast<double>(uy) * static_cast<double>(dt);
+    z += static_cast<double>(uz) * static_cast<double>(dt);
+    if (sph) {
+        if (has(p, GSPH_INTEGRATE_DENSITY)) {
+            float rho = fmaf(a.rhodot[i], dt, vr.w);
+            if (rho < 0.0f) rho = 0.0f;
+            vr.w = rho;
+        }
+        if (has(p, GSPH_SOLIDS)) {
+            float4 sa = a.sA[i], sb = a.sB[i];
+            const float4 da = a.dA[i], db = a.dB[i];
+            sa.x = fmaf(da.x, dt, sa.x); sa.y = fmaf(da.y, dt, sa.y); sa.z = fmaf(da.z, dt, sa.z);
+            sa.w = fmaf(da.w, dt, sa.w); sb.x = fmaf(db.x, dt, sb.x); sb.y = fmaf(db.y, dt, sb.y);
+            if (has(p, GSPH_PLASTICITY_MC))  // doPlasticity (integration.h:24-31), updated density
+                plasticity(sa, sb, p.tanfr * murnaghan(p, vr.w) + p.cohesion);
+            else if (has(p, GSPH_PLASTICITY_MIESE))
+                plasticity(sa, sb, p.Y);
+            a.sA[i] = sa;
+            a.sB[i] = sb;
+        }
+    }
+    if (has(p, GSPH_SIMPLE_BOX_BOUNDARY)) {  // handleBoundaryConditions (integration.h:33-73)
+        const float m = 1.0f + p.box_refl;
+        double* xc[3] = {&x, &y, &z};
+        float* vc[3] = {&vr.x, &vr.y, &vr.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (d == 2 && p.dim != 3) break;
+            if (*xc[d] > static_cast<double>(p.box_max[d])) {
+                *xc[d] = p.box_max[d];
+                *vc[d] -= m * *vc[d];
+            } else if (*xc[d] < static_cast<double>(p.box_min[d])) {
+                *xc[d] = p.box_min[d];
+                *vc[d] -= m * *vc[d];
+            }
+        }
+    }
+    a.pos64[i] = x;
+    a.pos64[np + i] = y;
+    a.pos64[2 * np + i] = z;
+    const float mass = a.posm[i].w;
+    a.posm[i] = make_float4(static_cast<float>(x), static_cast<float>(y), static_cast<float>(z), mass);
+    a.velrho[i] = vr;
+}
+
+__global__ void k_leapfrog_fixed(DevArrays a, DevParams p, float kick_dt) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    kick_drift(a, p, i, kick_dt, p.fixed_dt);
+}
+
+// variableTsLeapfrog_getNewTimestep (integration.h:130-169): closing half kick with the current
+// step and the min of the step criteria; block min, then an integer atomicMin on the positive
+// float's bit pattern
+__global__ void k_dt_criteria(DevArrays a, DevParams p) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const float dt = a.dt_state[0];
+    float mindt = p.max_dt;
+    if (i < a.n) {
+        float4 vr = a.velrho[i];
+        const float4 ac = a.acc[i];
+        vr.x = fmaf(ac.x, dt * 0.5f, vr.x);
+        vr.y = fmaf(ac.y, dt * 0.5f, vr.y);
+        vr.z = fmaf(ac.z, dt * 0.5f, vr.z);
+        a.velrho[i] = vr;
+        if (has(p, GSPH_ACCELERATION_CRITERION))
+            mindt = fminf(mindt, sqrtf(p.accel_acc * p.H / sqrtf(ac.x * ac.x + ac.y * ac.y + ac.z * ac.z)));
+        if (has(p, GSPH_VELOCITY_CRITERION)) mindt = fminf(mindt, p.vel_acc * p.H / ac.w);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mindt = fminf(mindt, __shfl_xor_sync(0xffffffffu, mindt, o));
+    __shared__ float wmin[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) wmin[warp] = mindt;
+    __syncthreads();
+    if (warp == 0) {
+        mindt = (lane < static_cast<int>(blockDim.x >> 5)) ? wmin[lane] : p.max_dt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mindt = fminf(mindt, __shfl_xor_sync(0xffffffffu, mindt, o));
+        if (lane == 0) atomicMin(reinterpret_cast<int*>(a.dt_state + 1), __float_as_int(mindt));
+    }
+}
+
+__global__ void k_dt_first(DevArrays a, DevParams p) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) a.dt_state[1] = p.initial_dt;  // integration.h:235-236
+}
+
+// variableTsLeapfrog_useNewTimestep (integration.h:171-217)
+__global__ void k_leapfrog_variable(DevArrays a, DevParams p) {
+    const float nxt = a.dt_state[1];
+    const float dt = nxt < p.min_dt ? p.min_dt : nxt;
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    kick_drift(a, p, i, dt * 0.5f, dt);
+}
+
+// commit the step chosen above as the current one (after every block has read `next`)
+__global__ void k_dt_commit(DevArrays a, DevParams p) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const float nxt = a.dt_state[1];
+        a.dt_state[0] = nxt < p.min_dt ? p.min_dt : nxt;
+    }
+}
+
+// ---- FP64 diagnostics ---------------------------------------------------------------------------
+constexpr int kDiagFields = 12;  // e_kin, e_grav, e_int, e_shear, px, py, pz, lx, ly, lz, mass, (pad)
+constexpr int kDiagThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) r += sh[w];  // fixed order
+    return r;
+}
+
+// per-particle terms and, per i, its share of the pair potential against j > i; one row of
+// kDiagFields block partials per CTA (deterministic second stage)
+__global__ void __launch_bounds__(kDiagThreads) k_diag(DevArrays a, DevParams p, double half_kick) {
+    __shared__ double tile[4][kDiagThreads];
+    __shared__ double red[32];
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t np = a.n_pad;
+    double f[kDiagFields];
+#pragma unroll
+    for (int k = 0; k < kDiagFields; ++k) f[k] = 0.0;
+    double xi = 0, yi = 0, zi = 0, mi = 0;
+    if (i < a.n) {
+        const float4 pm = a.posm[i];
+        const float4 vr = a.velrho[i];
+        const float4 ac = a.acc[i];
+        mi = pm.w;
+        xi = a.pos64[i]; yi = a.pos64[np + i]; zi = a.pos64[2 * np + i];
+        const double vx = vr.x + half_kick * ac.x, vy = vr.y + half_kick * ac.y, vz = vr.z + half_kick * ac.z;
+        f[0] = 0.5 * mi * (vx * vx + vy * vy + vz * vz);
+        f[4] = mi * vx; f[5] = mi * vy; f[6] = mi * vz;
+        f[7] = mi * (yi * vz - zi * vy); f[8] = mi * (zi * vx - xi * vz); f[9] = mi * (xi * vy - yi * vx);
+        f[10] = mi;
+        if (has(p, GSPH_SPH)) {
+            const double rho = vr.w, r0 = p.rho0;
+            if (has(p, GSPH_SOLIDS)) {
+                const double K = p.bulk, nn = p.dbulk;
+                double u;
+                if (fabs(nn - 1.0) < 1e-12) u = K / r0 * (log(rho / r0) + r0 / rho - 1.0);
+                else u = K / nn * ((pow(rho, nn - 1.0) - pow(r0, nn - 1.0)) / ((nn - 1.0) * pow(r0, nn)) + (1.0 / rho - 1.0 / r0));
+                f[2] = mi * u;
+                const float4 sa = a.sA[i], sb = a.sB[i];
+                const double ss = double(sa.x) * sa.x + double(sa.y) * sa.y + double(sa.z) * sa.z +
+                                  2.0 * (double(sa.w) * sa.w + double(sb.x) * sb.x + double(sb.y) * sb.y);
+                f[3] = mi * ss / (4.0 * p.shear * rho);
+            } else {
+                const double c2 = double(p.c) * p.c;
+                f[2] = mi * c2 * (log(rho / r0) + r0 / rho - 1.0);
+            }
+        }
+    }
+    // pair potential: -G m_i sum_{j>i} m_j / sqrt(r^2 + eps^2), j-tiles of blockDim through shared memory
+    if (has(p, GSPH_SELF_GRAVITY)) {
+        const double eps2 = static_cast<double>(p.eps2);
+        double phi = 0.0;
+        const int64_t j_first = static_cast<int64_t>(blockIdx.x) * blockDim.x;  // j > i needs j >= block start
+        for (int64_t t0 = j_first; t0 < a.n; t0 += blockDim.x) {
+            const int64_t j = t0 + threadIdx.x;
+            __syncthreads();
+            if (j < a.n) {
+                tile[0][threadIdx.x] = a.pos64[j];
+                tile[1][threadIdx.x] = a.pos64[np + j];
+                tile[2][threadIdx.x] = a.pos64[2 * np + j];
+                tile[3][threadIdx.x] = a.posm[j].w;
+            } else {
+                tile[3][threadIdx.x] = 0.0;
+                tile[0][threadIdx.x] = tile[1][threadIdx.x] = tile[2][threadIdx.x] = 0.0;
+            }
+            __syncthreads();
+            if (i < a.n) {
+                const int64_t rem = a.n - t0;
+                const int cnt = rem < static_cast<int64_t>(blockDim.x) ? static_cast<int>(rem) : static_cast<int>(blockDim.x);
+                for (int jj = 0; jj < cnt; ++jj) {
+                    if (t0 + jj <= i) continue;
+                    const double dx = tile[0][jj] - xi, dy = tile[1][jj] - yi, dz = tile[2][jj] - zi;
+                    phi += tile[3][jj] / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+                }
+            }
+        }
+        f[1] = -static_cast<double>(p.G) * mi * phi;
+    }
+    for (int k = 0; k < kDiagFields; ++k) {
+        const double s = block_sum(f[k], red);
+        if (threadIdx.x == 0) a.diag[static_cast<int64_t>(blockIdx.x) * kDiagFields + k] = s;
+    }
+}
+
+__global__ void k_diag_reduce(DevArrays a, int nblocks, double* out) {
+    const int k = threadIdx.x;
+    if (k >= kDiagFields) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += a.diag[static_cast<int64_t>(b) * kDiagFields + k];
+    out[k] = s;
+}
+
+// ---- host layout <-> device layout ------------------------------------------------------------
+// attribute ids follow the bit order of GSPH_POS ... GSPH_MAXVSIG
+__global__ void k_pack(DevArrays a, int attr, const float* __restrict__ src) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t np = a.n_pad;
+    switch (attr) {
+        case 0: {  // POS
+            const float x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+            a.pos64[i] = x; a.pos64[np + i] = y; a.pos64[2 * np + i] = z;
+            float4 q = a.posm[i];
+            q.x = x; q.y = y; q.z = z;
+            a.posm[i] = q;
+            break;
+        }
+        case 1: { float4 q = a.posm[i]; q.w = src[i]; a.posm[i] = q; break; }  // MASS
+        case 2: { float4 q = a.velrho[i]; q.x = src[3 * i]; q.y = src[3 * i + 1]; q.z = src[3 * i + 2]; a.velrho[i] = q; break; }
+        case 3: { float4 q = a.acc[i]; q.x = src[3 * i]; q.y = src[3 * i + 1]; q.z = src[3 * i + 2]; a.acc[i] = q; break; }
+        case 4: a.balsara[i] = src[i]; break;
+        case 5: a.xvel[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f); break;
+        case 6: { float4 q = a.velrho[i]; q.w = src[i]; a.velrho[i] = q; break; }
+        case 7: a.rhodot[i] = src[i]; break;
+        case 8:
+        case 9: {  // DSTRESS / DSTRESS_DT: 9 row-major values, symmetrised
+            const float* m = src + 9 * i;
+            const float4 A = make_float4(m[0], m[4], m[8], 0.5f * (m[1] + m[3]));
+            const float4 B = make_float4(0.5f * (m[2] + m[6]), 0.5f * (m[5] + m[7]), 0.0f, 0.0f);
+            if (attr == 8) { a.sA[i] = A; a.sB[i] = B; }
+            else { a.dA[i] = A; a.dB[i] = B; }
+            break;
+        }
+        case 10: { float4 q = a.acc[i]; q.w = src[i]; a.acc[i] = q; break; }
+        default: break;
+    }
+}
+
+__global__ void k_unpack(DevArrays a, int attr, float* __restrict__ dst) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    switch (attr) {
+        case 0: { const float4 q = a.posm[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
+        case 1: dst[i] = a.posm[i].w; break;
+        case 2: { const float4 q = a.velrho[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
+        case 3: { const float4 q = a.acc[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
+        case 4: dst[i] = a.balsara[i]; break;
+        case 5: { const float4 q = a.xvel[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
+        case 6: dst[i] = a.velrho[i].w; break;
+        case 7: dst[i] = a.rhodot[i]; break;
+        case 8:
+        case 9: {
+            const float4 A = (attr == 8) ? a.sA[i] : a.dA[i];
+            const float4 B = (attr == 8) ? a.sB[i] : a.dB[i];
+            float* m = dst + 9 * i;
+            m[0] = A.x; m[1] = A.w; m[2] = B.x;
+            m[3] = A.w; m[4] = A.y; m[5] = B.y;
+            m[6] = B.x; m[7] = B.y; m[8] = A.z;
+            break;
+        }
+        case 10: dst[i] = a.acc[i].w; break;
+        default: break;
+    }
+}
+
+__global__ void k_pack_pos64(DevArrays a, const double* __restrict__ src) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t np = a.n_pad;
+    const double x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+    a.pos64[i] = x; a.pos64[np + i] = y; a.pos64[2 * np + i] = z;
+    float4 q = a.posm[i];
+    q.x = static_cast<float>(x); q.y = static_cast<float>(y); q.z = static_cast<float>(z);
+    a.posm[i] = q;
+}
+
+__global__ void k_unpack_pos64(DevArrays a, double* __restrict__ dst) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t np = a.n_pad;
+    dst[3 * i] = a.pos64[i]; dst[3 * i + 1] = a.pos64[np + i]; dst[3 * i + 2] = a.pos64[2 * np + i];
+}
+
+// inert padding: zero mass, far away (never a neighbour, no gravitational pull), unit density
+__global__ void k_init_padding(DevArrays a) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n_pad) return;
+    const float far = 1e18f;
+    if (i >= a.n) {
+        a.posm[i] = make_float4(far, far, far, 0.0f);
+        a.velrho[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        a.pos64[i] = far; a.pos64[a.n_pad + i] = far; a.pos64[2 * a.n_pad + i] = far;
+    } else {
+        a.posm[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        a.velrho[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        a.pos64[i] = 0.0; a.pos64[a.n_pad + i] = 0.0; a.pos64[2 * a.n_pad + i] = 0.0;
+    }
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.acc[i] = z; a.xvel[i] = z; a.sA[i] = z; a.sB[i] = z; a.dA[i] = z; a.dB[i] = z; a.jA[i] = z; a.jB[i] = z;
+    a.rhodot[i] = 0.0f;
+    a.balsara[i] = 0.0f;
+}
+
+// scan for NaN/Inf in the state (host-requested check); sets status bit 2
+__global__ void k_check_finite(DevArrays a) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float4 q = a.posm[i], v = a.velrho[i];
+    const bool bad = !(isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w) && isfinite(v.x) &&
+                       isfinite(v.y) && isfinite(v.z) && isfinite(v.w));
+    if (bad) atomicOr(a.status, 2);
+}
+
+}  // namespace
+
+cudaError_t launch_leapfrog(const DevArrays& a, const DevParams& p, int not_first_step, cudaStream_t s) {
+    const unsigned nb = blocks_for(a.n, 256);
+    if (!has(p, GSPH_VARIABLE_TIMESTEP)) {
+        k_leapfrog_fixed<<<nb, 256, 0, s>>>(a, p, p.fixed_dt * (not_first_step ? 1.0f : 0.5f));
+        return cudaGetLastError();
+    }
+    if (not_first_step) k_dt_criteria<<<nb, 256, 0, s>>>(a, p);
+    else k_dt_first<<<1, 32, 0, s>>>(a, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_leapfrog_variable<<<nb, 256, 0, s>>>(a, p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_dt_commit<<<1, 32, 0, s>>>(a, p);
+    return cudaGetLastError();
+}
+
+int leapfrog_kernel_count(const DevParams& p) { return has(p, GSPH_VARIABLE_TIMESTEP) ? 3 : 1; }
+
+size_t diag_scratch_doubles(int64_t n) { return static_cast<size_t>(blocks_for(n, kDiagThreads)) * kDiagFields + kDiagFields; }
+
+cudaError_t launch_diagnostics(const DevArrays& a, const DevParams& p, double half_kick, double* out_dev, cudaStream_t s) {
+    const unsigned nb = blocks_for(a.n, kDiagThreads);
+    k_diag<<<nb, kDiagThreads, 0, s>>>(a, p, half_kick);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_diag_reduce<<<1, 32, 0, s>>>(a, static_cast<int>(nb), out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const DevArrays& a, int attr, const float* src_dev, cudaStream_t s) {
+    k_pack<<<blocks_for(a.n, 256), 256, 0, s>>>(a, attr, src_dev);
+    return cudaGetLastError();
+}
+cudaError_t launch_unpack(const DevArrays& a, int attr, float* dst_dev, cudaStream_t s) {
+    k_unpack<<<blocks_for(a.n, 256), 256, 0, s>>>(a, attr, dst_dev);
+    return cudaGetLastError();
+}
+cudaError_t launch_pack_pos64(const DevArrays& a, const double* src_dev, cudaStream_t s) {
+    k_pack_pos64<<<blocks_for(a.n, 256), 256, 0, s>>>(a, src_dev);
+    return cudaGetLastError();
+}
+cudaError_t launch_unpack_pos64(const DevArrays& a, double* dst_dev, cudaStream_t s) {
+    k_unpack_pos64<<<blocks_for(a.n, 256), 256, 0, s>>>(a, dst_dev);
+    return cudaGetLastError();
+}
+cudaError_t launch_init_padding(const DevArrays& a, cudaStream_t s) {
+    k_init_padding<<<blocks_for(a.n_pad, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_check_finite(const DevArrays& a, cudaStream_t s) {
+    k_check_finite<<<blocks_for(a.n, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace gsph

@@ -1,0 +1,724 @@
+// pairs.cu -- the all-pairs kernels of computeDerivatives (src/computeDerivatives.h:52-328).
+//
+//   k_density        calcDensity            (:52-91)    rho_i = sum_{0<r<=H} m_j W(r_ij)
+//   k_pairs<VGRAD>   calcBalsaraDensityDTDStressDT (:96-162) strain/rotation rate, div v, curl
+//   k_pairs<ACC>     calcAcceleration       (:167-313)  gravity + stress + AV (+XSPH, art. stress)
+//   k_pairs<FUSED>   both in one pass, used whenever the acceleration does not need the Balsara
+//                    values of the same step (the switch off): one N^2 sweep instead of two
+//   k_gravity<I>     calcAcceleration with ENABLE_SPH off: register-blocked pure gravity
+//   *_finish         sum the j-segment partials in a fixed order, then the per-particle epilogue
+//                    (do_after of each job): density floor, Jaumann stress rate, drho/dt,
+//                    Balsara switch, environment acceleration
+//
+// Arithmetic is FP32. GSPH_ACCUM_COMPENSATED accumulates each j-tile in FP32, folds the tile
+// partial into a (sum, error) pair with a two-sum, and combines the j-segments in FP64.
+#include <algorithm>
+#include <cfloat>
+
+#include "pairs.cuh"
+
+namespace gsph {
+
+namespace {
+
+// ---- SPH building blocks (src/sph/kernel.h, eos.h, models.h) ---------------------------------
+// spline polynomial of Wspline without its prefactor, q in [0,1] (kernel.h:130-136)
+__device__ __forceinline__ float w_poly(float q) {
+    if (q > 1.0f) return 0.0f;
+    if (q < 0.5f) return 6.0f * q * q * q - 6.0f * q * q + 1.0f;
+    const float a = 1.0f - q;
+    return 2.0f * a * a * a;
+}
+// polynomial of dWspline without its prefactor (kernel.h:169-175)
+__device__ __forceinline__ float dw_poly(float q) {
+    if (q > 1.0f) return 0.0f;
+    if (q < 0.5f) return 3.0f * q * q - 2.0f * q;
+    const float a = 1.0f - q;
+    return -a * a;
+}
+// pressure of the selected EOS (eos.h:88-96; computeDerivatives.h:200,205)
+__device__ __forceinline__ float eos_pressure(const DevParams& p, float rho) {
+    if (has(p, GSPH_SOLIDS)) return p.bulk / p.dbulk * (powf(rho / p.rho0, p.dbulk) - 1.0f);
+    return p.c2 * (rho - p.rho0);
+}
+// j-record of one particle: sigma/rho^2 in (A, B) with B.z = Balsara value
+__device__ __forceinline__ void make_jrecord(const DevParams& p, float rho, float4 sA, float4 sB, float bal,
+                                             float4& jA, float4& jB) {
+    const float pres = eos_pressure(p, rho);
+    if (has(p, GSPH_SOLIDS)) {
+        jA = make_float4((sA.x - pres) / (rho * rho), (sA.y - pres) / (rho * rho), (sA.z - pres) / (rho * rho),
+                         sA.w / (rho * rho));
+        jB = make_float4(sB.x / (rho * rho), sB.y / (rho * rho), bal, 0.0f);
+    } else {
+        const float s = -pres / (rho * rho);
+        jA = make_float4(s, s, s, 0.0f);
+        jB = make_float4(0.0f, 0.0f, bal, 0.0f);
+    }
+}
+// artificialStress / artificialPressure (models.h:212-223)
+__device__ __forceinline__ float art(float mateps, float s) { return s > 0.0f ? -mateps * s : 0.0f; }
+
+// neighbour test 0 < x <= hi for a non-negative float x, on the bit patterns: one add, one compare
+__device__ __forceinline__ bool in_open_closed(float x, uint32_t lo_bits, uint32_t span_bits) {
+    return (__float_as_uint(x) - lo_bits - 1u) < span_bits;
+}
+
+// ================================================================================================
+// density
+// ================================================================================================
+template <bool COMP>
+__global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm, float* __restrict__ part,
+                                                  int64_t n_pad, int jt, int nseg, DevParams p, int* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    JTilePipe<1> pipe;
+    pipe.buf = reinterpret_cast<float4*>(smem_raw);
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * jt * sizeof(float4));
+    pipe.src[0] = posm;
+    pipe.jt = jt;
+    pipe.status = status;
+    segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const float4 pi = posm[i];
+    const uint32_t span = __float_as_uint(p.H2);
+    float rho_s = 0.0f, rho_c = 0.0f;
+
+    pipe.start();
+    pipe.run([&](const float4* J) {
+        float rho_t = 0.0f;
+#pragma unroll 8
+        for (int j = 0; j < jt; ++j) {
+            const float4 q = J[j];
+            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (in_open_closed(r2, 0u, span)) {  // calcDensity: r2 <= H2 && r2 > 0
+                const float r = r2 * rsqrtf(r2);
+                rho_t = fmaf(q.w, w_poly(r * p.inv_h), rho_t);
+            }
+        }
+        if (COMP) fold(rho_s, rho_c, rho_t);
+        else rho_s += rho_t;
+    });
+    const int64_t seg = blockIdx.y;
+    part[(seg * (COMP ? 2 : 1)) * n_pad + i] = rho_s;
+    if (COMP) part[(seg * 2 + 1) * n_pad + i] = rho_c;
+}
+
+// sum the segments, apply the prefactor and the optional floor (computeDerivatives.h:85-88), then
+// build the j-record sigma/rho^2 of the new density
+template <bool COMP>
+__global__ void k_density_finish(DevArrays a, DevParams p, int nseg) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    float rho;
+    if (COMP) {
+        double s = 0.0;
+        for (int k = 0; k < nseg; ++k)
+            s += static_cast<double>(a.part[(2 * k) * a.n_pad + i]) + static_cast<double>(a.part[(2 * k + 1) * a.n_pad + i]);
+        rho = static_cast<float>(s * static_cast<double>(p.w_pref));
+    } else {
+        float s = 0.0f;
+        for (int k = 0; k < nseg; ++k) s += a.part[k * a.n_pad + i];
+        rho = s * p.w_pref;
+    }
+    if (has(p, GSPH_DEAL_WITH_NO_PARTNERS) && rho < 0.001f) rho = p.rho0 * 0.01f;
+    float4 vr = a.velrho[i];
+    vr.w = rho;
+    a.velrho[i] = vr;
+    float4 jA, jB;
+    make_jrecord(p, rho, a.sA[i], a.sB[i], a.balsara[i], jA, jB);
+    a.jA[i] = jA;
+    a.jB[i] = jB;
+}
+
+// j-records from the current density (INTEGRATE_DENSITY: no density pass precedes the pairs)
+__global__ void k_prepare(DevArrays a, DevParams p) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    float4 jA, jB;
+    make_jrecord(p, a.velrho[i].w, a.sA[i], a.sB[i], a.balsara[i], jA, jB);
+    a.jA[i] = jA;
+    a.jB[i] = jB;
+}
+
+// ================================================================================================
+// SPH pair passes
+// ================================================================================================
+struct PairAcc {
+    float f[F_COUNT];
+};
+
+// GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: the self pair must contribute 0)
+template <int PASS, int GRAV, bool SOLIDS, bool COMP>
+__global__ void __launch_bounds__(128) k_pairs(DevArrays a, DevParams p, int jt, int nseg) {
+    constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
+    constexpr int K = popc_c(MASK);
+    constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
+    constexpr bool DO_V = PASS != PASS_ACC;
+    constexpr bool DO_A = PASS != PASS_VGRAD;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    JTilePipe<NS> pipe;
+    pipe.buf = reinterpret_cast<float4*>(smem_raw);
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * NS * jt * sizeof(float4));
+    pipe.src[0] = a.posm;
+    pipe.src[1] = a.velrho;
+    if constexpr (NS == 4) {
+        pipe.src[2] = a.jA;
+        pipe.src[3] = a.jB;
+    }
+    pipe.jt = jt;
+    pipe.status = a.status;
+    segment_tiles(a.n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const float4 pi = a.posm[i];
+    const float4 vi = a.velrho[i];
+    float4 jAi = make_float4(0, 0, 0, 0), jBi = make_float4(0, 0, 0, 0);
+    if (DO_A) {
+        jAi = a.jA[i];
+        jBi = a.jB[i];
+    }
+    const bool bals = has(p, GSPH_BALSARA_SWITCH);
+    const bool av = has(p, GSPH_ARTIFICIAL_VISCOSITY);
+    const bool xsph = has(p, GSPH_XSPH);
+    const bool arts = has(p, GSPH_ARTIFICIAL_STRESS);
+    const bool curl = !SOLIDS && bals;
+    const bool divv_on = bals || has(p, GSPH_INTEGRATE_DENSITY);
+    const float bi = bals ? jBi.z : 1.0f;
+    // artificial stress of i (computeDerivatives.h:210-217)
+    const float ai_xx = art(p.mateps, jAi.x), ai_yy = art(p.mateps, jAi.y), ai_zz = art(p.mateps, jAi.z),
+                ai_xy = art(p.mateps, jAi.w), ai_xz = art(p.mateps, jBi.x), ai_yz = art(p.mateps, jBi.y);
+
+    // neighbour window on r2 (+eps^2 when gravity shares the squared distance)
+    const float eps2 = (GRAV == 1) ? p.eps2 : 0.0f;
+    const uint32_t lo = __float_as_uint(eps2);
+    const uint32_t span = __float_as_uint(p.H2 + eps2) - lo;
+
+    PairAcc S, C;
+#pragma unroll
+    for (int f = 0; f < F_COUNT; ++f) {
+        S.f[f] = 0.0f;
+        C.f[f] = 0.0f;
+    }
+    float maxv = 0.0f;
+
+    pipe.start();
+    pipe.run([&](const float4* stage) {
+        const float4* P = stage;
+        const float4* V = stage + jt;
+        const float4* JA = stage + 2 * jt;
+        const float4* JB = stage + 3 * jt;
+        PairAcc T;
+#pragma unroll
+        for (int f = 0; f < F_COUNT; ++f) T.f[f] = 0.0f;
+#pragma unroll 4
+        for (int j = 0; j < jt; ++j) {
+            const float4 q = P[j];
+            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;  // d = x_j - x_i = -r_ij
+            const float r2e = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+            if (GRAV != 0) {  // computeDerivatives.h:229-235 (G applied by the finish kernel)
+                float inv = rsqrtf(r2e);
+                if (GRAV == 2) inv = fminf(inv, 1e12f);
+                const float s = q.w * inv * (inv * inv);
+                T.f[F_GX] = fmaf(dx, s, T.f[F_GX]);
+                T.f[F_GY] = fmaf(dy, s, T.f[F_GY]);
+                T.f[F_GZ] = fmaf(dz, s, T.f[F_GZ]);
+            }
+            if (in_open_closed(r2e, lo, span)) {  // 0 < r2 <= H2
+                const float r2 = r2e - eps2;
+                const float inv_r = rsqrtf(r2);
+                const float r = r2 * inv_r;
+                const float qq = r * p.inv_h;
+                const float gf = -p.dw_pref * dw_poly(qq) * inv_r;  // gradW = -gf * r_ij... see below
+                // grad_i W = (dW/r) r_ij with r_ij = -d:  g = -(dW/r) d
+                const float gx = gf * dx, gy = gf * dy, gz = gf * dz;
+                const float4 vj = V[j];
+                const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;  // v_ij
+                const float mj = q.w, rhoj = vj.w;
+                if (DO_V) {  // calcBalsaraDensityDTDStressDT pair body (:118-141)
+                    const float mr = mj / rhoj;
+                    if (SOLIDS) {  // addStrainRateAndRotationRate (models.h:225-248)
+                        const float t = -0.5f * mr;
+                        T.f[F_E00] = fmaf(t, vx * gx + vx * gx, T.f[F_E00]);
+                        T.f[F_E11] = fmaf(t, vy * gy + vy * gy, T.f[F_E11]);
+                        T.f[F_E22] = fmaf(t, vz * gz + vz * gz, T.f[F_E22]);
+                        T.f[F_E01] = fmaf(t, vx * gy + vy * gx, T.f[F_E01]);
+                        T.f[F_E02] = fmaf(t, vx * gz + vz * gx, T.f[F_E02]);
+                        T.f[F_E12] = fmaf(t, vy * gz + vz * gy, T.f[F_E12]);
+                        T.f[F_W01] = fmaf(t, vx * gy - vy * gx, T.f[F_W01]);
+                        T.f[F_W02] = fmaf(t, vx * gz - vz * gx, T.f[F_W02]);
+                        T.f[F_W12] = fmaf(t, vy * gz - vz * gy, T.f[F_W12]);
+                    } else if (curl) {
+                        T.f[F_C0] = fmaf(mr, vy * gz - vz * gy, T.f[F_C0]);
+                        T.f[F_C1] = fmaf(mr, vz * gx - vx * gz, T.f[F_C1]);
+                        T.f[F_C2] = fmaf(mr, vx * gy - vy * gx, T.f[F_C2]);
+                    }
+                    if (divv_on) T.f[F_DIVV] = fmaf(-mr, vx * gx + vy * gy + vz * gz, T.f[F_DIVV]);
+                }
+                if (DO_A) {  // calcAcceleration SPH body (:237-295)
+                    const float4 ja = JA[j];
+                    const float4 jb = JB[j];
+                    float sxx = jAi.x + ja.x, syy = jAi.y + ja.y, szz = jAi.z + ja.z;
+                    float sxy = jAi.w + ja.w, sxz = jBi.x + jb.x, syz = jBi.y + jb.y;
+                    if (arts) {
+                        const float f = powf(p.w_pref * w_poly(qq) * p.inv_w_normalsep, p.matexp);
+                        sxx += f * (ai_xx + art(p.mateps, ja.x));
+                        syy += f * (ai_yy + art(p.mateps, ja.y));
+                        szz += f * (ai_zz + art(p.mateps, ja.z));
+                        sxy += f * (ai_xy + art(p.mateps, ja.w));
+                        sxz += f * (ai_xz + art(p.mateps, jb.x));
+                        syz += f * (ai_yz + art(p.mateps, jb.y));
+                    }
+                    T.f[F_AX] = fmaf(mj, sxx * gx + sxy * gy + sxz * gz, T.f[F_AX]);
+                    T.f[F_AY] = fmaf(mj, sxy * gx + syy * gy + syz * gz, T.f[F_AY]);
+                    T.f[F_AZ] = fmaf(mj, sxz * gx + syz * gy + szz * gz, T.f[F_AZ]);
+                    if (av) {  // artificialViscosity (models.h:158-185)
+                        const float w = -(dx * vx + dy * vy + dz * vz) * inv_r;  // r_ij . v_ij / r
+                        if (w < 0.0f) {
+                            const float vsig = p.c + p.c - p.beta * w;
+                            const float rhoij = (vi.w + rhoj) * 0.5f;
+                            const float bj = bals ? jb.z : 1.0f;
+                            const float II = -0.25f * (bi + bj) * p.alpha * w * vsig / rhoij;
+                            const float m2 = -mj * II;
+                            T.f[F_AX] = fmaf(m2, gx, T.f[F_AX]);
+                            T.f[F_AY] = fmaf(m2, gy, T.f[F_AY]);
+                            T.f[F_AZ] = fmaf(m2, gz, T.f[F_AZ]);
+                            if (bals) maxv = fmaxf(maxv, vsig);
+                        }
+                    }
+                    if (xsph) {
+                        const float f = 2.0f * mj / (vi.w + rhoj) * (p.w_pref * w_poly(qq));
+                        T.f[F_XV0] = fmaf(f, -vx, T.f[F_XV0]);
+                        T.f[F_XV1] = fmaf(f, -vy, T.f[F_XV1]);
+                        T.f[F_XV2] = fmaf(f, -vz, T.f[F_XV2]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < F_COUNT; ++f) {
+            if (!((MASK >> f) & 1u) || f == F_MAXV) continue;
+            if (COMP) fold(S.f[f], C.f[f], T.f[f]);
+            else S.f[f] += T.f[f];
+        }
+    });
+
+    const int64_t seg = blockIdx.y;
+    float* out = a.part + seg * static_cast<int64_t>(COMP ? 2 * K : K) * a.n_pad + i;
+#pragma unroll
+    for (int f = 0; f < F_COUNT; ++f) {
+        if (!((MASK >> f) & 1u)) continue;
+        const int o = field_offset<MASK>(f);
+        out[o * a.n_pad] = (f == F_MAXV) ? maxv : S.f[f];
+        if (COMP) out[(K + o) * a.n_pad] = (f == F_MAXV) ? 0.0f : C.f[f];
+    }
+}
+
+// Sum the segments of one field (fixed order): FP32 in plain mode, FP64 of (sum + error) in
+// compensated mode. The max signal velocity is a max over segments.
+template <uint32_t MASK, bool COMP>
+__device__ __forceinline__ float seg_sum(const DevArrays& a, int nseg, int64_t i, int f) {
+    constexpr int K = popc_c(MASK);
+    const int o = field_offset<MASK>(f);
+    const int64_t stride = static_cast<int64_t>(COMP ? 2 * K : K) * a.n_pad;
+    if (f == F_MAXV) {
+        float m = 0.0f;
+        for (int k = 0; k < nseg; ++k) m = fmaxf(m, a.part[k * stride + o * a.n_pad + i]);
+        return m;
+    }
+    if (COMP) {
+        double s = 0.0;
+        for (int k = 0; k < nseg; ++k)
+            s += static_cast<double>(a.part[k * stride + o * a.n_pad + i]) +
+                 static_cast<double>(a.part[k * stride + (K + o) * a.n_pad + i]);
+        return static_cast<float>(s);
+    }
+    float s = 0.0f;
+    for (int k = 0; k < nseg; ++k) s += a.part[k * stride + o * a.n_pad + i];
+    return s;
+}
+
+// environmentAcceleration (computeDerivatives.h:33-47); the Clohessy-Wiltshire terms are scalars
+// added to all three components, as the reference's f3_t += f1_t does
+__device__ __forceinline__ void environment(const DevParams& p, float4 x, float4 v, float& ax, float& ay, float& az) {
+    if (has(p, GSPH_CLOHESSY_WILTSHIRE)) {
+        const float n = p.cw_n;
+        const float s1 = 3 * n * n * x.x + 2 * n * v.y;
+        ax += s1; ay += s1; az += s1;
+        const float s2 = -2 * n * v.x;
+        ax += s2; ay += s2; az += s2;
+        const float s3 = -n * n * x.z;
+        ax += s3; ay += s3; az += s3;
+    }
+    if (has(p, GSPH_CONSTANT_ACCELERATION)) {
+        ax += p.const_acc[0];
+        ay += p.const_acc[1];
+        az += p.const_acc[2];
+    }
+}
+
+template <int PASS, bool GRAV, bool SOLIDS, bool COMP>
+__global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg) {
+    constexpr uint32_t MASK = field_mask<PASS, GRAV, SOLIDS>();
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (PASS != PASS_VGRAD && has(p, GSPH_VARIABLE_TIMESTEP) && i == 0)
+        a.dt_state[1] = p.max_dt;  // nextTS reset of calcAcceleration::do_after (:306-309)
+    if (i >= a.n) return;
+    const float4 vi = a.velrho[i];
+    if (PASS != PASS_ACC) {  // calcBalsaraDensityDTDStressDT::do_after (:144-161)
+        const float divv = seg_sum<MASK, COMP>(a, nseg, i, F_DIVV);
+        float c0 = 0, c1 = 0, c2 = 0;
+        if (SOLIDS) {
+            const float e[6] = {seg_sum<MASK, COMP>(a, nseg, i, F_E00), seg_sum<MASK, COMP>(a, nseg, i, F_E11),
+                                seg_sum<MASK, COMP>(a, nseg, i, F_E22), seg_sum<MASK, COMP>(a, nseg, i, F_E01),
+                                seg_sum<MASK, COMP>(a, nseg, i, F_E02), seg_sum<MASK, COMP>(a, nseg, i, F_E12)};
+            const float w01 = seg_sum<MASK, COMP>(a, nseg, i, F_W01), w02 = seg_sum<MASK, COMP>(a, nseg, i, F_W02),
+                        w12 = seg_sum<MASK, COMP>(a, nseg, i, F_W12);
+            const float E[3][3] = {{e[0], e[3], e[4]}, {e[3], e[1], e[5]}, {e[4], e[5], e[2]}};
+            const float R[3][3] = {{0.0f, w01, w02}, {-w01, 0.0f, w12}, {-w02, -w12, 0.0f}};
+            const float4 sa = a.sA[i], sb = a.sB[i];
+            const float Sm[3][3] = {{sa.x, sa.w, sb.x}, {sa.w, sa.y, sb.y}, {sb.x, sb.y, sa.z}};
+            const float tr = E[0][0] + E[1][1] + E[2][2];
+            float D[3][3];
+            // dstress_dt (models.h:250-268): Hooke deviatoric rate + Jaumann rotation terms
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+#pragma unroll
+                for (int ee = 0; ee < 3; ++ee) {
+                    float v = 2.0f * p.shear * E[d][ee];
+                    if (d == ee) v -= 2.0f * p.shear * tr / 3.0f;
+#pragma unroll
+                    for (int f = 0; f < 3; ++f) v += Sm[d][f] * R[ee][f] + Sm[ee][f] * R[d][f];
+                    D[d][ee] = v;
+                }
+            a.dA[i] = make_float4(D[0][0], D[1][1], D[2][2], 0.5f * (D[0][1] + D[1][0]));
+            a.dB[i] = make_float4(0.5f * (D[0][2] + D[2][0]), 0.5f * (D[1][2] + D[2][1]), 0.0f, 0.0f);
+            c0 = -2.0f * R[1][2];
+            c1 = -2.0f * R[2][0];
+            c2 = -2.0f * R[0][1];
+        } else {
+            c0 = seg_sum<MASK, COMP>(a, nseg, i, F_C0);
+            c1 = seg_sum<MASK, COMP>(a, nseg, i, F_C1);
+            c2 = seg_sum<MASK, COMP>(a, nseg, i, F_C2);
+        }
+        a.rhodot[i] = has(p, GSPH_INTEGRATE_DENSITY) ? -vi.w * divv : 0.0f;
+        float bal = 0.0f;
+        if (has(p, GSPH_BALSARA_SWITCH)) {  // balsaraSwitch (models.h:187-192)
+            const float absdiv = fabsf(divv);
+            const float abscurl = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+            bal = absdiv / (absdiv + abscurl + p.balsara_floor);
+            float4 jb = a.jB[i];
+            jb.z = bal;
+            a.jB[i] = jb;
+        }
+        a.balsara[i] = bal;
+    }
+    if (PASS != PASS_VGRAD) {  // calcAcceleration::do_after (:301-312)
+        float ax = seg_sum<MASK, COMP>(a, nseg, i, F_AX);
+        float ay = seg_sum<MASK, COMP>(a, nseg, i, F_AY);
+        float az = seg_sum<MASK, COMP>(a, nseg, i, F_AZ);
+        if (GRAV) {
+            ax = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GX), ax);
+            ay = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GY), ay);
+            az = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GZ), az);
+        }
+        const float4 x = a.posm[i];
+        environment(p, x, vi, ax, ay, az);
+        a.acc[i] = make_float4(ax, ay, az, seg_sum<MASK, COMP>(a, nseg, i, F_MAXV));
+        a.xvel[i] = make_float4(seg_sum<MASK, COMP>(a, nseg, i, F_XV0), seg_sum<MASK, COMP>(a, nseg, i, F_XV1),
+                                seg_sum<MASK, COMP>(a, nseg, i, F_XV2), 0.0f);
+    }
+}
+
+// ================================================================================================
+// pure gravity (ENABLE_SPH off): I i-particles per thread share every j read from shared memory
+// ================================================================================================
+template <int I, int GRAV, bool COMP>
+__global__ void __launch_bounds__(128) k_gravity(const float4* __restrict__ posm, float* __restrict__ part,
+                                                  int64_t n_pad, int jt, int nseg, float eps2, int* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    JTilePipe<1> pipe;
+    pipe.buf = reinterpret_cast<float4*>(smem_raw);
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * jt * sizeof(float4));
+    pipe.src[0] = posm;
+    pipe.jt = jt;
+    pipe.status = status;
+    segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x * I + threadIdx.x;
+    float xi[I], yi[I], zi[I], ax[I], ay[I], az[I], cx[I], cy[I], cz[I];
+#pragma unroll
+    for (int k = 0; k < I; ++k) {
+        const float4 q = posm[base + static_cast<int64_t>(k) * blockDim.x];
+        xi[k] = q.x; yi[k] = q.y; zi[k] = q.z;
+        ax[k] = ay[k] = az[k] = 0.0f;
+        cx[k] = cy[k] = cz[k] = 0.0f;
+    }
+
+    pipe.start();
+    pipe.run([&](const float4* J) {
+        float tx[I], ty[I], tz[I];
+#pragma unroll
+        for (int k = 0; k < I; ++k) tx[k] = ty[k] = tz[k] = 0.0f;
+#pragma unroll 4
+        for (int j = 0; j < jt; ++j) {
+            const float4 q = J[j];
+#pragma unroll
+            for (int k = 0; k < I; ++k) {
+                const float dx = q.x - xi[k], dy = q.y - yi[k], dz = q.z - zi[k];
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+                float inv = rsqrtf(r2);
+                if (GRAV == 2) inv = fminf(inv, 1e12f);
+                const float s = q.w * inv * (inv * inv);
+                if (COMP) {
+                    tx[k] = fmaf(dx, s, tx[k]);
+                    ty[k] = fmaf(dy, s, ty[k]);
+                    tz[k] = fmaf(dz, s, tz[k]);
+                } else {
+                    ax[k] = fmaf(dx, s, ax[k]);
+                    ay[k] = fmaf(dy, s, ay[k]);
+                    az[k] = fmaf(dz, s, az[k]);
+                }
+            }
+        }
+        if (COMP) {
+#pragma unroll
+            for (int k = 0; k < I; ++k) {
+                fold(ax[k], cx[k], tx[k]);
+                fold(ay[k], cy[k], ty[k]);
+                fold(az[k], cz[k], tz[k]);
+            }
+        }
+    });
+
+    const int64_t seg = blockIdx.y;
+    const int K = COMP ? 6 : 3;
+#pragma unroll
+    for (int k = 0; k < I; ++k) {
+        float* out = part + seg * K * n_pad + base + static_cast<int64_t>(k) * blockDim.x;
+        out[0] = ax[k];
+        out[n_pad] = ay[k];
+        out[2 * n_pad] = az[k];
+        if (COMP) {
+            out[3 * n_pad] = cx[k];
+            out[4 * n_pad] = cy[k];
+            out[5 * n_pad] = cz[k];
+        }
+    }
+}
+
+template <bool COMP>
+__global__ void k_gravity_finish(DevArrays a, DevParams p, int nseg) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (has(p, GSPH_VARIABLE_TIMESTEP) && i == 0) a.dt_state[1] = p.max_dt;
+    if (i >= a.n) return;
+    const int K = COMP ? 6 : 3;
+    float acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (COMP) {
+            double s = 0.0;
+            for (int k = 0; k < nseg; ++k)
+                s += static_cast<double>(a.part[(k * K + c) * a.n_pad + i]) +
+                     static_cast<double>(a.part[(k * K + 3 + c) * a.n_pad + i]);
+            acc[c] = static_cast<float>(s * static_cast<double>(p.G));
+        } else {
+            float s = 0.0f;
+            for (int k = 0; k < nseg; ++k) s += a.part[(k * K + c) * a.n_pad + i];
+            acc[c] = p.G * s;
+        }
+    }
+    environment(p, a.posm[i], a.velrho[i], acc[0], acc[1], acc[2]);
+    a.acc[i] = make_float4(acc[0], acc[1], acc[2], 0.0f);
+    a.xvel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+inline unsigned blocks_for(int64_t n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
+
+}  // namespace
+
+// ---- host launchers ----------------------------------------------------------------------------
+// Event record that also works while `s` is being captured into a graph (as an event-record node).
+cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &st);
+    if (e != cudaSuccess) return e;
+    if (st == cudaStreamCaptureStatusActive) return cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
+    return cudaEventRecord(ev, s);
+}
+
+#define GSPH_TIMER_MARK(t, which)                          \
+    do {                                                   \
+        if (t) {                                           \
+            cudaError_t te_ = timer_record((t)->which, s); \
+            if (te_ != cudaSuccess) return te_;            \
+        }                                                  \
+    } while (0)
+
+cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+    const int T = 256;
+    const dim3 grid(static_cast<unsigned>(a.n_pad / T), static_cast<unsigned>(L.nseg));
+    const size_t smem = pipe_smem_bytes(1, L.jt);
+    GSPH_TIMER_MARK(t, start);
+    if (L.accum == GSPH_ACCUM_COMPENSATED)
+        k_density<true><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status);
+    else
+        k_density<false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    GSPH_TIMER_MARK(t, stop);
+    if (L.accum == GSPH_ACCUM_COMPENSATED)
+        k_density_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg);
+    else
+        k_density_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s) {
+    k_prepare<<<blocks_for(a.n, 256), 256, 0, s>>>(a, p);
+    return cudaGetLastError();
+}
+
+namespace {
+template <int PASS, int GRAV, bool SOLIDS, bool COMP>
+cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+    constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
+    const size_t smem = pipe_smem_bytes(NS, L.jt);
+    auto kern = k_pairs<PASS, GRAV, SOLIDS, COMP>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    const dim3 grid(static_cast<unsigned>(a.n_pad / L.threads), static_cast<unsigned>(L.nseg));
+    GSPH_TIMER_MARK(t, start);
+    kern<<<grid, L.threads, smem, s>>>(a, p, L.jt, L.nseg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    GSPH_TIMER_MARK(t, stop);
+    k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg);
+    return cudaGetLastError();
+}
+
+template <int PASS, int GRAV>
+cudaError_t pairs_g(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+    const bool solids = has(p, GSPH_SOLIDS);
+    const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
+    if (solids)
+        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t) : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t);
+    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t) : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t);
+}
+}  // namespace
+
+cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                         const KTimer* t) {
+    const int grav = !has(p, GSPH_SELF_GRAVITY) ? 0 : (p.eps2 > 0.0f ? 1 : 2);
+    switch (pass) {
+        case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t);
+        case PASS_ACC:
+            return grav == 0 ? pairs_g<PASS_ACC, 0>(a, p, L, s, t)
+                             : (grav == 1 ? pairs_g<PASS_ACC, 1>(a, p, L, s, t) : pairs_g<PASS_ACC, 2>(a, p, L, s, t));
+        default:
+            return grav == 0 ? pairs_g<PASS_FUSED, 0>(a, p, L, s, t)
+                             : (grav == 1 ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t)
+                                          : pairs_g<PASS_FUSED, 2>(a, p, L, s, t));
+    }
+}
+
+namespace {
+template <int I, int GRAV, bool COMP>
+cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+    const int T = L.grav_threads;
+    const dim3 grid(static_cast<unsigned>(a.n_pad / (static_cast<int64_t>(T) * I)), static_cast<unsigned>(L.grav_nseg));
+    const size_t smem = pipe_smem_bytes(1, L.jt);
+    GSPH_TIMER_MARK(t, start);
+    k_gravity<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.grav_nseg, p.eps2, a.status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    GSPH_TIMER_MARK(t, stop);
+    k_gravity_finish<COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.grav_nseg);
+    return cudaGetLastError();
+}
+template <int GRAV, bool COMP>
+cudaError_t gravity_i(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+    switch (L.grav_ipt) {
+        case 1: return gravity_t<1, GRAV, COMP>(a, p, L, s, t);
+        case 2: return gravity_t<2, GRAV, COMP>(a, p, L, s, t);
+        case 8: return gravity_t<8, GRAV, COMP>(a, p, L, s, t);
+        default: return gravity_t<4, GRAV, COMP>(a, p, L, s, t);
+    }
+}
+}  // namespace
+
+cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+    const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
+    if (!has(p, GSPH_SELF_GRAVITY)) {  // neither gravity nor SPH: environment terms only
+        if (comp) k_gravity_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 0);
+        else k_gravity_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 0);
+        return cudaGetLastError();
+    }
+    if (p.eps2 > 0.0f) return comp ? gravity_i<1, true>(a, p, L, s, t) : gravity_i<1, false>(a, p, L, s, t);
+    return comp ? gravity_i<2, true>(a, p, L, s, t) : gravity_i<2, false>(a, p, L, s, t);
+}
+
+// ---- FP32 FFMA throughput probe (roofline denominator) -------------------------------------------
+namespace {
+constexpr int kPeakThreads = 256;
+constexpr int kPeakBlocksPerSM = 4;
+constexpr int kPeakChains = 16;
+constexpr int kPeakUnroll = 16;
+__global__ void __launch_bounds__(kPeakThreads) k_fp32_peak(float* sink, int iters) {
+    float x[kPeakChains];
+#pragma unroll
+    for (int c = 0; c < kPeakChains; ++c) x[c] = static_cast<float>(threadIdx.x + c) * 1e-3f;
+    const float a = 0.999999f, b = 1e-7f;
+    for (int k = 0; k < iters; ++k) {
+#pragma unroll
+        for (int u = 0; u < kPeakUnroll; ++u)
+#pragma unroll
+            for (int c = 0; c < kPeakChains; ++c) x[c] = fmaf(x[c], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kPeakChains; ++c) s += x[c];
+    if (s == -1.0f) sink[blockIdx.x] = s;  // never true; keeps the chains live
+}
+}  // namespace
+
+cudaError_t launch_fp32_peak(int sm_count, int iters, float* sink, cudaStream_t s) {
+    k_fp32_peak<<<sm_count * kPeakBlocksPerSM, kPeakThreads, 0, s>>>(sink, iters);
+    return cudaGetLastError();
+}
+
+int64_t fp32_peak_flops(int sm_count, int iters) {
+    return static_cast<int64_t>(sm_count) * kPeakBlocksPerSM * kPeakThreads * static_cast<int64_t>(iters) *
+           kPeakUnroll * kPeakChains * 2;
+}
+
+size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad) {
+    const int mult = (L.accum == GSPH_ACCUM_COMPENSATED) ? 2 : 1;
+    size_t k = 0;
+    if (has(p, GSPH_SPH)) {
+        const size_t kd = 1;
+        const size_t kp = static_cast<size_t>(popc_c(field_mask<PASS_FUSED, true, true>()));
+        k = std::max(kd, kp);
+        k = std::max<size_t>(k, static_cast<size_t>(popc_c(field_mask<PASS_FUSED, true, false>())));
+        k *= static_cast<size_t>(std::max(L.nseg, 1));
+    } else {
+        k = 3 * static_cast<size_t>(std::max(L.grav_nseg, 1));
+    }
+    return k * mult * static_cast<size_t>(n_pad);
+}
+
+int kernels_per_derivatives(const DevParams& p) {
+    if (!has(p, GSPH_SPH)) return 2;
+    int k = 0;
+    if (!has(p, GSPH_INTEGRATE_DENSITY)) k += 2;
+    else k += 1;  // prepare
+    const bool vgrad = has(p, GSPH_SOLIDS) || has(p, GSPH_INTEGRATE_DENSITY) || has(p, GSPH_BALSARA_SWITCH);
+    if (vgrad && has(p, GSPH_BALSARA_SWITCH)) k += 4;
+    else k += 2;
+    return k;
+}
+
+}  // namespace gsph

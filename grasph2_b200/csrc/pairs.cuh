@@ -1,0 +1,164 @@
+// pairs.cuh -- the all-pairs j-tile engine shared by the density, velocity-gradient, acceleration
+// and gravity kernels.
+//
+// Replaces the reference's tile loop detail::do_for_each_pair_fast_impl
+// (src/particles/algorithms.h:270-309) with:
+//   * a 2-D grid: blockIdx.x = block of i-particles, blockIdx.y = segment of j-tiles (j-split),
+//     so small N still fills 148 SMs and large N has no tail wave; each (i-block, segment)
+//     writes its partial sums, which a finish kernel adds up in a fixed order (deterministic);
+//   * j-tiles of `jt` particles staged in shared memory by 1-D bulk copies (cp.async.bulk, no
+//     multicast), double-buffered against the i-loop and completed on mbarriers;
+//   * arrays padded to a multiple of kPad with inert particles (zero mass, far away), so every tile
+//     is full and the reference's remainder-tile bug (algorithms.h:285-301) cannot arise.
+#pragma once
+
+#include "common.cuh"
+
+namespace gsph {
+
+// Two-stage pipeline over the j-tiles [t_begin, t_end) of up to 4 float4 streams.
+template <int NS>
+struct JTilePipe {
+    float4* buf;          // shared: [2][NS][jt]
+    uint64_t* bar;        // shared: [2]
+    const float4* src[NS];
+    int jt;
+    int64_t t_begin, t_end;
+    int* status;
+
+    __device__ __forceinline__ void issue(int b, int64_t t) {
+        mbar_expect_tx(&bar[b], static_cast<uint32_t>(NS * jt * sizeof(float4)));
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+            bulk_g2s(buf + (static_cast<int64_t>(b) * NS + s) * jt, src[s] + t * jt,
+                     static_cast<uint32_t>(jt * sizeof(float4)), &bar[b]);
+    }
+
+    // init barriers and start the first two tiles; all threads must call it
+    __device__ __forceinline__ void start() {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+            fence_barrier_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (t_begin < t_end) issue(0, t_begin);
+            if (t_begin + 1 < t_end) issue(1, t_begin + 1);
+        }
+    }
+
+    // for each tile: wait for it, run body(stage pointers), release the buffer and refill it
+    template <typename Body>
+    __device__ __forceinline__ void run(Body&& body) {
+        int k = 0;
+        for (int64_t t = t_begin; t < t_end; ++t, ++k) {
+            const int b = k & 1;
+            const bool ok = mbar_wait_bounded(&bar[b], static_cast<uint32_t>((k >> 1) & 1), status);
+            if (__syncthreads_or(!ok)) {
+                drain(k);
+                return;
+            }
+            const float4* stage = buf + static_cast<int64_t>(b) * NS * jt;
+            body(stage);
+            __syncthreads();
+            if (threadIdx.x == 0 && t + 2 < t_end) issue(b, t + 2);
+        }
+    }
+
+    // after a timed-out wait: give copies still in flight a bounded time to land before exit
+    __device__ __forceinline__ void drain(int k) {
+        if (threadIdx.x == 0) {
+            for (int extra = 0; extra < 2; ++extra) {
+                const int kk = k + extra;
+                const int64_t t = t_begin + kk;
+                if (t >= t_end) break;
+                mbar_wait_bounded(&bar[kk & 1], static_cast<uint32_t>((kk >> 1) & 1), status);
+            }
+        }
+        __syncthreads();
+    }
+};
+
+// shared-memory bytes of a pipeline: 2 stages of NS streams plus the two barriers
+__host__ __device__ inline size_t pipe_smem_bytes(int ns, int jt) {
+    return static_cast<size_t>(2) * ns * jt * sizeof(float4) + 2 * sizeof(uint64_t);
+}
+
+// tile range of segment `seg` out of `nseg` over `ntiles` tiles (balanced to within one tile)
+__device__ __forceinline__ void segment_tiles(int64_t ntiles, int seg, int nseg, int64_t& t0, int64_t& t1) {
+    t0 = ntiles * seg / nseg;
+    t1 = ntiles * (seg + 1) / nseg;
+}
+
+// ---- partial-sum fields of the SPH pair passes -----------------------------------------------
+enum Field : int {
+    F_GX = 0, F_GY, F_GZ,                    // gravity (G applied in the finish kernel)
+    F_AX, F_AY, F_AZ,                        // stress + AV acceleration
+    F_XV0, F_XV1, F_XV2,                     // XSPH
+    F_E00, F_E11, F_E22, F_E01, F_E02, F_E12,  // strain rate (symmetric)
+    F_W01, F_W02, F_W12,                     // rotation rate (antisymmetric)
+    F_DIVV,                                  // velocity divergence
+    F_C0, F_C1, F_C2,                        // velocity curl (fluid + Balsara)
+    F_MAXV,                                  // max signal velocity (a max, not a sum)
+    F_COUNT
+};
+
+enum Pass : int { PASS_VGRAD = 0, PASS_ACC = 1, PASS_FUSED = 2 };
+
+template <int PASS, bool GRAV, bool SOLIDS>
+__host__ __device__ constexpr uint32_t field_mask() {
+    uint32_t m = 0;
+    if (PASS != PASS_VGRAD) {
+        m |= (1u << F_AX) | (1u << F_AY) | (1u << F_AZ) | (1u << F_XV0) | (1u << F_XV1) | (1u << F_XV2) |
+             (1u << F_MAXV);
+        if (GRAV) m |= (1u << F_GX) | (1u << F_GY) | (1u << F_GZ);
+    }
+    if (PASS != PASS_ACC) {
+        m |= (1u << F_DIVV);
+        if (SOLIDS)
+            m |= (1u << F_E00) | (1u << F_E11) | (1u << F_E22) | (1u << F_E01) | (1u << F_E02) | (1u << F_E12) |
+                 (1u << F_W01) | (1u << F_W02) | (1u << F_W12);
+        else
+            m |= (1u << F_C0) | (1u << F_C1) | (1u << F_C2);
+    }
+    return m;
+}
+
+__host__ __device__ constexpr int popc_c(uint32_t x) { return x == 0 ? 0 : int(x & 1u) + popc_c(x >> 1); }
+
+template <uint32_t MASK>
+__host__ __device__ constexpr int field_offset(int f) {
+    return popc_c(MASK & ((1u << f) - 1u));
+}
+
+// Optional event pair bracketing one pair-kernel launch (per-kernel timing, graph-capturable).
+struct KTimer {
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s);
+
+// host launchers (pairs.cu)
+struct Launch {
+    int threads;     // threads per CTA of the SPH pair kernels
+    int jt;          // j-tile
+    int nseg;        // j-split of the SPH pair kernels
+    int grav_threads;
+    int grav_ipt;    // i per thread of the gravity kernel
+    int grav_nseg;
+    int accum;       // GSPH_ACCUM_*
+};
+
+cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                           const KTimer* t = nullptr);
+cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s);
+cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                         const KTimer* t = nullptr);
+cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                           const KTimer* t = nullptr);
+cudaError_t launch_fp32_peak(int sm_count, int iters, float* sink, cudaStream_t s);
+int64_t fp32_peak_flops(int sm_count, int iters);
+size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad);
+int kernels_per_derivatives(const DevParams& p);
+
+}  // namespace gsph

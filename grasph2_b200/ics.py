@@ -1,0 +1,104 @@
+"""Seeded initial conditions for the named workloads.
+
+The reference draws its spheres with mpUtils' random point pickers (UniformSphere.cu:39,
+PlummerSphere.cu:39-88, not vendored); these generators produce the same distributions from
+numpy's PCG64 so that the CUDA path and the oracle receive identical arrays:
+
+* uniform sphere: radius R*U^(1/3), isotropic direction, equal masses, density = rest density
+  (src/initialConditions/particleSources/UniformSphere.cu:35-44), optional rigid rotation
+  v = omega x r (ParticleSource::addAngularVelocity);
+* Plummer sphere: r = a (U^(-2/3) - 1)^(-1/2) (PlummerSphere.cu:41-51, no cutoff), speeds from
+  the von Neumann rejection of g(q) = q^2 (1-q^2)^(7/2) with v = q sqrt(2GM / sqrt(r^2+a^2))
+  (PlummerSphere.cu:60-88);
+* centre-of-mass and centre-of-mass-velocity correction (InitGenerator.h:113-152).
+"""
+
+import math
+
+import numpy as np
+
+from .state import new_state
+
+
+def _isotropic(rng, n):
+    z = rng.uniform(-1.0, 1.0, n)
+    phi = rng.uniform(0.0, 2.0 * math.pi, n)
+    s = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    return np.stack([s * np.cos(phi), s * np.sin(phi), z], axis=1)
+
+
+def uniform_sphere_positions(rng, n, radius):
+    r = radius * rng.uniform(0.0, 1.0, n) ** (1.0 / 3.0)
+    return _isotropic(rng, n) * r[:, None]
+
+
+def _com_correct(state):
+    m = state["mass"].astype(np.float64)
+    for key in ("pos", "vel"):
+        a = state[key].astype(np.float64)
+        c = (m[:, None] * a).sum(0) / m.sum()
+        state[key] = (a - c).astype(state[key].dtype)
+
+
+def uniform_sphere(n, radius=1.0, total_mass=1.0, rho0=1.0, omega=(0.0, 0.0, 0.0), seed=0, dtype=np.float64,
+                   com_correct=True):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    st = new_state(n, dtype)
+    x = uniform_sphere_positions(rng, n, radius)
+    st["pos"][:] = x
+    st["mass"][:] = total_mass / n
+    st["density"][:] = rho0
+    st["vel"][:] = np.cross(np.asarray(omega, dtype=np.float64)[None, :], x)
+    if com_correct:
+        _com_correct(st)
+    return st
+
+
+def two_sphere_impact(n_big=58254, n_small=7282, r_big=1.0, r_small=0.5, v_rel=0.5, y_offset=0.3, rho0=1.0,
+                      seed=0, dtype=np.float64):
+    """Two uniform spheres of equal number density: the big one at rest at the origin, the small
+    one touching its surface with centre offset y_offset in y and moving +x at v_rel; then the
+    centre-of-mass frame. Masses m = rho0 * V_total / N."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = n_big + n_small
+    st = new_state(n, dtype)
+    xb = uniform_sphere_positions(rng, n_big, r_big)
+    xs = uniform_sphere_positions(rng, n_small, r_small)
+    d = r_big + r_small
+    xs += np.array([-math.sqrt(d * d - y_offset * y_offset), y_offset, 0.0])
+    st["pos"][:n_big] = xb
+    st["pos"][n_big:] = xs
+    vol = 4.0 / 3.0 * math.pi * (r_big ** 3 + r_small ** 3)
+    st["mass"][:] = rho0 * vol / n
+    st["density"][:] = rho0
+    st["vel"][n_big:, 0] = v_rel
+    _com_correct(st)
+    return st
+
+
+def plummer_sphere(n, a=1.0, total_mass=1.0, G=1.0, seed=0, dtype=np.float64):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    st = new_state(n, dtype)
+    u = rng.uniform(0.0, 1.0, n)
+    u = np.clip(u, 1e-300, 1.0 - 1e-16)
+    r = a / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+    st["pos"][:] = _isotropic(rng, n) * r[:, None]
+    q = np.empty(n)
+    todo = np.arange(n)
+    while todo.size:
+        x = rng.uniform(0.0, 1.0, todo.size)
+        y = rng.uniform(0.0, 0.1, todo.size)
+        ok = y <= x * x * (1.0 - x * x) ** 3.5
+        q[todo[ok]] = x[ok]
+        todo = todo[~ok]
+    speed = q * np.sqrt(2.0 * G * total_mass / np.sqrt(r * r + a * a))
+    st["vel"][:] = _isotropic(rng, n) * speed[:, None]
+    st["mass"][:] = total_mass / n
+    _com_correct(st)
+    return st
+
+
+def ensemble_sizes(count=512, lo=1024, hi=32768, seed=0):
+    """Seeded log-uniform integer sizes in [lo, hi]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.floor(np.exp(rng.uniform(math.log(lo), math.log(hi + 1), count))).astype(np.int64).clip(lo, hi)

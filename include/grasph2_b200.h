@@ -1,0 +1,272 @@
+/*
+ * grasph2_b200.h -- C-ABI of the B200 (sm_100a) implementation of GraSPH2's per-step hot path:
+ * all-pairs self-gravity with Plummer softening, the SPH density sum, the stress/pressure
+ * acceleration with artificial viscosity, the Jaumann stress rate, the plasticity limiter and the
+ * leapfrog integrator.
+ *
+ * Plain C: fixed-width integers, plain pointers and sizes. No CUDA or C++ types appear in the
+ * signatures; a stream is passed as `void*` (a cudaStream_t, or NULL for the legacy default
+ * stream). Every entry point returns an int status: 0 on success, a negative GSPH_E_* code on
+ * failure. The text of the last failure on a context is available from gsph_last_error().
+ *
+ * Reference surface this replaces (GraSPH2 source tree):
+ *   - compile-time switches and constants   settings/settings.h:26-185
+ *   - precision types f1_t/f3_t/m3_t        settings/precisionSettings.h:16-17, src/types.h:32-56
+ *   - particle attributes, in this order    src/particles/partice_attributes.h:91-106
+ *   - DeviceParticleBuffer (owning buffers) src/particles/DeviceParticleBuffer.h:47-233,
+ *                                           src/particles/Device_base.h:126-203
+ *   - computeDerivatives(pb)                src/computeDerivatives.h:315-328
+ *   - integrate(pb, notFirstStep)           src/integration.h:219-244
+ *   - getCurrentTimestep()                  src/integration.h:246-255
+ *
+ * One context = one simulation (or one ensemble) on the current CUDA device. Calls on one
+ * context are not thread-safe; distinct contexts may be driven from distinct host threads.
+ */
+#ifndef GRASPH2_B200_H
+#define GRASPH2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSPH_ABI_VERSION 1
+
+/* ---------------------------------------------------------------------------------------------
+ * status codes
+ * ------------------------------------------------------------------------------------------- */
+#define GSPH_OK              0
+#define GSPH_E_INVALID     (-1)  /* bad argument: null pointer, size out of range, bad mask/flags */
+#define GSPH_E_CUDA        (-2)  /* a CUDA runtime call or a kernel launch failed */
+#define GSPH_E_NOMEM       (-3)  /* device or pinned host allocation failed */
+#define GSPH_E_STATE       (-4)  /* call not valid in the context's current state */
+#define GSPH_E_NUMERIC     (-5)  /* non-finite values found by a host-requested scan */
+#define GSPH_E_TIMEOUT     (-6)  /* a bounded device-side wait gave up (status word set) */
+#define GSPH_E_UNSUPPORTED (-7)  /* feature combination not implemented */
+
+/* ---------------------------------------------------------------------------------------------
+ * physics switches: one bit per `#define` of settings/settings.h
+ * ------------------------------------------------------------------------------------------- */
+#define GSPH_SELF_GRAVITY          (1u << 0)   /* ENABLE_SELF_GRAVITY         settings.h:34  */
+#define GSPH_SPH                   (1u << 1)   /* ENABLE_SPH                  settings.h:37  */
+#define GSPH_INTEGRATE_DENSITY     (1u << 2)   /* INTEGRATE_DENSITY           settings.h:40  */
+#define GSPH_DEAL_WITH_NO_PARTNERS (1u << 3)   /* DEAL_WITH_NO_PARTNERS       settings.h:41  */
+#define GSPH_SOLIDS                (1u << 4)   /* SOLIDS                      settings.h:42  */
+#define GSPH_VARIABLE_TIMESTEP     (1u << 5)   /* VARIABLE_TIMESTEP_LEAPFROG  settings.h:55 (off: FIXED_TIMESTEP_LEAPFROG :49) */
+#define GSPH_ACCELERATION_CRITERION (1u << 6)  /* ACCELERATION_CRITERION      settings.h:59  */
+#define GSPH_VELOCITY_CRITERION    (1u << 7)   /* VELOCITY_CRITERION          settings.h:61  */
+#define GSPH_PLASTICITY_MIESE      (1u << 8)   /* PLASTICITY_MIESE            settings.h:116 */
+#define GSPH_PLASTICITY_MC         (1u << 9)   /* PLASTICITY_MC               settings.h:120 */
+#define GSPH_CLOHESSY_WILTSHIRE    (1u << 10)  /* CLOHESSY_WILTSHIRE          settings.h:136 */
+#define GSPH_CONSTANT_ACCELERATION (1u << 11)  /* CONSTANT_ACCELERATION       settings.h:141 */
+#define GSPH_SIMPLE_BOX_BOUNDARY   (1u << 12)  /* SIMPLE_BOX_BOUNDARY         settings.h:146 */
+#define GSPH_ARTIFICIAL_VISCOSITY  (1u << 13)  /* ARTIFICIAL_VISCOSITY        settings.h:155 */
+#define GSPH_BALSARA_SWITCH        (1u << 14)  /* BALSARA_SWITCH              settings.h:159 */
+#define GSPH_ARTIFICIAL_STRESS     (1u << 15)  /* ARTIFICIAL_STRESS           settings.h:163 */
+#define GSPH_XSPH                  (1u << 16)  /* XSPH                        settings.h:170 */
+#define GSPH_ALL_FLAGS             ((1u << 17) - 1u)
+
+/* ---------------------------------------------------------------------------------------------
+ * runtime parameters: the `constexpr` values of settings/settings.h, plus two knobs the
+ * reference hard-wires (grav_eps, av_beta). Doubles on the host; the kernels round them to the
+ * arithmetic type they compute in.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct gsph_params {
+    uint32_t flags;            /* GSPH_* switches above */
+    int32_t  dimension;        /* 1, 2 or 3                                   settings.h:31      */
+    double   H;                /* smoothing length; kernel support radius   settings.h:99      */
+    double   grav_eps;         /* Plummer softening; the reference uses eps == H
+                                  (src/computeDerivatives.h:231)                                  */
+    double   grav_G;           /* gravitational constant; the reference uses 1                    */
+    double   rho0;             /* rest density                               settings.h:105     */
+    double   bulk;             /* bulk modulus K0 (Murnaghan)                settings.h:106     */
+    double   dbulk_dp;         /* dK0/dP (Murnaghan exponent)                settings.h:107     */
+    double   soundspeed;       /* c: liquid EOS c^2 and AV signal speed      settings.h:108     */
+    double   shear;            /* shear modulus mu                           settings.h:111     */
+    double   Y;                /* von Mises yield stress                     settings.h:117     */
+    double   tanfr;            /* tan(friction angle), Mohr-Coulomb          settings.h:122     */
+    double   cohesion;         /* Mohr-Coulomb cohesion                      settings.h:123     */
+    double   av_alpha;         /* artificial viscosity strength              settings.h:156     */
+    double   av_beta;          /* AV signal velocity v_sig = c_i + c_j - av_beta * w; the
+                                  reference fixes av_beta = 3 (src/sph/models.h:179)             */
+    double   mateps;           /* artificial stress strength                 settings.h:164     */
+    double   matexp;           /* artificial stress exponent                 settings.h:165     */
+    double   normalsep;        /* artificial stress reference separation     settings.h:166     */
+    double   xsph_factor;      /* XSPH velocity smoothing factor             settings.h:171     */
+    double   fixed_dt;         /* fixed leapfrog step                        settings.h:50      */
+    double   initial_dt;       /* variable leapfrog: first step              settings.h:56      */
+    double   min_dt;           /*                    lower clamp             settings.h:57      */
+    double   max_dt;           /*                    upper clamp             settings.h:58      */
+    double   accel_accuracy;   /* dt <= sqrt(accel_accuracy * H / |a|)       settings.h:60      */
+    double   velocity_accuracy;/* dt <= velocity_accuracy * H / v_sig,max    settings.h:62      */
+    double   cw_n;             /* Clohessy-Wiltshire mean motion n           settings.h:137     */
+    double   const_acc[3];     /* constant acceleration                      settings.h:142     */
+    double   box_min[3];       /* simple box boundary                        settings.h:147     */
+    double   box_max[3];       /*                                            settings.h:148     */
+    double   box_reflectiveness; /*                                          settings.h:149     */
+} gsph_params;
+
+/* Fill `p` with the values of the reference's shipped settings/settings.h (a rotating solid
+ * sphere with Mohr-Coulomb plasticity, variable time step, AV and the Balsara switch). */
+int gsph_params_reference_defaults(gsph_params* p);
+
+/* Check a parameter set; returns GSPH_OK or GSPH_E_INVALID / GSPH_E_UNSUPPORTED and, when
+ * `msg`/`msg_len` are given, a one-line reason. */
+int gsph_params_validate(const gsph_params* p, char* msg, size_t msg_len);
+
+/* ---------------------------------------------------------------------------------------------
+ * particle attributes: bit order = particle_bases (src/particles/partice_attributes.h:106)
+ * ------------------------------------------------------------------------------------------- */
+#define GSPH_POS        (1u << 0)   /* f3  */
+#define GSPH_MASS       (1u << 1)   /* f1  */
+#define GSPH_VEL        (1u << 2)   /* f3  */
+#define GSPH_ACC        (1u << 3)   /* f3  */
+#define GSPH_BALSARA    (1u << 4)   /* f1  */
+#define GSPH_XVEL       (1u << 5)   /* f3  */
+#define GSPH_DENSITY    (1u << 6)   /* f1  */
+#define GSPH_DENSITY_DT (1u << 7)   /* f1  */
+#define GSPH_DSTRESS    (1u << 8)   /* m3: 9 values, row-major (tsv/h5 order, src/ResultStorageManager.cu:141-149) */
+#define GSPH_DSTRESS_DT (1u << 9)   /* m3 */
+#define GSPH_MAXVSIG    (1u << 10)  /* f1  */
+#define GSPH_ALL_ATTRIBS ((1u << 11) - 1u)
+
+/* Host-side particle data in the reference's attribute layout (array-of-structs per attribute,
+ * i.e. pos = x0,y0,z0,x1,...). Only the pointers whose bit is set in the call's mask are read or
+ * written; the others may be NULL. Single precision, as f1_t with SINGLE_PRECISION. */
+typedef struct gsph_host_particles {
+    float* pos;        /* 3N */
+    float* mass;       /* N  */
+    float* vel;        /* 3N */
+    float* acc;        /* 3N */
+    float* balsara;    /* N  */
+    float* xvel;       /* 3N */
+    float* density;    /* N  */
+    float* density_dt; /* N  */
+    float* dstress;    /* 9N */
+    float* dstress_dt; /* 9N */
+    float* maxvsig;    /* N  */
+} gsph_host_particles;
+
+/* ---------------------------------------------------------------------------------------------
+ * numerics and launch options of a context
+ * ------------------------------------------------------------------------------------------- */
+#define GSPH_ACCUM_PLAIN       0  /* FP32 accumulation throughout the pair sums */
+#define GSPH_ACCUM_COMPENSATED 1  /* FP32 within a j-tile, two-sum (Kahan-Babuska) fold of each
+                                     tile's partial into the running sum, FP64 combine of j-splits */
+
+typedef struct gsph_options {
+    int32_t accum;           /* GSPH_ACCUM_* */
+    int32_t j_split;         /* j-segments per i-block (0 = pick from N and the SM count) */
+    int32_t j_tile;          /* j-particles per shared-memory stage (0 = default) */
+    int32_t i_per_thread;    /* register blocking of the gravity-only kernel: 1, 2, 4 or 8 (0 = default) */
+    int32_t threads;         /* threads per CTA of the pair kernels (0 = default) */
+    int32_t check_finite;    /* nonzero: scan inputs at upload for NaN/Inf and fail with GSPH_E_NUMERIC */
+    int32_t reserved[10];
+} gsph_options;
+
+int gsph_options_defaults(gsph_options* o);
+
+typedef struct gsph_ctx gsph_ctx;
+
+/* Create a simulation of n particles on the current device with parameters `p` (copied).
+ * Allocates the device attribute buffers (the analogue of DeviceParticleBuffer's constructor,
+ * src/particles/Device_base.h:126-145). `opt` may be NULL for defaults. */
+int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_ctx** out);
+int gsph_destroy(gsph_ctx* ctx);
+
+/* Copy host attributes -> device (pb = hostBuffer, src/particles/Device_base.h:163-181).
+ * `attr_mask` picks the attributes; DSTRESS is symmetrised on upload (the kernels store the six
+ * independent components). Positions are also kept as an FP64 master copy on the device. */
+int gsph_upload(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
+/* Copy device -> host for the attributes in `attr_mask`; synchronises `stream`. */
+int gsph_download(gsph_ctx* ctx, uint32_t attr_mask, gsph_host_particles* dst, void* stream);
+/* FP64 positions (3N, x0,y0,z0,...): upload overrides the FP32 positions; download reads the master. */
+int gsph_upload_pos64(gsph_ctx* ctx, const double* pos, void* stream);
+int gsph_download_pos64(gsph_ctx* ctx, double* pos, void* stream);
+
+/* computeDerivatives(pb)  -- src/computeDerivatives.h:315-328.
+ * Density sum (unless INTEGRATE_DENSITY), then one fused all-pairs pass for gravity, stress
+ * acceleration, AV, strain/rotation rates and the Jaumann stress rate. With the Balsara switch
+ * on, the velocity-gradient pass runs first as its own pass (the reference's
+ * calcBalsaraDensityDTDStressDT), since the acceleration needs every B_j. Asynchronous. */
+int gsph_compute_derivatives(gsph_ctx* ctx, void* stream);
+
+/* integrate(pb, notFirstStep) -- src/integration.h:219-244. Fixed or variable leapfrog with
+ * density/stress update, plasticity and boundaries. The variable step keeps dt on the device
+ * (no host synchronisation). Asynchronous. */
+int gsph_integrate(gsph_ctx* ctx, int not_first_step, void* stream);
+
+/* nsteps x { computeDerivatives; integrate(notFirstStep = true) } -- the loop of
+ * src/main.cu:249-273 without I/O. The step is captured once into a CUDA graph and replayed. */
+int gsph_step(gsph_ctx* ctx, int32_t nsteps, void* stream);
+
+/* getCurrentTimestep() -- src/integration.h:246-255: the fixed step, or the last variable step
+ * (synchronises `stream`). */
+int gsph_current_timestep(gsph_ctx* ctx, double* dt, void* stream);
+
+/* FP64 diagnostics of the current state (no reference counterpart: the reference has none). */
+typedef struct gsph_diag {
+    double e_kin;        /* 1/2 sum m v^2 (v as stored)                      */
+    double e_grav;       /* -G sum_{i<j} m_i m_j / sqrt(r^2 + eps^2)          */
+    double e_int;        /* sum m u(rho), barotropic u of the EOS             */
+    double e_shear;      /* sum m S:S / (4 mu rho) (solids)                   */
+    double momentum[3];  /* sum m v                                           */
+    double ang_mom[3];   /* sum m x cross v                                   */
+    double mass;         /* sum m                                             */
+} gsph_diag;
+/* The velocity used is v + half_kick * a (a as last computed): pass 0 for the stored velocity, or
+ * 0.5*dt right after gsph_compute_derivatives to synchronise the leapfrog's half-step velocity
+ * v_{n-1/2} to v_n. Synchronises `stream`. */
+int gsph_diagnostics(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stream);
+
+/* Number of particles of the context. */
+int gsph_size(gsph_ctx* ctx, int64_t* n);
+/* Text of the last failure on `ctx` (or of the last failed gsph_create when ctx is NULL). */
+const char* gsph_last_error(gsph_ctx* ctx);
+/* Device pointers of the resident arrays, for zero-copy callers (read-only view). */
+typedef struct gsph_device_view {
+    int64_t n;
+    void* posm;      /* float4 x,y,z,m */
+    void* velrho;    /* float4 vx,vy,vz,rho */
+    void* acc;       /* float4 ax,ay,az,max_vsig */
+    void* pos64;     /* double[3][n] (SoA) */
+} gsph_device_view;
+int gsph_device_view_get(gsph_ctx* ctx, gsph_device_view* v);
+
+/* Number of kernels this context launched since creation (host-side count). */
+int gsph_launch_count(gsph_ctx* ctx, int64_t* count);
+
+/* ---------------------------------------------------------------------------------------------
+ * measurement hooks (no reference counterpart: the reference has no kernel timers; its console
+ * frontend prints wall-clock fps only, src/frontends/consoleFrontend.cpp:43-57)
+ * ------------------------------------------------------------------------------------------- */
+#define GSPH_KSLOT_DENSITY  0   /* density-sum pair kernel                        */
+#define GSPH_KSLOT_VGRAD    1   /* velocity-gradient pair kernel (Balsara on)     */
+#define GSPH_KSLOT_PAIRS    2   /* acceleration / fused pair kernel               */
+#define GSPH_KSLOT_GRAVITY  3   /* gravity-only pair kernel                       */
+#define GSPH_KSLOT_STEP     4   /* one whole step (derivatives + integrate)       */
+#define GSPH_KSLOTS         5
+typedef struct gsph_profile {
+    double  ms[GSPH_KSLOTS];        /* accumulated device time per slot (CUDA events) */
+    int64_t launches[GSPH_KSLOTS];  /* launches timed per slot                         */
+} gsph_profile;
+/* Turn per-kernel event timing on or off. When on, each pair kernel launch (including those
+ * inside the step graph, captured after this call) is bracketed by CUDA events on its stream.
+ * Enabling or disabling drops a previously captured step graph. */
+int gsph_profile_enable(gsph_ctx* ctx, int on);
+/* Wait for the events recorded since the last collect and add their durations to the totals. */
+int gsph_profile_collect(gsph_ctx* ctx);
+int gsph_profile_read(gsph_ctx* ctx, gsph_profile* out);
+int gsph_profile_reset(gsph_ctx* ctx);
+
+/* FP32 FFMA throughput of the current device, measured by a dependent-chain-free FMA kernel
+ * running for about `seconds` (the roofline denominator of the FP32-bound pair kernels).
+ * Reports TFLOP/s counting an FMA as 2 flops. */
+int gsph_measure_fp32_peak(double seconds, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRASPH2_B200_H */

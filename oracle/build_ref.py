@@ -1,0 +1,85 @@
+"""Build recipe for the checker libraries (test infrastructure only).
+
+  python oracle/build_ref.py            # both: oracle/liboracle.so and oracle/_ref/*.so
+  python oracle/build_ref.py --oracle   # only the FP64 restatement
+
+oracle/liboracle.so   the FP64 restatement, oracle/oracle.cpp (g++ -O2 -fopenmp)
+oracle/_ref/libref_<variant>_<fp32|fp64>.so
+                      GraSPH2's own job headers compiled in place from the reference tree with
+                      g++ -O3 -march=native -fopenmp against the stand-ins in oracle/ref_shim/
+                      (mpUtils is not vendored with the reference and not installed). Needs the
+                      reference source tree; skipped with a message when it is absent.
+"""
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import ref_variants  # noqa: E402
+
+REFERENCE_SRC = os.environ.get("GRASPH2_REFERENCE", "/root/reference")
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_oracle(force=False):
+    src = os.path.join(HERE, "oracle.cpp")
+    out = os.path.join(HERE, "liboracle.so")
+    hdr = os.path.join(HERE, "..", "include", "grasph2_b200.h")
+    if force or _stale(out, [src, hdr]):
+        _run(["g++", "-std=c++17", "-O2", "-fopenmp", "-fPIC", "-shared", "-o", out, src])
+    return out
+
+
+def build_ref(force=False, march="native"):
+    src_dir = os.path.join(REFERENCE_SRC, "src")
+    if not os.path.isdir(src_dir):
+        print("build_ref: reference tree not found at %s; oracle/_ref not built" % REFERENCE_SRC)
+        return []
+    out_dir = os.path.join(HERE, "_ref")
+    os.makedirs(out_dir, exist_ok=True)
+    shim = os.path.join(HERE, "ref_shim")
+    deps = [os.path.join(HERE, "ref_driver.cpp"), os.path.join(HERE, "ref_variants.py")]
+    for root, _, files in os.walk(shim):
+        deps += [os.path.join(root, f) for f in files]
+    outs = []
+    for name, v in ref_variants.VARIANTS.items():
+        for double in (False, True):
+            out = os.path.join(out_dir, "libref_%s_%s.so" % (name, "fp64" if double else "fp32"))
+            outs.append(out)
+            if not (force or _stale(out, deps)):
+                continue
+            cmd = ["g++", "-std=c++17", "-O3", "-march=%s" % march, "-fopenmp", "-fPIC", "-shared", "-w",
+                   "-I", shim, "-I", src_dir, "-o", out, os.path.join(HERE, "ref_driver.cpp")]
+            cmd += ref_variants.compile_defines(v, double)
+            _run(cmd)
+    return outs
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--oracle", action="store_true", help="build only liboracle.so")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build_oracle(a.force))
+    if not a.oracle:
+        for o in build_ref(a.force):
+            print(o)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,270 @@
+"""Parity of the CUDA path (through the C-ABI) with GraSPH2's own FP64 results and the FP64 oracle.
+
+Tolerances (norm-wise, max_i |x_gpu - x_ref| / max_i |x_ref| over all particles and components),
+after one computeDerivatives on float32-representable inputs:
+    acceleration        1e-5     (the north-star bound)
+    density             1e-6     (the north-star bound)
+    stress rate, drho/dt, Balsara, v_sig,max   1e-5
+After 3 full steps: positions 1e-6, velocities / density / stress 1e-5.
+The reference's own FP32 build meets the same bounds on these inputs (test_oracle.py).
+"""
+
+import numpy as np
+import pytest
+
+import ref_variants
+from grasph2_b200 import ics
+from grasph2_b200.params import config0_params, config1_params, config2_params, make_options, make_params
+from grasph2_b200.sim import DeviceParticleBuffer, GsphError
+from grasph2_b200.state import as_dtype
+from helpers import copy_state, f32_exact, golden_state, rel_max
+
+pytestmark = pytest.mark.gpu
+
+TOL_ACC = 1e-5
+TOL_RHO = 1e-6
+TOL_RATE = 1e-5
+TOL_POS_STEP = 1e-6
+TOL_STATE_STEP = 1e-5
+
+GOLDEN_DIR = __import__("os").path.join(__import__("os").path.dirname(__file__), "golden")
+
+
+def variant_params(name):
+    return make_params(**ref_variants.params_dict(ref_variants.VARIANTS[name]))
+
+
+def load_golden(name):
+    return np.load(__import__("os").path.join(GOLDEN_DIR, "ref_%s.npz" % name))
+
+
+def assert_close(got, want, tol, what):
+    if np.abs(want).max() == 0:
+        assert np.abs(got).max() <= tol, (what, float(np.abs(got).max()))
+        return
+    e = rel_max(got, want)
+    assert e <= tol, "%s: %.3e > %.1e" % (what, e, tol)
+
+
+def gpu_derivatives(params, state, accum="plain", **opt):
+    with DeviceParticleBuffer(params, state["mass"].shape[0], make_options(accum=accum, **opt)) as pb:
+        pb.upload(state)
+        pb.compute_derivatives()
+        return pb.download()
+
+
+def check_derivatives(got, ref, params, tol_acc=TOL_ACC, what=""):
+    flags = params.flags
+    from grasph2_b200._abi import FLAG_BITS as F
+    assert_close(got["acc"], ref["acc"], tol_acc, what + " acc")
+    if flags & F["SPH"]:
+        assert_close(got["density"], ref["density"], TOL_RHO, what + " density")
+        if flags & (F["SOLIDS"] | F["INTEGRATE_DENSITY"] | F["BALSARA_SWITCH"]):
+            assert_close(got["dstress_dt"], ref["dstress_dt"], TOL_RATE, what + " dstress_dt")
+            assert_close(got["density_dt"], ref["density_dt"], TOL_RATE, what + " density_dt")
+            assert_close(got["balsara"], ref["balsara"], TOL_RATE, what + " balsara")
+        assert_close(got["maxvsig"], ref["maxvsig"], TOL_RATE, what + " maxvsig")
+        if flags & F["XSPH"]:
+            assert_close(got["xvel"], ref["xvel"], TOL_RATE, what + " xvel")
+
+
+@pytest.mark.parametrize("accum", ["plain", "compensated"])
+@pytest.mark.parametrize("name", list(ref_variants.VARIANTS))
+def test_golden_derivatives(name, accum):
+    """computeDerivatives vs the reference's own FP64 results (tests/golden)."""
+    z = load_golden(name)
+    p = variant_params(name)
+    got = gpu_derivatives(p, golden_state(z, "in_"), accum)
+    check_derivatives(got, golden_state(z, "d64_"), p, what="%s/%s" % (name, accum))
+
+
+@pytest.mark.parametrize("accum", ["plain", "compensated"])
+@pytest.mark.parametrize("name", list(ref_variants.VARIANTS))
+def test_golden_three_steps(name, accum):
+    """3 x {computeDerivatives; integrate(notFirstStep=true)} vs the reference's FP64 run."""
+    z = load_golden(name)
+    p = variant_params(name)
+    st = golden_state(z, "in_")
+    with DeviceParticleBuffer(p, st["mass"].shape[0], make_options(accum=accum)) as pb:
+        pb.upload(st)
+        dts = []
+        for _ in range(3):
+            pb.compute_derivatives()
+            pb.integrate(True)
+            dts.append(pb.current_timestep())
+        got = pb.download()
+        pos64 = pb.download_pos64()
+    ref = golden_state(z, "s64_")
+    assert_close(pos64, ref["pos"], TOL_POS_STEP, name + " pos64")
+    assert_close(got["pos"], ref["pos"], TOL_POS_STEP, name + " pos")
+    assert_close(got["vel"], ref["vel"], TOL_STATE_STEP, name + " vel")
+    assert_close(got["density"], ref["density"], TOL_STATE_STEP, name + " density")
+    assert_close(got["dstress"], ref["dstress"], TOL_STATE_STEP, name + " dstress")
+    np.testing.assert_allclose(dts, z["dt64"], rtol=1e-6)
+
+
+def _edge_state(name, n, seed):
+    v = ref_variants.VARIANTS[name]
+    rng = np.random.default_rng(seed)
+    st = ics.uniform_sphere(n, radius=1.0, rho0=v["rho0"], omega=(0.0, 0.0, 0.3), seed=seed)
+    st["vel"] += 0.02 * rng.normal(size=(n, 3))
+    st["density"][:] = v["rho0"] * (1 + 0.02 * rng.normal(size=n))
+    S = rng.normal(size=(n, 3, 3)) * 0.05
+    st["dstress"][:] = 0.5 * (S + S.transpose(0, 2, 1))
+    return f32_exact(st)
+
+
+@pytest.mark.parametrize("n", [1, 2, 255, 256, 257, 1000, 1023, 1025, 3000])
+@pytest.mark.parametrize("name", ["nbody", "fluid", "solid", "solid_mc"])
+def test_edge_sizes_vs_oracle(oracle, name, n):
+    """Every N works (the reference's tile loop needs N % 256 == 0, algorithms.h:285-301)."""
+    p = variant_params(name)
+    st = _edge_state(name, n, seed=n)
+    ref = copy_state(st)
+    oracle.ts.current = oracle.ts.next = 0.0
+    oracle.compute_derivatives(p, ref)
+    got = gpu_derivatives(p, st)
+    check_derivatives(got, ref, p, what="%s/n=%d" % (name, n))
+
+
+@pytest.mark.parametrize("opt", [
+    dict(j_split=1), dict(j_split=3), dict(j_split=7), dict(j_tile=64), dict(j_tile=1024),
+    dict(threads=64), dict(threads=256), dict(i_per_thread=1), dict(i_per_thread=2), dict(i_per_thread=8),
+    dict(j_tile=512, threads=256, j_split=5),
+])
+@pytest.mark.parametrize("name", ["nbody", "solid"])
+def test_launch_shapes_vs_oracle(oracle, name, opt):
+    p = variant_params(name)
+    st = _edge_state(name, 2500, seed=11)
+    ref = copy_state(st)
+    oracle.compute_derivatives(p, ref)
+    for accum in ("plain", "compensated"):
+        got = gpu_derivatives(p, st, accum, **opt)
+        check_derivatives(got, ref, p, what="%s/%s/%s" % (name, opt, accum))
+
+
+def test_config0_one_step_vs_oracle(oracle):
+    """SPH + gravity fluid sphere, N=4096 (eps=0.02 != h=0.15): one full step."""
+    p = config0_params()
+    st = f32_exact(ics.uniform_sphere(4096, radius=1.0, rho0=0.239, omega=(0, 0, 0.1), seed=20261203))
+    ref = copy_state(st)
+    oracle.compute_derivatives(p, ref)
+    d = copy_state(ref)
+    oracle.integrate(p, ref, True)
+    with DeviceParticleBuffer(p, 4096) as pb:
+        pb.upload(st)
+        pb.compute_derivatives()
+        got_d = pb.download()
+        pb.integrate(True)
+        got = pb.download()
+    check_derivatives(got_d, d, p, what="config0")
+    assert_close(got["pos"], ref["pos"], TOL_POS_STEP, "config0 pos")
+    assert_close(got["vel"], ref["vel"], TOL_STATE_STEP, "config0 vel")
+
+
+@pytest.mark.slow
+def test_config1_subsample_vs_oracle(oracle):
+    """Elastic-plastic impact at full size N=65536; oracle rows on two target windows."""
+    p = config1_params()
+    st = ics.two_sphere_impact(seed=20261204)
+    rng = np.random.default_rng(5)
+    S = rng.normal(size=(st["mass"].shape[0], 3, 3)) * 0.05
+    st["dstress"][:] = 0.5 * (S + S.transpose(0, 2, 1))
+    st = f32_exact(st)
+    with DeviceParticleBuffer(p, 65536) as pb:
+        pb.upload(st)
+        pb.compute_derivatives()
+        got = pb.download()
+    for i0, i1 in ((0, 384), (65536 - 384, 65536)):
+        ref = copy_state(st)
+        oracle.compute_derivatives(p, ref, i0, i1)
+        sub = {k: v[i0:i1] for k, v in got.items()}
+        rsub = {k: v[i0:i1] for k, v in ref.items()}
+        check_derivatives(sub, rsub, p, what="config1[%d:%d]" % (i0, i1))
+        assert_close(got["density"], ref["density"], TOL_RHO, "config1 density (all)")
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("accum", ["plain", "compensated"])
+def test_config2_gravity_subsample_vs_oracle(oracle, accum):
+    """Plummer sphere N=1,048,576: accelerations of 1024 seeded targets vs FP64 (all sources)."""
+    p = config2_params()
+    st = f32_exact(ics.plummer_sphere(1 << 20, seed=20261205))
+    got = gpu_derivatives(p, st, accum)
+    idx = np.random.default_rng(1).choice(1 << 20, 1024, replace=False)
+    ref = oracle.gravity_targets(p, st["pos"], st["mass"], idx)
+    assert_close(got["acc"][idx], ref, TOL_ACC, "config2 acc " + accum)
+
+
+def test_graph_step_matches_eager():
+    p = variant_params("solid_mc")
+    st = _edge_state("solid_mc", 3000, seed=3)
+    with DeviceParticleBuffer(p, 3000) as a, DeviceParticleBuffer(p, 3000) as b:
+        a.upload(st)
+        b.upload(st)
+        for _ in range(4):
+            a.compute_derivatives()
+            a.integrate(True)
+        b.step(4)
+        x, y = a.download(), b.download()
+        assert a.current_timestep() == b.current_timestep()
+    for k in x:
+        np.testing.assert_array_equal(x[k], y[k], err_msg=k)
+
+
+def test_deterministic():
+    p = variant_params("solid")
+    st = _edge_state("solid", 5000, seed=4)
+    r1 = gpu_derivatives(p, st)
+    r2 = gpu_derivatives(p, st)
+    for k in r1:
+        np.testing.assert_array_equal(r1[k], r2[k], err_msg=k)
+
+
+def test_momentum_conservation_gpu():
+    p = make_params(switches=("SELF_GRAVITY", "SPH", "SOLIDS", "ARTIFICIAL_VISCOSITY", "INTEGRATE_DENSITY"),
+                    H=0.3, rho0=1.0, bulk=10.0, soundspeed=3.0, shear=5.0)
+    st = _edge_state("solid", 3000, seed=9)
+    for accum in ("plain", "compensated"):
+        got = gpu_derivatives(p, st, accum)
+        f = st["mass"][:, None] * got["acc"].astype(np.float64)
+        assert np.abs(f.sum(0)).max() < 1e-5 * np.abs(f).sum(0).max()
+
+
+@pytest.mark.parametrize("name", ["solid", "fluid", "nbody"])
+def test_diagnostics_vs_oracle(oracle, name):
+    p = variant_params(name)
+    st = _edge_state(name, 3000, seed=8)
+    ref = copy_state(st)
+    oracle.compute_derivatives(p, ref)
+    with DeviceParticleBuffer(p, 3000) as pb:
+        pb.upload(st)
+        pb.compute_derivatives()
+        d = pb.diagnostics(half_kick=0.5e-3)
+    o = oracle.diagnostics(p, ref, half_kick=0.5e-3)
+    for k in ("e_kin", "e_grav", "e_int", "e_shear", "mass"):
+        assert abs(d[k] - o[k]) <= 1e-5 * max(abs(o[k]), 1e-30), (k, d[k], o[k])
+    for k in ("momentum", "ang_mom"):
+        scale = abs(o["e_kin"]) ** 0.5 + 1e-12
+        assert np.abs(np.array(d[k]) - np.array(o[k])).max() < 1e-5 * scale, k
+
+
+def test_error_paths_on_device():
+    p = variant_params("fluid")
+    st = _edge_state("fluid", 100, seed=1)
+    with DeviceParticleBuffer(p, 100, make_options(check_finite=1)) as pb:
+        pb.upload(st)
+        with pytest.raises(ValueError):
+            pb.upload({"pos": st["pos"][:50]})
+        bad = as_dtype(st, np.float32)
+        bad["vel"][7, 1] = np.nan
+        with pytest.raises(GsphError) as e:
+            pb.upload(bad)
+        assert e.value.code == -5
+        lib = pb.lib
+        assert lib.gsph_upload(pb.handle, 1 << 20, None, None) == -1
+        from grasph2_b200._abi import GsphHostParticles
+        import ctypes
+        hp = GsphHostParticles()
+        assert lib.gsph_upload(pb.handle, 1, ctypes.byref(hp), None) == -1
+        assert b"NULL" in lib.gsph_last_error(pb.handle)

@@ -1,0 +1,259 @@
+"""The FP64 oracle (oracle/oracle.cpp) pinned to GraSPH2's own code, plus known-answer tests.
+
+CPU only. The golden fixtures in tests/golden/ were produced by the reference's own job headers
+compiled for the host (tests/golden/make_golden.py); when oracle/_ref is built here the oracle is
+also compared with it directly on fresh inputs.
+"""
+
+import glob
+import math
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle
+import ref_variants
+from grasph2_b200 import ics
+from grasph2_b200.params import make_params
+from helpers import copy_state, f32_exact, golden_state, rel_max
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz")))
+FIELDS_D = ("acc", "density", "density_dt", "dstress_dt", "balsara", "maxvsig", "xvel")
+FIELDS_S = ("pos", "vel", "density", "dstress")
+
+
+def variant_params(name):
+    return make_params(**ref_variants.params_dict(ref_variants.VARIANTS[name]))
+
+
+def test_golden_fixtures_present():
+    assert len(GOLDEN) == len(ref_variants.VARIANTS)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p))
+def test_oracle_matches_reference_golden(oracle, path):
+    """Oracle == reference FP64 build, after computeDerivatives and after 3 full steps (1e-11)."""
+    z = np.load(path)
+    name = str(z["variant"])
+    p = variant_params(name)
+    st = golden_state(z, "in_")
+    d = copy_state(st)
+    oracle.ts.current = 0.0
+    oracle.ts.next = 0.0
+    oracle.compute_derivatives(p, d)
+    ref = golden_state(z, "d64_")
+    for k in FIELDS_D:
+        assert rel_max(d[k], ref[k]) < 1e-11 or np.abs(ref[k]).max() == 0 and np.abs(d[k]).max() < 1e-300, (name, k)
+    s = copy_state(st)
+    oracle.ts.current = 0.0
+    oracle.ts.next = 0.0
+    dts = []
+    variable = "VARIABLE_TIMESTEP" in ref_variants.VARIANTS[name]["switches"]
+    for _ in range(3):
+        oracle.compute_derivatives(p, s)
+        oracle.integrate(p, s, True)
+        dts.append(oracle.ts.current if variable else p.fixed_dt)
+    ref = golden_state(z, "s64_")
+    for k in FIELDS_S:
+        if np.abs(ref[k]).max() == 0:
+            assert np.abs(s[k]).max() == 0
+        else:
+            assert rel_max(s[k], ref[k]) < 1e-11, (name, k, rel_max(s[k], ref[k]))
+    np.testing.assert_allclose(dts, z["dt64"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p))
+def test_reference_fp32_close_to_fp64(path):
+    """The reference as shipped (FP32) agrees with its FP64 build to FP32 accuracy: sanity of the
+    fixtures and of the tolerance scale the CUDA path is held to."""
+    z = np.load(path)
+    a32, a64 = golden_state(z, "d32_"), golden_state(z, "d64_")
+    assert rel_max(a32["acc"], a64["acc"]) < 2e-5
+    if np.abs(a64["density"]).max() > 0:
+        assert rel_max(a32["density"], a64["density"]) < 2e-6
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("name", list(ref_variants.VARIANTS))
+@pytest.mark.parametrize("n", [1, 2, 255, 257])
+def test_oracle_matches_reference_build_edge_sizes(oracle, name, n):
+    v = ref_variants.VARIANTS[name]
+    p = variant_params(name)
+    st = ics.uniform_sphere(n, radius=1.0, rho0=v["rho0"], omega=(0.1, 0.2, 0.3), seed=n)
+    rng = np.random.default_rng(n)
+    st["vel"] += 0.05 * rng.normal(size=(n, 3))
+    st["density"][:] = v["rho0"] * (1 + 0.01 * rng.normal(size=n))
+    S = rng.normal(size=(n, 3, 3)) * 0.05
+    st["dstress"][:] = 0.5 * (S + S.transpose(0, 2, 1))
+    st = f32_exact(st)
+    R = pyoracle.RefBuild(name, True)
+    R.lib.ref_set_timestep(0.0, 0.0)
+    oracle.ts.current = oracle.ts.next = 0.0
+    a, b = copy_state(st), copy_state(st)
+    variable = "VARIABLE_TIMESTEP" in v["switches"]
+    for _ in range(2):
+        oracle.compute_derivatives(p, a)
+        R.compute_derivatives(b)
+        oracle.integrate(p, a, True)
+        R.integrate(b, True, variable)
+    for k in ("pos", "vel", "acc", "density", "dstress", "dstress_dt", "density_dt"):
+        if np.abs(b[k]).max() == 0:
+            assert np.abs(a[k]).max() == 0, (name, k)
+        else:
+            assert rel_max(a[k], b[k]) < 1e-11, (name, k, n)
+
+
+# ---- known-answer tests from the formulas --------------------------------------------------------
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_kernel_normalisation(oracle, dim):
+    """int W dV = 1 over the support ball of radius h (kernel.h:41-60, support radius h)."""
+    h = 0.37
+    r = np.linspace(0, h, 20001)
+    w = np.array([oracle.w(x, h, dim) for x in r])
+    shell = {1: 2.0 * np.ones_like(r), 2: 2 * math.pi * r, 3: 4 * math.pi * r * r}[dim]
+    integral = np.trapezoid(w * shell, r)
+    assert abs(integral - 1.0) < 1e-6
+
+
+def test_kernel_derivative(oracle):
+    h = 0.21
+    for r in np.linspace(0.01, 0.2, 40):
+        fd = (oracle.w(r + 1e-7, h) - oracle.w(r - 1e-7, h)) / 2e-7
+        assert abs(fd - oracle.dw(r, h)) < 1e-5 * max(1.0, abs(fd))
+    assert oracle.w(h * 1.0001, h) == 0 and oracle.dw(h * 1.0001, h) == 0
+
+
+def _random_state(n, rho0, seed, stress=0.05):
+    rng = np.random.default_rng(seed)
+    st = ics.uniform_sphere(n, radius=1.0, rho0=rho0, seed=seed)
+    st["vel"][:] = 0.1 * rng.normal(size=(n, 3))
+    st["density"][:] = rho0 * (1 + 0.05 * rng.normal(size=n))
+    S = rng.normal(size=(n, 3, 3)) * stress
+    st["dstress"][:] = 0.5 * (S + S.transpose(0, 2, 1))
+    return st
+
+
+@pytest.mark.parametrize("switches", [
+    ("SELF_GRAVITY",),
+    ("SELF_GRAVITY", "SPH"),
+    ("SELF_GRAVITY", "SPH", "SOLIDS", "ARTIFICIAL_VISCOSITY", "INTEGRATE_DENSITY"),
+    ("SELF_GRAVITY", "SPH", "ARTIFICIAL_VISCOSITY", "BALSARA_SWITCH", "ARTIFICIAL_STRESS", "INTEGRATE_DENSITY"),
+])
+def test_momentum_conservation(oracle, switches):
+    """Every pair term is antisymmetric: sum_i m_i a_i = 0 to rounding (Newton's third law)."""
+    p = make_params(switches=switches, H=0.35, rho0=1.0, bulk=10.0, soundspeed=3.0, shear=5.0)
+    st = _random_state(300, 1.0, 3)
+    oracle.compute_derivatives(p, st)
+    f = st["mass"][:, None] * st["acc"]
+    scale = np.abs(f).sum(0).max()
+    assert np.abs(f.sum(0)).max() < 1e-12 * scale
+
+
+def test_density_excludes_self_and_floor(oracle):
+    """calcDensity skips r = 0 (computeDerivatives.h:72); DEAL_WITH_NO_PARTNERS floors to rho0/100."""
+    st = _random_state(2, 1.0, 1)
+    st["pos"][:] = [[0, 0, 0], [5, 0, 0]]  # far apart: no partner
+    p = make_params(switches=("SPH",), H=0.5, rho0=2.0)
+    oracle.compute_derivatives(p, st)
+    assert np.all(st["density"] == 0.0)
+    p = make_params(switches=("SPH", "DEAL_WITH_NO_PARTNERS"), H=0.5, rho0=2.0)
+    oracle.compute_derivatives(p, st)
+    assert np.allclose(st["density"], 0.02)
+    st["pos"][1] = [0.25, 0, 0]  # partner at q = 1/2: W = prefactor * 2 (1/2)^3
+    p = make_params(switches=("SPH",), H=0.5, rho0=2.0)
+    oracle.compute_derivatives(p, st)
+    w = 8.0 / (math.pi * 0.5 ** 3) * 2 * 0.5 ** 3
+    assert np.allclose(st["density"], st["mass"][::-1] * w)
+
+
+def test_eos_zero_at_rest_density(oracle):
+    """p(rho0) = 0 for both EOS: a static configuration at rest density feels no SPH force."""
+    for sw in [("SPH", "INTEGRATE_DENSITY"), ("SPH", "SOLIDS", "INTEGRATE_DENSITY")]:
+        p = make_params(switches=sw, H=0.5, rho0=1.3, bulk=7.0, soundspeed=2.0)
+        st = _random_state(50, 1.3, 5, stress=0.0)
+        st["density"][:] = 1.3
+        st["vel"][:] = 0
+        oracle.compute_derivatives(p, st)
+        assert np.abs(st["acc"]).max() < 1e-13
+
+
+def test_jaumann_rate(oracle):
+    """dstress_dt (models.h:250-268) == 2 mu (E - tr E / 3 I) + S R^T + R S^T for symmetric S."""
+    rng = np.random.default_rng(0)
+    for _ in range(10):
+        E = rng.normal(size=(3, 3))
+        E = E + E.T
+        R = rng.normal(size=(3, 3))
+        R = R - R.T
+        S = rng.normal(size=(3, 3))
+        S = S + S.T
+        mu = 3.7
+        want = 2 * mu * (E - np.trace(E) / 3 * np.eye(3)) + S @ R.T + R @ S.T
+        np.testing.assert_allclose(oracle.dstress_dt(E, R, S, mu), want, rtol=1e-12, atol=1e-12)
+        # objectivity: for E = 0 the rate is the rotation of S, trace-free and symmetric
+        D = oracle.dstress_dt(np.zeros((3, 3)), R, S, mu)
+        assert abs(np.trace(D)) < 1e-12 and np.abs(D - D.T).max() < 1e-12
+
+
+def test_plasticity_limiter(oracle):
+    """S *= Y^2 / (3 J2) when that factor is < 1, with J2 = 1/2 S:S and no square root."""
+    S = np.diag([1.0, -0.5, -0.5])
+    J2 = 0.5 * (S * S).sum()
+    Y = 0.5
+    out = oracle.plasticity(S, Y)
+    np.testing.assert_allclose(out, S * (Y * Y / (3 * J2)))
+    small = S * 0.01
+    np.testing.assert_array_equal(oracle.plasticity(small, Y), small)
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="oracle/_ref not built")
+def test_plasticity_and_jaumann_match_reference_functions(oracle):
+    R = pyoracle.RefBuild("solid", True)
+    rng = np.random.default_rng(1)
+    for _ in range(5):
+        S = rng.normal(size=(3, 3))
+        S = S + S.T
+        a = S.copy().ravel()
+        R.lib.ref_plasticity(a.ctypes.data_as(pyoracle.ctypes.POINTER(pyoracle.ctypes.c_double)), 0.3)
+        np.testing.assert_allclose(oracle.plasticity(S, 0.3).ravel(), a, rtol=1e-14)
+        E = rng.normal(size=(3, 3))
+        W = rng.normal(size=(3, 3))
+        out = np.zeros(9)
+        dp = pyoracle.ctypes.POINTER(pyoracle.ctypes.c_double)
+        args = [np.ascontiguousarray(x).ravel() for x in (E, W, S)]
+        R.lib.ref_dstress_dt(*[x.ctypes.data_as(dp) for x in args], 2.5, out.ctypes.data_as(dp))
+        np.testing.assert_allclose(oracle.dstress_dt(E, W, S, 2.5).ravel(), out, rtol=1e-13, atol=1e-14)
+
+
+def test_kepler_two_body_leapfrog(oracle):
+    """Fixed-step KDK on a softened two-body orbit: energy bounded, orbit closes (integration.h)."""
+    p = make_params(switches=("SELF_GRAVITY",), H=1e-3, grav_eps=1e-3, fixed_dt=1e-3)
+    from grasph2_b200.state import new_state
+    st = new_state(2, np.float64)
+    st["mass"][:] = 0.5
+    st["pos"][:] = [[-0.5, 0, 0], [0.5, 0, 0]]
+    v = math.sqrt(1.0 / 1.0) / 2  # circular orbit: v^2 = G M_tot / (4 r) for separation 2r = 1
+    st["vel"][:] = [[0, -v, 0], [0, v, 0]]
+    e0 = None
+    es = []
+    for k in range(6000):
+        oracle.compute_derivatives(p, st)
+        d = oracle.diagnostics(p, st, half_kick=0.0 if k == 0 else 0.5 * p.fixed_dt)
+        es.append(d["e_kin"] + d["e_grav"])
+        oracle.integrate(p, st, k > 0)
+    es = np.array(es)
+    assert np.abs(es - es[0]).max() < 1e-5 * abs(es[0])
+
+
+def test_diagnostics_potential_pairs(oracle):
+    p = make_params(switches=("SELF_GRAVITY",), H=0.1, grav_eps=0.1)
+    from grasph2_b200.state import new_state
+    st = new_state(3, np.float64)
+    st["mass"][:] = [1.0, 2.0, 3.0]
+    st["pos"][:] = [[0, 0, 0], [1, 0, 0], [0, 2, 0]]
+    d = oracle.diagnostics(p, st)
+    e = 0.01
+    want = -(1 * 2 / math.sqrt(1 + e) + 1 * 3 / math.sqrt(4 + e) + 2 * 3 / math.sqrt(5 + e))
+    assert abs(d["e_grav"] - want) < 1e-13
+    assert d["mass"] == 6.0
