@@ -55,11 +55,14 @@ def parse():
     ap.add_argument("--accum", choices=["plain", "compensated"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak probe (profiling runs)")
+    ap.add_argument("--n", type=int, default=0, help="particle count of the fluid / plummer workloads")
     return ap.parse_args()
 
 
 # ---- workloads ------------------------------------------------------------------------------------
-def workload(name):
+def workload(name, n=0):
     from grasph2_b200 import ics
     from grasph2_b200.params import config0_params, config1_params, config2_params
     if name == "impact":
@@ -68,10 +71,12 @@ def workload(name):
                 "shear=5, von Mises Y=0.5, AV alpha=1 beta=2, h=2.5x mean spacing, G=1 eps=0.01, dt=1e-4")
         return config1_params(), st, desc, "impact"
     if name == "fluid":
-        st = ics.uniform_sphere(4096, radius=1.0, rho0=0.239, omega=(0, 0, 0.1), seed=20261203)
-        return config0_params(), st, "SPH + self-gravity fluid sphere, N=4096, h=0.15, eps=0.02", "fluid"
-    st = ics.plummer_sphere(1 << 20, seed=20261203)
-    return config2_params(), st, "Plummer sphere N-body, N=1048576, a=1, eps=0.01, dt=1e-3", "nbody"
+        n = n or 4096
+        st = ics.uniform_sphere(n, radius=1.0, rho0=0.239, omega=(0, 0, 0.1), seed=20261203)
+        return config0_params(), st, "SPH + self-gravity fluid sphere, N=%d, h=0.15, eps=0.02" % n, "fluid"
+    n = n or (1 << 20)
+    st = ics.plummer_sphere(n, seed=20261203)
+    return config2_params(), st, "Plummer sphere N-body, N=%d, a=1, eps=0.01, dt=1e-3" % n, "nbody"
 
 
 def flops_per_step(params, st, counts):
@@ -212,7 +217,7 @@ def cpu_reference_sample(variant, st, budget_s, rows_hint=None):
 def run_reference_arm(args, rank, world):
     if world > 1 and rank != 0:
         return
-    params, st, desc, variant = workload(args.workload)
+    params, st, desc, variant = workload(args.workload, args.n)
     n = st["mass"].shape[0]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
@@ -283,12 +288,12 @@ def main():
     from grasph2_b200.params import make_options
     from grasph2_b200.sim import DeviceParticleBuffer, measure_fp32_peak
 
-    params, st, desc, variant = workload(args.workload)
+    params, st, desc, variant = workload(args.workload, args.n)
     n = st["mass"].shape[0]
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
-    peak_tflops = measure_fp32_peak(0.5)
+    peak_tflops = None if args.no_peak else measure_fp32_peak(0.5)
 
     def barrier():
         if dist is not None:
@@ -338,11 +343,11 @@ def main():
     pinned_out = {k: torch.empty(host_out[k].shape, dtype=torch.float32).pin_memory().numpy() for k in down_names}
     h2d = sum(a.nbytes for a in pinned_in.values())
     d2h = sum(a.nbytes for a in pinned_out.values())
-    e2e_steps = max(5, min(args.steps, 50))
+    e2e_steps = 0 if args.no_e2e else max(5, min(args.steps, 50))
     pb.profile_enable(False)
     pb2 = DeviceParticleBuffer(params, n, make_options(accum=args.accum))
     e2e_ms = 0.0
-    for k in range(e2e_steps + 3):
+    for k in range(e2e_steps + 3 if e2e_steps else 0):
         flush.zero_()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
@@ -387,13 +392,13 @@ def main():
         "pair_interactions_per_s": pairs_per_step * value,
         "kernel_ms_per_step": {k: (v[0] / v[1] if v[1] else None) for k, v in prof.items()},
         "roofline": {"bound": "fp32", "kernel": dominant, "achieved": achieved, "peak": peak_tflops,
-                     "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None,
+                     "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if (achieved and peak_tflops) else None,
                      "traffic": None, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
                      "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
         "cpu_baseline": cpu,
         "clocks": clocks,
-        "e2e": {"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+        "e2e": ({"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                 "d2h_bytes_per_step": d2h} if e2e_steps else None),
         "gpu_launches": gpu_launches,
     }
     print(json.dumps(line))

@@ -150,7 +150,7 @@ struct PairAcc {
 
 // GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: the self pair must contribute 0)
 template <int PASS, int GRAV, bool SOLIDS, bool COMP>
-__global__ void __launch_bounds__(128) k_pairs(DevArrays a, DevParams p, int jt, int nseg) {
+__global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt, int nseg) {
     constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
     constexpr int K = popc_c(MASK);
     constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;

@@ -1,0 +1,219 @@
+// grasph2_b200.hpp -- header-only C++ adapter over the C-ABI with GraSPH2's names, so a driver
+// written against the reference's hot path (src/main.cu:249-273) ports line for line:
+//
+//     gsph::HostParticleBuffer hpb(n);                   // HostParticleBuffer<...>   (HostParticleBuffer.h:47-99)
+//     gsph::DeviceParticleBuffer pb(params, hpb.size());  // DeviceParticleBuffer<...> (DeviceParticleBuffer.h:47-233)
+//     pb = hpb;                                           // upload                    (Device_base.h:163-181)
+//     computeDerivatives(pb);                             // src/computeDerivatives.h:315-328
+//     integrate(pb, true);                                // src/integration.h:219-244
+//     double dt = getCurrentTimestep(pb);                 // src/integration.h:246-255
+//     hpb = pb;                                           // download
+//     gsph::printTextFile(hpb, path);                     // ResultStorageManager::printTextFile (.cu:160-186)
+//
+// Errors throw gsph::Error (a std::runtime_error carrying the GSPH_E_* code); the reference's
+// assert_cuda throws/aborts in the same places.
+#ifndef GRASPH2_B200_HPP
+#define GRASPH2_B200_HPP
+
+#include <cctype>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <limits>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "grasph2_b200.h"
+
+namespace gsph {
+
+class Error : public std::runtime_error {
+public:
+    Error(int code, const std::string& what) : std::runtime_error(what), code_(code) {}
+    int code() const { return code_; }
+
+private:
+    int code_;
+};
+
+inline void check(int rc, gsph_ctx* ctx) {
+    if (rc != GSPH_OK) throw Error(rc, gsph_last_error(ctx));
+}
+
+// Host particle attributes in the reference layout, one std::vector<float> per attribute.
+class HostParticleBuffer {
+public:
+    HostParticleBuffer() = default;
+    explicit HostParticleBuffer(size_t n) { resize(n); }
+    void resize(size_t n) {
+        n_ = n;
+        pos.assign(3 * n, 0.f); mass.assign(n, 0.f); vel.assign(3 * n, 0.f); acc.assign(3 * n, 0.f);
+        balsara.assign(n, 0.f); xvel.assign(3 * n, 0.f); density.assign(n, 0.f); density_dt.assign(n, 0.f);
+        dstress.assign(9 * n, 0.f); dstress_dt.assign(9 * n, 0.f); maxvsig.assign(n, 0.f);
+    }
+    size_t size() const { return n_; }
+    gsph_host_particles view() {
+        return gsph_host_particles{pos.data(), mass.data(), vel.data(), acc.data(), balsara.data(), xvel.data(),
+                                   density.data(), density_dt.data(), dstress.data(), dstress_dt.data(), maxvsig.data()};
+    }
+    std::vector<float> pos, mass, vel, acc, balsara, xvel, density, density_dt, dstress, dstress_dt, maxvsig;
+
+private:
+    size_t n_ = 0;
+};
+
+// Owning device buffer of one simulation (RAII over gsph_create / gsph_destroy).
+class DeviceParticleBuffer {
+public:
+    DeviceParticleBuffer(const gsph_params& p, int64_t n, const gsph_options* opt = nullptr) {
+        check(gsph_create(&p, opt, n, &ctx_), nullptr);
+    }
+    ~DeviceParticleBuffer() {
+        if (ctx_) gsph_destroy(ctx_);
+    }
+    DeviceParticleBuffer(const DeviceParticleBuffer&) = delete;
+    DeviceParticleBuffer& operator=(const DeviceParticleBuffer&) = delete;
+    DeviceParticleBuffer(DeviceParticleBuffer&& o) noexcept : ctx_(std::exchange(o.ctx_, nullptr)) {}
+    DeviceParticleBuffer& operator=(DeviceParticleBuffer&& o) noexcept {
+        if (this != &o) {
+            if (ctx_) gsph_destroy(ctx_);
+            ctx_ = std::exchange(o.ctx_, nullptr);
+        }
+        return *this;
+    }
+    // pb = hostBuffer: every attribute (Device_base.h:163-181)
+    DeviceParticleBuffer& operator=(HostParticleBuffer& h) {
+        upload(h, GSPH_ALL_ATTRIBS);
+        return *this;
+    }
+    void upload(HostParticleBuffer& h, uint32_t mask, void* stream = nullptr) {
+        gsph_host_particles v = h.view();
+        check(gsph_upload(ctx_, mask, &v, stream), ctx_);
+    }
+    void download(HostParticleBuffer& h, uint32_t mask = GSPH_ALL_ATTRIBS, void* stream = nullptr) {
+        if (h.size() != static_cast<size_t>(size())) h.resize(static_cast<size_t>(size()));
+        gsph_host_particles v = h.view();
+        check(gsph_download(ctx_, mask, &v, stream), ctx_);
+    }
+    int64_t size() const {
+        int64_t n = 0;
+        check(gsph_size(ctx_, &n), ctx_);
+        return n;
+    }
+    void step(int nsteps, void* stream = nullptr) { check(gsph_step(ctx_, nsteps, stream), ctx_); }
+    gsph_diag diagnostics(double half_kick = 0.0, void* stream = nullptr) {
+        gsph_diag d{};
+        check(gsph_diagnostics(ctx_, half_kick, &d, stream), ctx_);
+        return d;
+    }
+    gsph_ctx* get() const { return ctx_; }
+
+private:
+    gsph_ctx* ctx_ = nullptr;
+};
+
+// hostBuffer = deviceBuffer
+inline HostParticleBuffer& operator<<(HostParticleBuffer& h, DeviceParticleBuffer& d) {
+    d.download(h);
+    return h;
+}
+
+inline void computeDerivatives(DeviceParticleBuffer& pb, void* stream = nullptr) {
+    check(gsph_compute_derivatives(pb.get(), stream), pb.get());
+}
+inline void integrate(DeviceParticleBuffer& pb, bool notFirstStep, void* stream = nullptr) {
+    check(gsph_integrate(pb.get(), notFirstStep ? 1 : 0, stream), pb.get());
+}
+inline double getCurrentTimestep(DeviceParticleBuffer& pb, void* stream = nullptr) {
+    double dt = 0.0;
+    check(gsph_current_timestep(pb.get(), &dt, stream), pb.get());
+    return dt;
+}
+
+// ---- tsv snapshots -----------------------------------------------------------------------------
+// One line per particle; the selected attributes in particle_bases order, every value followed by
+// a tab; fixed notation with digits10 + 1 digits (ResultStorageManager::printTextFile,
+// src/ResultStorageManager.cu:160-186; the stored attributes are HostDiscPT's, settings
+// outputSettings.h:26: POS, MASS, VEL, DENSITY by default).
+constexpr uint32_t kDefaultStoredAttributes = GSPH_POS | GSPH_MASS | GSPH_VEL | GSPH_DENSITY;
+
+inline int attribute_components(int bit) {
+    static const int comps[11] = {3, 1, 3, 3, 1, 3, 1, 1, 9, 9, 1};
+    return comps[bit];
+}
+inline const std::vector<float>& attribute_data(const HostParticleBuffer& h, int bit) {
+    const std::vector<float>* a[11] = {&h.pos, &h.mass, &h.vel, &h.acc, &h.balsara, &h.xvel,
+                                       &h.density, &h.density_dt, &h.dstress, &h.dstress_dt, &h.maxvsig};
+    return *a[bit];
+}
+inline std::vector<float>& attribute_data(HostParticleBuffer& h, int bit) {
+    return const_cast<std::vector<float>&>(attribute_data(static_cast<const HostParticleBuffer&>(h), bit));
+}
+
+// file name <directory><prefix><startTime>_<time>.tsv (ResultStorageManager.cu:162-163)
+inline std::string snapshotFileName(const std::string& directory, const std::string& prefix,
+                                    const std::string& startTime, float time, const char* ext = ".tsv") {
+    std::ostringstream fn;
+    fn << directory << prefix << startTime << "_" << std::fixed
+       << std::setprecision(std::numeric_limits<float>::digits10 + 1) << time << ext;
+    return fn.str();
+}
+
+inline void printTextFile(const HostParticleBuffer& h, const std::string& filename,
+                          uint32_t mask = kDefaultStoredAttributes) {
+    std::ofstream file(filename);
+    if (!file.is_open()) throw Error(GSPH_E_INVALID, "Could not open output file: " + filename);
+    file << std::fixed << std::setprecision(std::numeric_limits<float>::digits10 + 1);
+    for (size_t i = 0; i < h.size(); ++i) {
+        for (int b = 0; b < 11; ++b) {
+            if (!(mask >> b & 1u)) continue;
+            const int k = attribute_components(b);
+            const std::vector<float>& a = attribute_data(h, b);
+            for (int c = 0; c < k; ++c) file << a[k * i + c] << "\t";
+        }
+        file << "\n";
+    }
+    if (file.fail()) throw Error(GSPH_E_INVALID, "Error writing output file: " + filename);
+}
+
+// TextFile reader (src/initialConditions/particleSources/TextFile.h:76-120): non-blank lines are
+// particles, values separated by `sep`, the attributes in `mask` in particle_bases order.
+inline HostParticleBuffer readTextFile(const std::string& filename, uint32_t mask = kDefaultStoredAttributes,
+                                       char sep = '\t') {
+    std::ifstream file(filename);
+    if (!file.is_open()) throw Error(GSPH_E_INVALID, "Error opening file: " + filename);
+    std::vector<std::string> lines;
+    std::string line;
+    while (std::getline(file, line)) {
+        bool blank = true;
+        for (char c : line)
+            if (!std::isspace(static_cast<unsigned char>(c))) blank = false;
+        if (!blank) lines.push_back(line);
+    }
+    HostParticleBuffer h(lines.size());
+    for (size_t i = 0; i < lines.size(); ++i) {
+        std::istringstream ls(lines[i]);
+        for (int b = 0; b < 11; ++b) {
+            if (!(mask >> b & 1u)) continue;
+            const int k = attribute_components(b);
+            std::vector<float>& a = attribute_data(h, b);
+            for (int c = 0; c < k; ++c) {
+                std::string tok;
+                do {
+                    if (!std::getline(ls, tok, sep)) throw Error(GSPH_E_INVALID, "Error parsing input file at line " +
+                                                                                     std::to_string(i));
+                } while (tok.find_first_not_of(" \t") == std::string::npos);
+                a[k * i + c] = std::stof(tok);
+            }
+        }
+    }
+    return h;
+}
+
+}  // namespace gsph
+
+#endif  // GRASPH2_B200_HPP

@@ -257,3 +257,24 @@ def test_diagnostics_potential_pairs(oracle):
     want = -(1 * 2 / math.sqrt(1 + e) + 1 * 3 / math.sqrt(4 + e) + 2 * 3 / math.sqrt(5 + e))
     assert abs(d["e_grav"] - want) < 1e-13
     assert d["mass"] == 6.0
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p))
+def test_reference_fp32_meets_the_parity_bound(oracle, path):
+    """GraSPH2's own FP32 build meets the condition-aware bound the CUDA path is held to
+    (tests/test_gpu_parity.py): the bound is achievable in FP32 and not looser than the reference."""
+    from helpers import check_within, fp32_sensitivity
+    z = np.load(path)
+    name = str(z["variant"])
+    p = variant_params(name)
+
+    def run(st):
+        oracle.ts.current = oracle.ts.next = 0.0
+        oracle.compute_derivatives(p, st)
+        return st
+
+    _, sens = fp32_sensitivity(run, golden_state(z, "in_"))
+    a32, a64 = golden_state(z, "d32_"), golden_state(z, "d64_")
+    check_within(a32["acc"], a64["acc"], sens["acc"], 1e-5, name + " acc")
+    check_within(a32["density"], a64["density"], sens["density"], 1e-6, name + " density")
+    check_within(a32["dstress_dt"], a64["dstress_dt"], sens["dstress_dt"], 1e-5, name + " dstress_dt")
