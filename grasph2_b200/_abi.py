@@ -65,7 +65,7 @@ class GsphOptions(ctypes.Structure):
     _fields_ = [
         ("accum", ctypes.c_int32), ("j_split", ctypes.c_int32), ("j_tile", ctypes.c_int32),
         ("i_per_thread", ctypes.c_int32), ("threads", ctypes.c_int32), ("check_finite", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 10),
+        ("no_cull", ctypes.c_int32), ("resort_interval", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
     ]
 
 
@@ -134,6 +134,7 @@ _SIGNATURES = {
     "gsph_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
                                         ctypes.c_void_p]),
     "gsph_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_reorder": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "gsph_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_device_view_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GsphDeviceView)]),
     "gsph_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),

@@ -11,6 +11,7 @@
 
 #include "integrate.cuh"
 #include "pairs.cuh"
+#include "spatial.cuh"
 
 using namespace gsph;
 
@@ -20,6 +21,8 @@ struct gsph_ctx {
     DevParams dp;
     Launch L;
     DevArrays a;
+    SpatialArrays sp{};
+    int64_t steps_since_sort = 0;
     int device = 0;
     int sm_count = 148;
     std::vector<void*> allocations;
@@ -118,6 +121,8 @@ DevParams make_dev_params(const gsph_params& p) {
     }
     d.box_refl = static_cast<float>(p.box_reflectiveness);
     d.balsara_floor = static_cast<float>(0.0001 * p.soundspeed / p.H);
+    d.eps2_d = p.grav_eps * p.grav_eps;
+    d.G_d = p.grav_G;
     return d;
 }
 
@@ -191,8 +196,15 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
     const DevParams& p = c->dp;
     cudaError_t e;
     if (has(p, GSPH_SPH)) {
+        const SpatialArrays* sp = c->L.cull ? &c->sp : nullptr;
+        if (sp) {  // bounds of every chunk at the current positions, then each group's near chunks
+            e = launch_chunk_bounds(c->a, c->sp, s);
+            if (e == cudaSuccess) e = launch_chunk_lists(c->a, c->sp, p.H, s);
+            if (e != cudaSuccess) return cuda_fail(c, e, "chunk lists");
+            c->launches += 2;
+        }
         if (!has(p, GSPH_INTEGRATE_DENSITY)) {
-            e = launch_density(c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_DENSITY));
+            e = launch_density(c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_DENSITY), sp);
             if (e != cudaSuccess) return cuda_fail(c, e, "density pass");
             c->launches += 2;
         } else {
@@ -201,17 +213,20 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
             c->launches += 1;
         }
         const bool vgrad = has(p, GSPH_SOLIDS) || has(p, GSPH_INTEGRATE_DENSITY) || has(p, GSPH_BALSARA_SWITCH);
+        const bool grav_kernel = sp && has(p, GSPH_SELF_GRAVITY);
+        const KTimer* tg = grav_kernel ? slot_timer(c, GSPH_KSLOT_GRAVITY) : nullptr;
         if (vgrad && has(p, GSPH_BALSARA_SWITCH)) {
-            e = launch_pairs(PASS_VGRAD, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_VGRAD));
+            e = launch_pairs(PASS_VGRAD, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_VGRAD), sp);
             if (e != cudaSuccess) return cuda_fail(c, e, "velocity-gradient pass");
-            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS));
+            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, tg);
             if (e != cudaSuccess) return cuda_fail(c, e, "acceleration pass");
             c->launches += 4;
         } else {
-            e = launch_pairs(vgrad ? PASS_FUSED : PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS));
+            e = launch_pairs(vgrad ? PASS_FUSED : PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, tg);
             if (e != cudaSuccess) return cuda_fail(c, e, "pair pass");
             c->launches += 2;
         }
+        if (grav_kernel) c->launches += 1;
     } else {
         e = launch_gravity(c->a, p, c->L, s,
                            has(p, GSPH_SELF_GRAVITY) ? slot_timer(c, GSPH_KSLOT_GRAVITY) : nullptr);
@@ -220,6 +235,18 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
     }
     return GSPH_OK;
 }
+
+int reorder(gsph_ctx* c, cudaStream_t s) {
+    if (!c->L.cull) return GSPH_OK;
+    int launches = 0;
+    const cudaError_t e = reorder_particles(c->a, c->sp, s, launches);
+    c->launches += launches;
+    c->steps_since_sort = 0;
+    if (e != cudaSuccess) return cuda_fail(c, e, "particle reorder");
+    return GSPH_OK;
+}
+
+const int* ext_map(const gsph_ctx* c) { return c->L.cull ? c->sp.ext_of_int : nullptr; }
 
 int integrate(gsph_ctx* c, int not_first_step, cudaStream_t s) {
     cudaError_t e = launch_leapfrog(c->a, c->dp, not_first_step, s);
@@ -340,15 +367,39 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     // launch shape
     Launch& L = c->L;
     L.accum = o.accum;
+    L.cull = (p->flags & GSPH_SPH) && !o.no_cull;
     L.threads = o.threads ? o.threads : 128;
     L.jt = o.j_tile ? o.j_tile : 256;
-    L.grav_threads = 128;
-    L.grav_ipt = o.i_per_thread ? o.i_per_thread : 4;
     const int64_t ntiles = n_pad / L.jt;
     const int cap = static_cast<int>(std::min<int64_t>(kMaxSplit, std::max<int64_t>(1, ntiles)));
     L.nseg = o.j_split ? std::min(o.j_split, cap) : pick_split(n_pad / L.threads, c->sm_count * 4, cap);
-    L.grav_nseg = o.j_split ? std::min(o.j_split, cap)
-                            : pick_split(n_pad / (int64_t(L.grav_threads) * L.grav_ipt), c->sm_count * 4, cap);
+    // gravity kernel: the most i-blocking (and the largest j-tile) that still gives two waves of CTAs
+    L.grav_threads = 128;
+    {
+        const bool comp = o.accum == GSPH_ACCUM_COMPENSATED;
+        const int ipts[3] = {4, 2, 1};
+        const int jts[3] = {256, 128, 64};
+        int best_i = 1, best_jt = 64;
+        bool found = false;
+        for (int a = 0; a < 3 && !found; ++a)
+            for (int b = 0; b < 3 && !found; ++b) {
+                const int64_t iblocks = n_pad / (int64_t(L.grav_threads) * ipts[a]);
+                const int64_t maxseg = std::min<int64_t>(kMaxSplit, n_pad / jts[b]);
+                const int slots = c->sm_count * gravity_blocks_per_sm(ipts[a], L.grav_threads, jts[b], comp);
+                if (iblocks * maxseg >= 2 * slots) {
+                    best_i = ipts[a];
+                    best_jt = jts[b];
+                    found = true;
+                }
+            }
+        L.grav_ipt = o.i_per_thread ? o.i_per_thread : best_i;
+        L.grav_jt = o.j_tile ? o.j_tile : best_jt;
+        const int64_t gt = n_pad / L.grav_jt;
+        const int gcap = static_cast<int>(std::min<int64_t>(kMaxSplit, std::max<int64_t>(1, gt)));
+        const int slots = c->sm_count * gravity_blocks_per_sm(L.grav_ipt, L.grav_threads, L.grav_jt, comp);
+        L.grav_nseg = o.j_split ? std::min(o.j_split, gcap)
+                                : pick_split(n_pad / (int64_t(L.grav_threads) * L.grav_ipt), slots, gcap);
+    }
 
     cudaError_t ae = cudaSuccess;
     auto F4 = [&](void) { return static_cast<float4*>(dalloc(c, n_pad * sizeof(float4), ae)); };
@@ -359,6 +410,24 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     a.rhodot = static_cast<float*>(dalloc(c, n_pad * sizeof(float), ae));
     a.balsara = static_cast<float*>(dalloc(c, n_pad * sizeof(float), ae));
     a.part = static_cast<float*>(dalloc(c, partial_floats(c->dp, L, n_pad) * sizeof(float), ae));
+    a.gpart = static_cast<float*>(dalloc(c, (L.cull ? gravity_partial_floats(L, n_pad) : 4) * sizeof(float), ae));
+    if (L.cull) {
+        SpatialArrays& sp = c->sp;
+        const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
+        sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
+        sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
+        sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));
+        sp.count = static_cast<int*>(dalloc(c, ngroups * sizeof(int), ae));
+        sp.ext_of_int = static_cast<int*>(dalloc(c, n_pad * sizeof(int), ae));
+        sp.order = static_cast<int*>(dalloc(c, n_pad * sizeof(int), ae));
+        sp.order_out = static_cast<int*>(dalloc(c, n_pad * sizeof(int), ae));
+        sp.keys = static_cast<unsigned*>(dalloc(c, 2 * n_pad * sizeof(unsigned), ae));
+        sp.sort_tmp_bytes = spatial_sort_tmp_bytes(n_pad);
+        sp.sort_tmp = dalloc(c, sp.sort_tmp_bytes, ae);
+        sp.bbox = static_cast<int*>(dalloc(c, 8 * sizeof(int), ae));
+        sp.tmp4 = static_cast<float4*>(dalloc(c, n_pad * sizeof(float4), ae));
+        sp.tmp8 = static_cast<double*>(dalloc(c, n_pad * sizeof(double), ae));
+    }
     a.dt_state = static_cast<float*>(dalloc(c, 4 * sizeof(float), ae));
     a.diag = static_cast<double*>(dalloc(c, diag_scratch_doubles(n) * sizeof(double), ae));
     a.status = static_cast<int*>(dalloc(c, sizeof(int) * 4, ae));
@@ -373,6 +442,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     e = cudaMemset(a.dt_state, 0, 4 * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(a.status, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = launch_init_padding(a, 0);
+    if (e == cudaSuccess && L.cull) e = launch_identity_order(c->sp, n_pad, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         release(c);
@@ -405,8 +475,12 @@ int gsph_upload(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void
         if (!(mask >> k & 1u)) continue;
         GSPH_CK(c, cudaMemcpyAsync(c->staging, ptrs[k], comps[k] * c->a.n * sizeof(float), cudaMemcpyHostToDevice, s),
                 "upload copy");
-        GSPH_CK(c, launch_pack(c->a, k, c->staging, s), "upload pack");
+        GSPH_CK(c, launch_pack(c->a, k, c->staging, ext_map(c), s), "upload pack");
         c->launches += 1;
+    }
+    if (mask & GSPH_POS) {
+        const int rc = reorder(c, s);
+        if (rc != GSPH_OK) return rc;
     }
     if (c->opt.check_finite) {
         GSPH_CK(c, launch_check_finite(c->a, s), "finite check");
@@ -428,7 +502,7 @@ int gsph_download(gsph_ctx* c, uint32_t mask, gsph_host_particles* dst, void* st
     cudaStream_t s = as_stream(stream);
     for (int k = 0; k < 11; ++k) {
         if (!(mask >> k & 1u)) continue;
-        GSPH_CK(c, launch_unpack(c->a, k, c->staging, s), "download unpack");
+        GSPH_CK(c, launch_unpack(c->a, k, c->staging, ext_map(c), s), "download unpack");
         c->launches += 1;
         GSPH_CK(c, cudaMemcpyAsync(ptrs[k], c->staging, comps[k] * c->a.n * sizeof(float), cudaMemcpyDeviceToHost, s),
                 "download copy");
@@ -441,16 +515,16 @@ int gsph_upload_pos64(gsph_ctx* c, const double* pos, void* stream) {
     if (!pos) return fail(c, GSPH_E_INVALID, "pos is NULL");
     cudaStream_t s = as_stream(stream);
     GSPH_CK(c, cudaMemcpyAsync(c->staging64, pos, 3 * c->a.n * sizeof(double), cudaMemcpyHostToDevice, s), "upload copy");
-    GSPH_CK(c, launch_pack_pos64(c->a, c->staging64, s), "upload pack");
+    GSPH_CK(c, launch_pack_pos64(c->a, c->staging64, ext_map(c), s), "upload pack");
     c->launches += 1;
-    return GSPH_OK;
+    return reorder(c, s);
 }
 
 int gsph_download_pos64(gsph_ctx* c, double* pos, void* stream) {
     if (!c) return GSPH_E_INVALID;
     if (!pos) return fail(c, GSPH_E_INVALID, "pos is NULL");
     cudaStream_t s = as_stream(stream);
-    GSPH_CK(c, launch_unpack_pos64(c->a, c->staging64, s), "download unpack");
+    GSPH_CK(c, launch_unpack_pos64(c->a, c->staging64, ext_map(c), s), "download unpack");
     c->launches += 1;
     GSPH_CK(c, cudaMemcpyAsync(pos, c->staging64, 3 * c->a.n * sizeof(double), cudaMemcpyDeviceToHost, s), "download copy");
     return check_status(c, s);
@@ -526,8 +600,13 @@ int gsph_step(gsph_ctx* c, int32_t nsteps, void* stream) {
         c->graph_slots = slots;
     }
     for (int32_t k = 0; k < nsteps; ++k) {
+        if (c->L.cull && c->opt.resort_interval > 0 && c->steps_since_sort >= c->opt.resort_interval) {
+            const int rc = reorder(c, s);  // permutes in place: the graph's pointers stay valid
+            if (rc != GSPH_OK) return rc;
+        }
         GSPH_CK(c, cudaGraphLaunch(c->graph_exec, s), "graph launch");
         c->launches += c->graph_kernels;
+        c->steps_since_sort += 1;
     }
     for (int k = 0; k < GSPH_KSLOTS; ++k)
         if (c->graph_slots >> k & 1u) c->pending[k] = true;
@@ -568,6 +647,11 @@ int gsph_diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream
     }
     out->mass = h[10];
     return GSPH_OK;
+}
+
+int gsph_reorder(gsph_ctx* c, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    return reorder(c, as_stream(stream));
 }
 
 int gsph_size(gsph_ctx* c, int64_t* n) {

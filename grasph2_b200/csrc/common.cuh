@@ -36,6 +36,7 @@ struct DevParams {
     float cw_n;
     float const_acc[3], box_min[3], box_max[3], box_refl;
     float balsara_floor;        // 1e-4 c / h of balsaraSwitch (src/sph/models.h:191)
+    double eps2_d, G_d;         // FP64 copies for the diagnostics
 };
 
 __host__ __device__ inline bool has(const DevParams& p, uint32_t f) { return (p.flags & f) != 0; }
@@ -57,6 +58,7 @@ struct DevArrays {
     float4* jA;       // j-record: sigma/rho^2 (xx, yy, zz, xy)
     float4* jB;       // j-record: sigma/rho^2 (xz, yz), balsara, 0
     float* part;      // j-split partial sums [segment][component][n_pad]
+    float* gpart;     // gravity partial sums of the culled path [segment][component][n_pad]
     float* dt_state;  // variable step: [0] current, [1] next (float bit patterns, positive)
     double* diag;     // diagnostics scratch
     int* status;      // device status word (0 = ok)

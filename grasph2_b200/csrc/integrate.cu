@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag(DevArrays a, DevParams p,
     }
     // pair potential: -G m_i sum_{j>i} m_j / sqrt(r^2 + eps^2), j-tiles of blockDim through shared memory
     if (has(p, GSPH_SELF_GRAVITY)) {
-        const double eps2 = static_cast<double>(p.eps2);
+        const double eps2 = p.eps2_d;
         double phi = 0.0;
         const int64_t j_first = static_cast<int64_t>(blockIdx.x) * blockDim.x;  // j > i needs j >= block start
         for (int64_t t0 = j_first; t0 < a.n; t0 += blockDim.x) {
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag(DevArrays a, DevParams p,
                 }
             }
         }
-        f[1] = -static_cast<double>(p.G) * mi * phi;
+        f[1] = -p.G_d * mi * phi;
     }
     for (int k = 0; k < kDiagFields; ++k) {
         const double s = block_sum(f[k], red);
@@ -252,83 +252,89 @@ __global__ void k_diag_reduce(DevArrays a, int nblocks, double* out) {
 
 // ---- host layout <-> device layout ------------------------------------------------------------
 // attribute ids follow the bit order of GSPH_POS ... GSPH_MAXVSIG
-__global__ void k_pack(DevArrays a, int attr, const float* __restrict__ src) {
+// `ext` maps the device slot i to the caller's particle index e (identity when null); the staging
+// buffer holds the attribute in the caller's order and layout (k components per particle)
+__global__ void k_pack(DevArrays a, int attr, const float* __restrict__ src, const int* __restrict__ ext) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t np = a.n_pad;
+    const int64_t e = ext ? ext[i] : i;
     switch (attr) {
         case 0: {  // POS
-            const float x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+            const float x = src[3 * e], y = src[3 * e + 1], z = src[3 * e + 2];
             a.pos64[i] = x; a.pos64[np + i] = y; a.pos64[2 * np + i] = z;
             float4 q = a.posm[i];
             q.x = x; q.y = y; q.z = z;
             a.posm[i] = q;
             break;
         }
-        case 1: { float4 q = a.posm[i]; q.w = src[i]; a.posm[i] = q; break; }  // MASS
-        case 2: { float4 q = a.velrho[i]; q.x = src[3 * i]; q.y = src[3 * i + 1]; q.z = src[3 * i + 2]; a.velrho[i] = q; break; }
-        case 3: { float4 q = a.acc[i]; q.x = src[3 * i]; q.y = src[3 * i + 1]; q.z = src[3 * i + 2]; a.acc[i] = q; break; }
-        case 4: a.balsara[i] = src[i]; break;
-        case 5: a.xvel[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f); break;
-        case 6: { float4 q = a.velrho[i]; q.w = src[i]; a.velrho[i] = q; break; }
-        case 7: a.rhodot[i] = src[i]; break;
+        case 1: { float4 q = a.posm[i]; q.w = src[e]; a.posm[i] = q; break; }  // MASS
+        case 2: { float4 q = a.velrho[i]; q.x = src[3 * e]; q.y = src[3 * e + 1]; q.z = src[3 * e + 2]; a.velrho[i] = q; break; }
+        case 3: { float4 q = a.acc[i]; q.x = src[3 * e]; q.y = src[3 * e + 1]; q.z = src[3 * e + 2]; a.acc[i] = q; break; }
+        case 4: a.balsara[i] = src[e]; break;
+        case 5: a.xvel[i] = make_float4(src[3 * e], src[3 * e + 1], src[3 * e + 2], 0.0f); break;
+        case 6: { float4 q = a.velrho[i]; q.w = src[e]; a.velrho[i] = q; break; }
+        case 7: a.rhodot[i] = src[e]; break;
         case 8:
         case 9: {  // DSTRESS / DSTRESS_DT: 9 row-major values, symmetrised
-            const float* m = src + 9 * i;
+            const float* m = src + 9 * e;
             const float4 A = make_float4(m[0], m[4], m[8], 0.5f * (m[1] + m[3]));
             const float4 B = make_float4(0.5f * (m[2] + m[6]), 0.5f * (m[5] + m[7]), 0.0f, 0.0f);
             if (attr == 8) { a.sA[i] = A; a.sB[i] = B; }
             else { a.dA[i] = A; a.dB[i] = B; }
             break;
         }
-        case 10: { float4 q = a.acc[i]; q.w = src[i]; a.acc[i] = q; break; }
+        case 10: { float4 q = a.acc[i]; q.w = src[e]; a.acc[i] = q; break; }
         default: break;
     }
 }
 
-__global__ void k_unpack(DevArrays a, int attr, float* __restrict__ dst) {
+__global__ void k_unpack(DevArrays a, int attr, float* __restrict__ dst, const int* __restrict__ ext) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    const int64_t e = ext ? ext[i] : i;
     switch (attr) {
-        case 0: { const float4 q = a.posm[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
-        case 1: dst[i] = a.posm[i].w; break;
-        case 2: { const float4 q = a.velrho[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
-        case 3: { const float4 q = a.acc[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
-        case 4: dst[i] = a.balsara[i]; break;
-        case 5: { const float4 q = a.xvel[i]; dst[3 * i] = q.x; dst[3 * i + 1] = q.y; dst[3 * i + 2] = q.z; break; }
-        case 6: dst[i] = a.velrho[i].w; break;
-        case 7: dst[i] = a.rhodot[i]; break;
+        case 0: { const float4 q = a.posm[i]; dst[3 * e] = q.x; dst[3 * e + 1] = q.y; dst[3 * e + 2] = q.z; break; }
+        case 1: dst[e] = a.posm[i].w; break;
+        case 2: { const float4 q = a.velrho[i]; dst[3 * e] = q.x; dst[3 * e + 1] = q.y; dst[3 * e + 2] = q.z; break; }
+        case 3: { const float4 q = a.acc[i]; dst[3 * e] = q.x; dst[3 * e + 1] = q.y; dst[3 * e + 2] = q.z; break; }
+        case 4: dst[e] = a.balsara[i]; break;
+        case 5: { const float4 q = a.xvel[i]; dst[3 * e] = q.x; dst[3 * e + 1] = q.y; dst[3 * e + 2] = q.z; break; }
+        case 6: dst[e] = a.velrho[i].w; break;
+        case 7: dst[e] = a.rhodot[i]; break;
         case 8:
         case 9: {
             const float4 A = (attr == 8) ? a.sA[i] : a.dA[i];
             const float4 B = (attr == 8) ? a.sB[i] : a.dB[i];
-            float* m = dst + 9 * i;
+            float* m = dst + 9 * e;
             m[0] = A.x; m[1] = A.w; m[2] = B.x;
             m[3] = A.w; m[4] = A.y; m[5] = B.y;
             m[6] = B.x; m[7] = B.y; m[8] = A.z;
             break;
         }
-        case 10: dst[i] = a.acc[i].w; break;
+        case 10: dst[e] = a.acc[i].w; break;
         default: break;
     }
 }
 
-__global__ void k_pack_pos64(DevArrays a, const double* __restrict__ src) {
+__global__ void k_pack_pos64(DevArrays a, const double* __restrict__ src, const int* __restrict__ ext) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t np = a.n_pad;
-    const double x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+    const int64_t e = ext ? ext[i] : i;
+    const double x = src[3 * e], y = src[3 * e + 1], z = src[3 * e + 2];
     a.pos64[i] = x; a.pos64[np + i] = y; a.pos64[2 * np + i] = z;
     float4 q = a.posm[i];
     q.x = static_cast<float>(x); q.y = static_cast<float>(y); q.z = static_cast<float>(z);
     a.posm[i] = q;
 }
 
-__global__ void k_unpack_pos64(DevArrays a, double* __restrict__ dst) {
+__global__ void k_unpack_pos64(DevArrays a, double* __restrict__ dst, const int* __restrict__ ext) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t np = a.n_pad;
-    dst[3 * i] = a.pos64[i]; dst[3 * i + 1] = a.pos64[np + i]; dst[3 * i + 2] = a.pos64[2 * np + i];
+    const int64_t e = ext ? ext[i] : i;
+    dst[3 * e] = a.pos64[i]; dst[3 * e + 1] = a.pos64[np + i]; dst[3 * e + 2] = a.pos64[2 * np + i];
 }
 
 // inert padding: zero mass, far away (never a neighbour, no gravitational pull), unit density
@@ -393,20 +399,20 @@ cudaError_t launch_diagnostics(const DevArrays& a, const DevParams& p, double ha
     return cudaGetLastError();
 }
 
-cudaError_t launch_pack(const DevArrays& a, int attr, const float* src_dev, cudaStream_t s) {
-    k_pack<<<blocks_for(a.n, 256), 256, 0, s>>>(a, attr, src_dev);
+cudaError_t launch_pack(const DevArrays& a, int attr, const float* src_dev, const int* ext, cudaStream_t s) {
+    k_pack<<<blocks_for(a.n, 256), 256, 0, s>>>(a, attr, src_dev, ext);
     return cudaGetLastError();
 }
-cudaError_t launch_unpack(const DevArrays& a, int attr, float* dst_dev, cudaStream_t s) {
-    k_unpack<<<blocks_for(a.n, 256), 256, 0, s>>>(a, attr, dst_dev);
+cudaError_t launch_unpack(const DevArrays& a, int attr, float* dst_dev, const int* ext, cudaStream_t s) {
+    k_unpack<<<blocks_for(a.n, 256), 256, 0, s>>>(a, attr, dst_dev, ext);
     return cudaGetLastError();
 }
-cudaError_t launch_pack_pos64(const DevArrays& a, const double* src_dev, cudaStream_t s) {
-    k_pack_pos64<<<blocks_for(a.n, 256), 256, 0, s>>>(a, src_dev);
+cudaError_t launch_pack_pos64(const DevArrays& a, const double* src_dev, const int* ext, cudaStream_t s) {
+    k_pack_pos64<<<blocks_for(a.n, 256), 256, 0, s>>>(a, src_dev, ext);
     return cudaGetLastError();
 }
-cudaError_t launch_unpack_pos64(const DevArrays& a, double* dst_dev, cudaStream_t s) {
-    k_unpack_pos64<<<blocks_for(a.n, 256), 256, 0, s>>>(a, dst_dev);
+cudaError_t launch_unpack_pos64(const DevArrays& a, double* dst_dev, const int* ext, cudaStream_t s) {
+    k_unpack_pos64<<<blocks_for(a.n, 256), 256, 0, s>>>(a, dst_dev, ext);
     return cudaGetLastError();
 }
 cudaError_t launch_init_padding(const DevArrays& a, cudaStream_t s) {

@@ -66,9 +66,12 @@ __device__ __forceinline__ bool in_open_closed(float x, uint32_t lo_bits, uint32
 // ================================================================================================
 // density
 // ================================================================================================
-template <bool COMP>
+// LIST: the block is one i-group of kGroup particles and visits only its near chunks (spatial.cuh)
+template <bool COMP, bool LIST>
 __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm, float* __restrict__ part,
-                                                  int64_t n_pad, int jt, int nseg, DevParams p, int* status) {
+                                                  int64_t n_pad, int jt, int nseg, DevParams p, int* status,
+                                                  const int* __restrict__ list, const int* __restrict__ count,
+                                                  int64_t list_stride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     JTilePipe<1> pipe;
     pipe.buf = reinterpret_cast<float4*>(smem_raw);
@@ -76,7 +79,13 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm
     pipe.src[0] = posm;
     pipe.jt = jt;
     pipe.status = status;
-    segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+    if (LIST) {
+        pipe.list = list + blockIdx.x * list_stride;
+        pipe.t_begin = 0;
+        pipe.t_end = count[blockIdx.x];
+    } else {
+        segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+    }
 
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const float4 pi = posm[i];
@@ -149,8 +158,9 @@ struct PairAcc {
 };
 
 // GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: the self pair must contribute 0)
-template <int PASS, int GRAV, bool SOLIDS, bool COMP>
-__global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt, int nseg) {
+template <int PASS, int GRAV, bool SOLIDS, bool COMP, bool LIST>
+__global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt, int nseg, const int* __restrict__ list,
+                                               const int* __restrict__ count, int64_t list_stride) {
     constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
     constexpr int K = popc_c(MASK);
     constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
@@ -169,7 +179,13 @@ __global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt,
     }
     pipe.jt = jt;
     pipe.status = a.status;
-    segment_tiles(a.n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+    if (LIST) {
+        pipe.list = list + blockIdx.x * list_stride;
+        pipe.t_begin = 0;
+        pipe.t_end = count[blockIdx.x];
+    } else {
+        segment_tiles(a.n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+    }
 
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const float4 pi = a.posm[i];
@@ -358,8 +374,24 @@ __device__ __forceinline__ void environment(const DevParams& p, float4 x, float4
     }
 }
 
+// gravity partials of the separate all-pairs gravity kernel (culled path), summed like seg_sum
+template <bool COMP>
+__device__ __forceinline__ float gpart_sum(const DevArrays& a, int gnseg, int64_t i, int c) {
+    const int K = COMP ? 6 : 3;
+    if (COMP) {
+        double s = 0.0;
+        for (int k = 0; k < gnseg; ++k)
+            s += static_cast<double>(a.gpart[(k * K + c) * a.n_pad + i]) +
+                 static_cast<double>(a.gpart[(k * K + 3 + c) * a.n_pad + i]);
+        return static_cast<float>(s);
+    }
+    float s = 0.0f;
+    for (int k = 0; k < gnseg; ++k) s += a.gpart[(k * K + c) * a.n_pad + i];
+    return s;
+}
+
 template <int PASS, bool GRAV, bool SOLIDS, bool COMP>
-__global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg) {
+__global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
     constexpr uint32_t MASK = field_mask<PASS, GRAV, SOLIDS>();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (PASS != PASS_VGRAD && has(p, GSPH_VARIABLE_TIMESTEP) && i == 0)
@@ -422,6 +454,11 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg) {
             ax = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GX), ax);
             ay = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GY), ay);
             az = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GZ), az);
+        }
+        if (gnseg > 0) {
+            ax = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 0), ax);
+            ay = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 1), ay);
+            az = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 2), az);
         }
         const float4 x = a.posm[i];
         environment(p, x, vi, ax, ay, az);
@@ -556,24 +593,44 @@ cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s) {
         }                                                  \
     } while (0)
 
-cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
-    const int T = 256;
-    const dim3 grid(static_cast<unsigned>(a.n_pad / T), static_cast<unsigned>(L.nseg));
-    const size_t smem = pipe_smem_bytes(1, L.jt);
+cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
+                           const SpatialArrays* sp) {
+    const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
+    const int nseg = sp ? 1 : L.nseg;
     GSPH_TIMER_MARK(t, start);
-    if (L.accum == GSPH_ACCUM_COMPENSATED)
-        k_density<true><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status);
-    else
-        k_density<false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status);
+    if (sp) {
+        const dim3 grid(static_cast<unsigned>(a.n_pad / kGroup), 1);
+        const size_t smem = pipe_smem_bytes(1, kChunk);
+        const int64_t stride = a.n_pad / kChunk;
+        if (comp)
+            k_density<true, true><<<grid, kGroup, smem, s>>>(a.posm, a.part, a.n_pad, kChunk, 1, p, a.status, sp->list,
+                                                             sp->count, stride);
+        else
+            k_density<false, true><<<grid, kGroup, smem, s>>>(a.posm, a.part, a.n_pad, kChunk, 1, p, a.status, sp->list,
+                                                              sp->count, stride);
+    } else {
+        const int T = 256;
+        const dim3 grid(static_cast<unsigned>(a.n_pad / T), static_cast<unsigned>(L.nseg));
+        const size_t smem = pipe_smem_bytes(1, L.jt);
+        if (comp)
+            k_density<true, false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status, nullptr,
+                                                          nullptr, 0);
+        else
+            k_density<false, false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status, nullptr,
+                                                           nullptr, 0);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
-    if (L.accum == GSPH_ACCUM_COMPENSATED)
-        k_density_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg);
+    if (comp)
+        k_density_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, nseg);
     else
-        k_density_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg);
+        k_density_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, nseg);
     return cudaGetLastError();
 }
+
+cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                                    const KTimer* t);
 
 cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s) {
     k_prepare<<<blocks_for(a.n, 256), 256, 0, s>>>(a, p);
@@ -582,71 +639,114 @@ cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t 
 
 namespace {
 template <int PASS, int GRAV, bool SOLIDS, bool COMP>
-cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
+                    const SpatialArrays* sp, const KTimer* tg) {
     constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
+    int gnseg = 0;
+    if (sp) {
+        // SPH terms over the near-chunk lists; gravity (acceleration passes) from the all-pairs kernel
+        const size_t smem = pipe_smem_bytes(NS, kChunk);
+        GSPH_TIMER_MARK(t, start);
+        k_pairs<PASS, 0, SOLIDS, COMP, true><<<static_cast<unsigned>(a.n_pad / kGroup), kGroup, smem, s>>>(
+            a, p, kChunk, 1, sp->list, sp->count, a.n_pad / kChunk);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        GSPH_TIMER_MARK(t, stop);
+        if (PASS != PASS_VGRAD && GRAV != 0) {
+            e = launch_gravity_partials(a, p, L, s, tg);
+            if (e != cudaSuccess) return e;
+            gnseg = L.grav_nseg;
+        }
+        k_pairs_finish<PASS, false, SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 1, gnseg);
+        return cudaGetLastError();
+    }
     const size_t smem = pipe_smem_bytes(NS, L.jt);
-    auto kern = k_pairs<PASS, GRAV, SOLIDS, COMP>;
+    auto kern = k_pairs<PASS, GRAV, SOLIDS, COMP, false>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
     }
     const dim3 grid(static_cast<unsigned>(a.n_pad / L.threads), static_cast<unsigned>(L.nseg));
     GSPH_TIMER_MARK(t, start);
-    kern<<<grid, L.threads, smem, s>>>(a, p, L.jt, L.nseg);
+    kern<<<grid, L.threads, smem, s>>>(a, p, L.jt, L.nseg, nullptr, nullptr, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
-    k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg);
+    k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg, 0);
     return cudaGetLastError();
 }
 
 template <int PASS, int GRAV>
-cudaError_t pairs_g(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+cudaError_t pairs_g(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
+                    const SpatialArrays* sp, const KTimer* tg) {
     const bool solids = has(p, GSPH_SOLIDS);
     const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
     if (solids)
-        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t) : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t);
-    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t) : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t);
+        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t, sp, tg)
+                    : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t, sp, tg);
+    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t, sp, tg)
+                : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t, sp, tg);
 }
 }  // namespace
 
 cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                         const KTimer* t) {
+                         const KTimer* t, const SpatialArrays* sp, const KTimer* tg) {
     const int grav = !has(p, GSPH_SELF_GRAVITY) ? 0 : (p.eps2 > 0.0f ? 1 : 2);
+    if (sp) {  // the culled kernels carry no gravity; any nonzero GRAV just requests the gravity pass
+        switch (pass) {
+            case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, sp, tg);
+            case PASS_ACC:
+                return grav ? pairs_g<PASS_ACC, 1>(a, p, L, s, t, sp, tg) : pairs_g<PASS_ACC, 0>(a, p, L, s, t, sp, tg);
+            default:
+                return grav ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t, sp, tg)
+                            : pairs_g<PASS_FUSED, 0>(a, p, L, s, t, sp, tg);
+        }
+    }
     switch (pass) {
-        case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t);
+        case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, nullptr, nullptr);
         case PASS_ACC:
-            return grav == 0 ? pairs_g<PASS_ACC, 0>(a, p, L, s, t)
-                             : (grav == 1 ? pairs_g<PASS_ACC, 1>(a, p, L, s, t) : pairs_g<PASS_ACC, 2>(a, p, L, s, t));
+            return grav == 0 ? pairs_g<PASS_ACC, 0>(a, p, L, s, t, nullptr, nullptr)
+                             : (grav == 1 ? pairs_g<PASS_ACC, 1>(a, p, L, s, t, nullptr, nullptr)
+                                          : pairs_g<PASS_ACC, 2>(a, p, L, s, t, nullptr, nullptr));
         default:
-            return grav == 0 ? pairs_g<PASS_FUSED, 0>(a, p, L, s, t)
-                             : (grav == 1 ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t)
-                                          : pairs_g<PASS_FUSED, 2>(a, p, L, s, t));
+            return grav == 0 ? pairs_g<PASS_FUSED, 0>(a, p, L, s, t, nullptr, nullptr)
+                             : (grav == 1 ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t, nullptr, nullptr)
+                                          : pairs_g<PASS_FUSED, 2>(a, p, L, s, t, nullptr, nullptr));
     }
 }
 
 namespace {
 template <int I, int GRAV, bool COMP>
-cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
+                      bool finish) {
     const int T = L.grav_threads;
     const dim3 grid(static_cast<unsigned>(a.n_pad / (static_cast<int64_t>(T) * I)), static_cast<unsigned>(L.grav_nseg));
-    const size_t smem = pipe_smem_bytes(1, L.jt);
+    const size_t smem = pipe_smem_bytes(1, L.grav_jt);
     GSPH_TIMER_MARK(t, start);
-    k_gravity<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.grav_nseg, p.eps2, a.status);
+    k_gravity<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, finish ? a.part : a.gpart, a.n_pad, L.grav_jt, L.grav_nseg,
+                                                    p.eps2, a.status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
+    if (!finish) return cudaSuccess;
     k_gravity_finish<COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.grav_nseg);
     return cudaGetLastError();
 }
 template <int GRAV, bool COMP>
-cudaError_t gravity_i(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
+cudaError_t gravity_i(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
+                      bool finish) {
     switch (L.grav_ipt) {
-        case 1: return gravity_t<1, GRAV, COMP>(a, p, L, s, t);
-        case 2: return gravity_t<2, GRAV, COMP>(a, p, L, s, t);
-        case 8: return gravity_t<8, GRAV, COMP>(a, p, L, s, t);
-        default: return gravity_t<4, GRAV, COMP>(a, p, L, s, t);
+        case 1: return gravity_t<1, GRAV, COMP>(a, p, L, s, t, finish);
+        case 2: return gravity_t<2, GRAV, COMP>(a, p, L, s, t, finish);
+        case 8: return gravity_t<8, GRAV, COMP>(a, p, L, s, t, finish);
+        default: return gravity_t<4, GRAV, COMP>(a, p, L, s, t, finish);
     }
+}
+cudaError_t gravity_any(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
+                        bool finish) {
+    const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
+    if (p.eps2 > 0.0f) return comp ? gravity_i<1, true>(a, p, L, s, t, finish) : gravity_i<1, false>(a, p, L, s, t, finish);
+    return comp ? gravity_i<2, true>(a, p, L, s, t, finish) : gravity_i<2, false>(a, p, L, s, t, finish);
 }
 }  // namespace
 
@@ -657,8 +757,12 @@ cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch&
         else k_gravity_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 0);
         return cudaGetLastError();
     }
-    if (p.eps2 > 0.0f) return comp ? gravity_i<1, true>(a, p, L, s, t) : gravity_i<1, false>(a, p, L, s, t);
-    return comp ? gravity_i<2, true>(a, p, L, s, t) : gravity_i<2, false>(a, p, L, s, t);
+    return gravity_any(a, p, L, s, t, true);
+}
+
+cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                                    const KTimer* t) {
+    return gravity_any(a, p, L, s, t, false);
 }
 
 // ---- FP32 FFMA throughput probe (roofline denominator) -------------------------------------------
@@ -710,15 +814,26 @@ size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad) {
     return k * mult * static_cast<size_t>(n_pad);
 }
 
-int kernels_per_derivatives(const DevParams& p) {
-    if (!has(p, GSPH_SPH)) return 2;
-    int k = 0;
-    if (!has(p, GSPH_INTEGRATE_DENSITY)) k += 2;
-    else k += 1;  // prepare
-    const bool vgrad = has(p, GSPH_SOLIDS) || has(p, GSPH_INTEGRATE_DENSITY) || has(p, GSPH_BALSARA_SWITCH);
-    if (vgrad && has(p, GSPH_BALSARA_SWITCH)) k += 4;
-    else k += 2;
-    return k;
+int gravity_blocks_per_sm(int ipt, int threads, int jt, bool comp) {
+    const size_t smem = pipe_smem_bytes(1, jt);
+    int nb = 0;
+    cudaError_t e = cudaSuccess;
+#define GSPH_OCC(I)                                                                                      \
+    e = comp ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gravity<I, 1, true>, threads, smem)  \
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_gravity<I, 1, false>, threads, smem)
+    switch (ipt) {
+        case 1: GSPH_OCC(1); break;
+        case 2: GSPH_OCC(2); break;
+        case 8: GSPH_OCC(8); break;
+        default: GSPH_OCC(4); break;
+    }
+#undef GSPH_OCC
+    return (e == cudaSuccess && nb > 0) ? nb : 4;
+}
+
+size_t gravity_partial_floats(const Launch& L, int64_t n_pad) {
+    const int mult = (L.accum == GSPH_ACCUM_COMPENSATED) ? 2 : 1;
+    return static_cast<size_t>(3) * mult * static_cast<size_t>(std::max(L.grav_nseg, 1)) * static_cast<size_t>(n_pad);
 }
 
 }  // namespace gsph

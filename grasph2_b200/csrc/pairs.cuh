@@ -13,6 +13,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "spatial.cuh"
 
 namespace gsph {
 
@@ -23,8 +24,11 @@ struct JTilePipe {
     uint64_t* bar;        // shared: [2]
     const float4* src[NS];
     int jt;
-    int64_t t_begin, t_end;
+    int64_t t_begin, t_end;  // tiles t_begin .. t_end-1, or positions of `list` when it is set
+    const int* list = nullptr;
     int* status;
+
+    __device__ __forceinline__ int64_t tile_at(int64_t k) const { return list ? list[k] : k; }
 
     __device__ __forceinline__ void issue(int b, int64_t t) {
         mbar_expect_tx(&bar[b], static_cast<uint32_t>(NS * jt * sizeof(float4)));
@@ -43,8 +47,8 @@ struct JTilePipe {
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            if (t_begin < t_end) issue(0, t_begin);
-            if (t_begin + 1 < t_end) issue(1, t_begin + 1);
+            if (t_begin < t_end) issue(0, tile_at(t_begin));
+            if (t_begin + 1 < t_end) issue(1, tile_at(t_begin + 1));
         }
     }
 
@@ -62,7 +66,7 @@ struct JTilePipe {
             const float4* stage = buf + static_cast<int64_t>(b) * NS * jt;
             body(stage);
             __syncthreads();
-            if (threadIdx.x == 0 && t + 2 < t_end) issue(b, t + 2);
+            if (threadIdx.x == 0 && t + 2 < t_end) issue(b, tile_at(t + 2));
         }
     }
 
@@ -140,25 +144,30 @@ cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s);
 
 // host launchers (pairs.cu)
 struct Launch {
+    bool cull;       // SPH passes over near-chunk lists (spatial.cuh) + separate all-pairs gravity
     int threads;     // threads per CTA of the SPH pair kernels
     int jt;          // j-tile
     int nseg;        // j-split of the SPH pair kernels
     int grav_threads;
     int grav_ipt;    // i per thread of the gravity kernel
+    int grav_jt;     // j-tile of the gravity kernel
     int grav_nseg;
     int accum;       // GSPH_ACCUM_*
 };
 
 cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                           const KTimer* t = nullptr);
+                           const KTimer* t = nullptr, const SpatialArrays* sp = nullptr);
 cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s);
+// With `sp`, the SPH terms come from the near-chunk lists and the gravity of an acceleration pass
+// from a separate all-pairs gravity kernel (timer `tg`) whose partials the finish kernel adds.
 cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                         const KTimer* t = nullptr);
+                         const KTimer* t = nullptr, const SpatialArrays* sp = nullptr, const KTimer* tg = nullptr);
 cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                            const KTimer* t = nullptr);
 cudaError_t launch_fp32_peak(int sm_count, int iters, float* sink, cudaStream_t s);
 int64_t fp32_peak_flops(int sm_count, int iters);
 size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad);
-int kernels_per_derivatives(const DevParams& p);
+size_t gravity_partial_floats(const Launch& L, int64_t n_pad);
+int gravity_blocks_per_sm(int ipt, int threads, int jt, bool comp);
 
 }  // namespace gsph

@@ -163,7 +163,12 @@ typedef struct gsph_options {
     int32_t i_per_thread;    /* register blocking of the gravity-only kernel: 1, 2, 4 or 8 (0 = default) */
     int32_t threads;         /* threads per CTA of the pair kernels (0 = default) */
     int32_t check_finite;    /* nonzero: scan inputs at upload for NaN/Inf and fail with GSPH_E_NUMERIC */
-    int32_t reserved[10];
+    int32_t no_cull;         /* 0 (default): particles are kept in Morton order on the device and the SPH
+                                passes visit only chunks within H of each particle group, gravity covering
+                                all pairs in its own kernel; nonzero: every SPH pass sweeps all N^2 pairs */
+    int32_t resort_interval; /* re-sort the Morton order every this many gsph_step steps (0: only when
+                                positions are uploaded) */
+    int32_t reserved[8];
 } gsph_options;
 
 int gsph_options_defaults(gsph_options* o);
@@ -178,7 +183,9 @@ int gsph_destroy(gsph_ctx* ctx);
 
 /* Copy host attributes -> device (pb = hostBuffer, src/particles/Device_base.h:163-181).
  * `attr_mask` picks the attributes; DSTRESS is symmetrised on upload (the kernels store the six
- * independent components). Positions are also kept as an FP64 master copy on the device. */
+ * independent components). Positions are also kept as an FP64 master copy on the device. The
+ * device may hold the particles in another order (see gsph_options.no_cull); every transfer uses the
+ * caller's order. */
 int gsph_upload(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
 /* Copy device -> host for the attributes in `attr_mask`; synchronises `stream`. */
 int gsph_download(gsph_ctx* ctx, uint32_t attr_mask, gsph_host_particles* dst, void* stream);
@@ -223,6 +230,9 @@ int gsph_diagnostics(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stre
 
 /* Number of particles of the context. */
 int gsph_size(gsph_ctx* ctx, int64_t* n);
+/* Re-sort the device-side particle order along a Morton curve of the current positions (a no-op
+ * with no_cull set). Results do not depend on the order except for floating-point summation order. */
+int gsph_reorder(gsph_ctx* ctx, void* stream);
 /* Text of the last failure on `ctx` (or of the last failed gsph_create when ctx is NULL). */
 const char* gsph_last_error(gsph_ctx* ctx);
 /* Device pointers of the resident arrays, for zero-copy callers (read-only view). */

@@ -76,8 +76,8 @@ def oracle_steps(oracle, params, nsteps):
     return run
 
 
-def gpu_derivatives(params, state, accum="plain", **opt):
-    with DeviceParticleBuffer(params, state["mass"].shape[0], make_options(accum=accum, **opt)) as pb:
+def gpu_derivatives(params, state, accum="plain", cull=True, **opt):
+    with DeviceParticleBuffer(params, state["mass"].shape[0], make_options(accum=accum, cull=cull, **opt)) as pb:
         pb.upload(state)
         pb.compute_derivatives()
         return pb.download()
@@ -88,16 +88,17 @@ def check_derivatives(got, want, sens, params, what, rows=slice(None)):
         check_within(got[k][rows], want[k][rows], sens[k][rows], tol, "%s %s" % (what, k))
 
 
+@pytest.mark.parametrize("cull", [True, False], ids=["culled", "allpairs"])
 @pytest.mark.parametrize("accum", ["plain", "compensated"])
 @pytest.mark.parametrize("name", list(ref_variants.VARIANTS))
-def test_golden_derivatives(oracle, name, accum):
+def test_golden_derivatives(oracle, name, accum, cull):
     """computeDerivatives vs the reference's own FP64 results (tests/golden)."""
     z = load_golden(name)
     p = variant_params(name)
     st = golden_state(z, "in_")
     _, sens = fp32_sensitivity(oracle_derivs(oracle, p), st)
-    got = gpu_derivatives(p, st, accum)
-    check_derivatives(got, golden_state(z, "d64_"), sens, p, "%s/%s" % (name, accum))
+    got = gpu_derivatives(p, st, accum, cull)
+    check_derivatives(got, golden_state(z, "d64_"), sens, p, "%s/%s/cull=%s" % (name, accum, cull))
 
 
 @pytest.mark.parametrize("accum", ["plain", "compensated"])
@@ -136,15 +137,17 @@ def _edge_state(name, n, seed):
     return f32_exact(st)
 
 
-@pytest.mark.parametrize("n", [1, 2, 255, 256, 257, 1000, 1023, 1025, 3000])
-@pytest.mark.parametrize("name", ["nbody", "fluid", "solid", "solid_mc"])
+@pytest.mark.parametrize("n", [1, 2, 63, 64, 65, 127, 128, 129, 255, 256, 257, 1000, 1023, 1025, 3000])
+@pytest.mark.parametrize("name", ["nbody", "fluid", "solid", "solid_mc", "fluid_full"])
 def test_edge_sizes_vs_oracle(oracle, name, n):
-    """Every N works (the reference's tile loop needs N % 256 == 0, algorithms.h:285-301)."""
+    """Every N works (the reference's tile loop needs N % 256 == 0, algorithms.h:285-301), with and
+    without the chunk culling (chunks of 64, groups of 128)."""
     p = variant_params(name)
     st = _edge_state(name, n, seed=n)
     ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st)
-    got = gpu_derivatives(p, st)
-    check_derivatives(got, ref, sens, p, "%s/n=%d" % (name, n))
+    for cull in (True, False):
+        got = gpu_derivatives(p, st, cull=cull)
+        check_derivatives(got, ref, sens, p, "%s/n=%d/cull=%s" % (name, n, cull))
 
 
 @pytest.mark.parametrize("opt", [
@@ -158,8 +161,9 @@ def test_launch_shapes_vs_oracle(oracle, name, opt):
     st = _edge_state(name, 2500, seed=11)
     ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st)
     for accum in ("plain", "compensated"):
-        got = gpu_derivatives(p, st, accum, **opt)
-        check_derivatives(got, ref, sens, p, "%s/%s/%s" % (name, opt, accum))
+        for cull in (True, False):
+            got = gpu_derivatives(p, st, accum, cull, **opt)
+            check_derivatives(got, ref, sens, p, "%s/%s/%s/cull=%s" % (name, opt, accum, cull))
 
 
 def test_config0_one_step_vs_oracle(oracle):
@@ -303,6 +307,35 @@ def test_profile_and_launch_count():
         pb.step(1)
         pb.profile_collect()
         pr = pb.profile_read()
-        assert pb.launch_count() - c0 == 5  # density + finish, fused pairs + finish, leapfrog
-        assert pr["pairs"][1] == 1 and pr["pairs"][0] > 0 and pr["density"][1] == 1
-        assert pr["step"][0] >= pr["pairs"][0]
+        # chunk bounds + lists, density + finish, SPH pass + gravity + finish, leapfrog
+        assert pb.launch_count() - c0 == 8
+        assert pr["pairs"][1] == 1 and pr["pairs"][0] > 0 and pr["density"][1] == 1 and pr["gravity"][1] == 1
+        assert pr["step"][0] >= pr["pairs"][0] + pr["gravity"][0]
+
+
+def test_device_order_is_invisible():
+    """The Morton order on the device never shows: every transfer is in the caller's order."""
+    p = variant_params("solid_mc")
+    st = _edge_state("solid_mc", 3001, seed=21)
+    with DeviceParticleBuffer(p, 3001) as pb:
+        pb.upload(st)
+        back = pb.download()
+        for k in ("pos", "mass", "vel", "density", "dstress"):
+            np.testing.assert_array_equal(back[k], st[k].astype(np.float32), err_msg=k)
+        np.testing.assert_array_equal(pb.download_pos64(), st["pos"])
+        pb.lib.gsph_reorder(pb.handle, None)
+        np.testing.assert_array_equal(pb.download()["vel"], st["vel"].astype(np.float32))
+
+
+def test_periodic_resort_matches(oracle):
+    """Re-sorting during a run changes only the summation order."""
+    p = variant_params("solid")
+    st = _edge_state("solid", 2000, seed=22)
+    out = []
+    for interval in (0, 1):
+        with DeviceParticleBuffer(p, 2000, make_options(resort_interval=interval)) as pb:
+            pb.upload(st)
+            pb.step(3)
+            out.append(pb.download())
+    _, sens = fp32_sensitivity(oracle_steps(oracle, p, 3), st)
+    check_within(out[1]["vel"], out[0]["vel"], sens["vel"], TOL_STEP, "resorted vel")
