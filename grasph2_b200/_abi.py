@@ -65,7 +65,8 @@ class GsphOptions(ctypes.Structure):
     _fields_ = [
         ("accum", ctypes.c_int32), ("j_split", ctypes.c_int32), ("j_tile", ctypes.c_int32),
         ("i_per_thread", ctypes.c_int32), ("threads", ctypes.c_int32), ("check_finite", ctypes.c_int32),
-        ("no_cull", ctypes.c_int32), ("resort_interval", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
+        ("no_cull", ctypes.c_int32), ("resort_interval", ctypes.c_int32), ("scalar_fp32", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 

@@ -375,6 +375,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     L.nseg = o.j_split ? std::min(o.j_split, cap) : pick_split(n_pad / L.threads, c->sm_count * 4, cap);
     // gravity kernel: the most i-blocking (and the largest j-tile) that still gives two waves of CTAs
     L.grav_threads = 128;
+    L.grav_x2 = !o.scalar_fp32;
     {
         const bool comp = o.accum == GSPH_ACCUM_COMPENSATED;
         const int ipts[3] = {4, 2, 1};

@@ -471,6 +471,105 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
 // ================================================================================================
 // pure gravity (ENABLE_SPH off): I i-particles per thread share every j read from shared memory
 // ================================================================================================
+// Paired FP32 (PTX ISA 8.6, sm_100+): one add/sub/mul/fma.rn.f32x2 instruction performs the same
+// IEEE single-precision operation on two lanes of a 64-bit register pair, so two i-particles advance
+// per issued instruction with bit-identical results to the scalar form.
+__device__ __forceinline__ uint64_t u64_of(float2 v) { return *reinterpret_cast<uint64_t*>(&v); }
+__device__ __forceinline__ float2 f2_of(uint64_t v) { return *reinterpret_cast<float2*>(&v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(u64_of(a)), "l"(u64_of(b)), "l"(u64_of(c)));
+    return f2_of(d);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(u64_of(a)), "l"(u64_of(b)));
+    return f2_of(d);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(u64_of(a)), "l"(u64_of(b)));
+    return f2_of(d);
+}
+
+// I (even) i-particles per thread in I/2 register pairs; same arithmetic order as k_gravity
+template <int I, int GRAV, bool COMP>
+__global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ posm, float* __restrict__ part,
+                                                     int64_t n_pad, int jt, int nseg, float eps2, int* status) {
+    constexpr int P = I / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    JTilePipe<1> pipe;
+    pipe.buf = reinterpret_cast<float4*>(smem_raw);
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * jt * sizeof(float4));
+    pipe.src[0] = posm;
+    pipe.jt = jt;
+    pipe.status = status;
+    segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
+
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x * I + threadIdx.x;
+    float2 X[P], Y[P], Z[P], AX[P], AY[P], AZ[P], CX[P], CY[P], CZ[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        const float4 a = posm[base + static_cast<int64_t>(2 * k) * blockDim.x];
+        const float4 b = posm[base + static_cast<int64_t>(2 * k + 1) * blockDim.x];
+        X[k] = make_float2(a.x, b.x); Y[k] = make_float2(a.y, b.y); Z[k] = make_float2(a.z, b.z);
+        AX[k] = AY[k] = AZ[k] = make_float2(0.0f, 0.0f);
+        CX[k] = CY[k] = CZ[k] = make_float2(0.0f, 0.0f);
+    }
+    const float2 E2 = make_float2(eps2, eps2);
+
+    pipe.start();
+    pipe.run([&](const float4* J) {
+        float2 TX[P], TY[P], TZ[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) TX[k] = TY[k] = TZ[k] = make_float2(0.0f, 0.0f);
+#pragma unroll 4
+        for (int j = 0; j < jt; ++j) {
+            const float4 q = J[j];
+            const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y), qz = make_float2(q.z, q.z),
+                         qm = make_float2(q.w, q.w);
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                const float2 dx = sub2(qx, X[k]), dy = sub2(qy, Y[k]), dz = sub2(qz, Z[k]);
+                const float2 r2 = fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, E2)));
+                float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
+                const float2 s = mul2(mul2(qm, inv), mul2(inv, inv));
+                if (COMP) {
+                    TX[k] = fma2(dx, s, TX[k]); TY[k] = fma2(dy, s, TY[k]); TZ[k] = fma2(dz, s, TZ[k]);
+                } else {
+                    AX[k] = fma2(dx, s, AX[k]); AY[k] = fma2(dy, s, AY[k]); AZ[k] = fma2(dz, s, AZ[k]);
+                }
+            }
+        }
+        if (COMP) {
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                fold(AX[k].x, CX[k].x, TX[k].x); fold(AX[k].y, CX[k].y, TX[k].y);
+                fold(AY[k].x, CY[k].x, TY[k].x); fold(AY[k].y, CY[k].y, TY[k].y);
+                fold(AZ[k].x, CZ[k].x, TZ[k].x); fold(AZ[k].y, CZ[k].y, TZ[k].y);
+            }
+        }
+    });
+
+    const int64_t seg = blockIdx.y;
+    const int K = COMP ? 6 : 3;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float* out = part + seg * K * n_pad + base + static_cast<int64_t>(2 * k + h) * blockDim.x;
+            out[0] = h ? AX[k].y : AX[k].x;
+            out[n_pad] = h ? AY[k].y : AY[k].x;
+            out[2 * n_pad] = h ? AZ[k].y : AZ[k].x;
+            if (COMP) {
+                out[3 * n_pad] = h ? CX[k].y : CX[k].x;
+                out[4 * n_pad] = h ? CY[k].y : CY[k].x;
+                out[5 * n_pad] = h ? CZ[k].y : CZ[k].x;
+            }
+        }
+    }
+}
 template <int I, int GRAV, bool COMP>
 __global__ void __launch_bounds__(128) k_gravity(const float4* __restrict__ posm, float* __restrict__ part,
                                                   int64_t n_pad, int jt, int nseg, float eps2, int* status) {
@@ -723,8 +822,17 @@ cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, c
     const dim3 grid(static_cast<unsigned>(a.n_pad / (static_cast<int64_t>(T) * I)), static_cast<unsigned>(L.grav_nseg));
     const size_t smem = pipe_smem_bytes(1, L.grav_jt);
     GSPH_TIMER_MARK(t, start);
-    k_gravity<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, finish ? a.part : a.gpart, a.n_pad, L.grav_jt, L.grav_nseg,
-                                                    p.eps2, a.status);
+    if constexpr (I >= 2) {
+        if (L.grav_x2)
+            k_gravity_x2<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, finish ? a.part : a.gpart, a.n_pad, L.grav_jt,
+                                                               L.grav_nseg, p.eps2, a.status);
+        else
+            k_gravity<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, finish ? a.part : a.gpart, a.n_pad, L.grav_jt,
+                                                            L.grav_nseg, p.eps2, a.status);
+    } else {
+        k_gravity<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, finish ? a.part : a.gpart, a.n_pad, L.grav_jt,
+                                                        L.grav_nseg, p.eps2, a.status);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);

@@ -151,6 +151,7 @@ struct Launch {
     int grav_threads;
     int grav_ipt;    // i per thread of the gravity kernel
     int grav_jt;     // j-tile of the gravity kernel
+    bool grav_x2;    // paired FP32 (f32x2) form of the gravity kernel
     int grav_nseg;
     int accum;       // GSPH_ACCUM_*
 };

@@ -168,7 +168,9 @@ typedef struct gsph_options {
                                 all pairs in its own kernel; nonzero: every SPH pass sweeps all N^2 pairs */
     int32_t resort_interval; /* re-sort the Morton order every this many gsph_step steps (0: only when
                                 positions are uploaded) */
-    int32_t reserved[8];
+    int32_t scalar_fp32;     /* nonzero: scalar FP32 gravity kernel instead of the paired f32x2 form
+                                (identical results; for comparison) */
+    int32_t reserved[7];
 } gsph_options;
 
 int gsph_options_defaults(gsph_options* o);
