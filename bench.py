@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak probe (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="particle count of the fluid / plummer workloads")
+    ap.add_argument("--no-cull", action="store_true", help="all-pairs SPH sweeps (no chunk culling)")
+    ap.add_argument("--scalar-fp32", action="store_true", help="scalar instead of paired f32x2 gravity kernel")
     return ap.parse_args()
 
 
@@ -79,18 +81,28 @@ def workload(name, n=0):
     return config2_params(), st, "Plummer sphere N-body, N=%d, a=1, eps=0.01, dt=1e-3" % n, "nbody"
 
 
-def flops_per_step(params, st, counts):
+def flops_per_step(params, st, counts, culled):
+    """Algorithmic flops of each timed kernel slot in one step. With culling, gravity is its own
+    all-pairs kernel and the SPH slots carry only the neighbour work; without it the acceleration
+    pass also carries the N^2 gravity sweep and the density pass its N^2 distance tests."""
     from grasph2_b200._abi import FLAG_BITS as F
     n = st["mass"].shape[0]
     n2 = float(n) * n
     nb = counts
     out = {}
+    grav = bool(params.flags & F["SELF_GRAVITY"])
     if params.flags & F["SPH"]:
-        if not params.flags & F["INTEGRATE_DENSITY"]:
-            out["density"] = FLOP_DENS_PAIR * n2 + FLOP_DENS_NB * nb
         solids = params.flags & F["SOLIDS"]
-        out["pairs"] = FLOP_GRAV_PAIR * n2 + (FLOP_FUSED_NB if solids else FLOP_ACC_NB) * nb
-    else:
+        per_nb = FLOP_FUSED_NB if solids else FLOP_ACC_NB
+        if not params.flags & F["INTEGRATE_DENSITY"]:
+            out["density"] = FLOP_DENS_NB * nb + (0 if culled else FLOP_DENS_PAIR * n2)
+        if culled:
+            out["pairs"] = per_nb * nb
+            if grav:
+                out["gravity"] = FLOP_GRAV_PAIR * n2
+        else:
+            out["pairs"] = per_nb * nb + (FLOP_GRAV_PAIR * n2 if grav else 0)
+    elif grav:
         out["gravity"] = FLOP_GRAV_PAIR * n2
     return out
 
@@ -299,7 +311,8 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    pb = DeviceParticleBuffer(params, n, make_options(accum=args.accum))
+    opts = dict(accum=args.accum, cull=not args.no_cull, scalar_fp32=args.scalar_fp32)
+    pb = DeviceParticleBuffer(params, n, make_options(**opts))
     pb.upload(st, stream=stream)
     pb.profile_enable(True)
     for _ in range(args.warmup):
@@ -345,7 +358,7 @@ def main():
     d2h = sum(a.nbytes for a in pinned_out.values())
     e2e_steps = 0 if args.no_e2e else max(5, min(args.steps, 50))
     pb.profile_enable(False)
-    pb2 = DeviceParticleBuffer(params, n, make_options(accum=args.accum))
+    pb2 = DeviceParticleBuffer(params, n, make_options(**opts))
     e2e_ms = 0.0
     for k in range(e2e_steps + 3 if e2e_steps else 0):
         flush.zero_()
@@ -371,8 +384,9 @@ def main():
     value = steps_total / (total_ms * 1e-3)
     ms_per_step = total_ms / args.steps
     nb = neighbour_pairs(st["pos"], params.H, dev) if (params.flags & 2) else 0
-    fl = flops_per_step(params, st, nb)
-    dominant = max(fl, key=lambda k: fl[k])
+    fl = flops_per_step(params, st, nb, culled=not args.no_cull)
+    timed = {k: prof[k][0] / prof[k][1] for k in fl if prof[k][1]}
+    dominant = max(timed, key=lambda k: timed[k]) if timed else max(fl, key=lambda k: fl[k])
     ms_dom, cnt_dom = prof[dominant]
     achieved = fl[dominant] / (ms_dom / cnt_dom * 1e-3) / 1e12 if cnt_dom else None
     pairs_per_step = flops_pairs(params, n)
@@ -386,7 +400,9 @@ def main():
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded initial conditions)",
-        "config": {"workload": desc, "n": n, "form": args.accum, "l2": "flushed between timed steps (256 MiB write)",
+        "config": {"workload": desc, "n": n, "form": args.accum, "culled": not args.no_cull,
+                   "gravity_fp32": "scalar" if args.scalar_fp32 else "f32x2",
+                   "l2": "flushed between timed steps (256 MiB write)",
                    "step": "computeDerivatives + integrate, one captured CUDA graph",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "pair_interactions_per_s": pairs_per_step * value,

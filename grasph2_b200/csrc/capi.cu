@@ -23,6 +23,8 @@ struct gsph_ctx {
     DevArrays a;
     SpatialArrays sp{};
     int64_t steps_since_sort = 0;
+    cudaStream_t side = nullptr;   // gravity runs here, concurrent with the SPH chain (culled path)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int device = 0;
     int sm_count = 148;
     std::vector<void*> allocations;
@@ -161,6 +163,12 @@ void drop_graph(gsph_ctx* c) {
 
 void release(gsph_ctx* c) {
     drop_graph(c);
+    if (c->side) cudaStreamSynchronize(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
+    c->side = nullptr;
+    c->ev_fork = c->ev_join = nullptr;
     for (auto& t : c->timers) {
         if (t.start) cudaEventDestroy(t.start);
         if (t.stop) cudaEventDestroy(t.stop);
@@ -197,11 +205,23 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
     cudaError_t e;
     if (has(p, GSPH_SPH)) {
         const SpatialArrays* sp = c->L.cull ? &c->sp : nullptr;
-        if (sp) {  // bounds of every chunk at the current positions, then each group's near chunks
+        const bool grav_kernel = sp && has(p, GSPH_SELF_GRAVITY);
+        cudaEvent_t join = nullptr;
+        if (grav_kernel) {  // fork: all-pairs gravity on the side stream, joined before the finish
+            e = cudaEventRecord(c->ev_fork, s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+            if (e == cudaSuccess) e = launch_gravity_partials(c->a, p, c->L, c->side, slot_timer(c, GSPH_KSLOT_GRAVITY));
+            if (e == cudaSuccess) e = cudaEventRecord(c->ev_join, c->side);
+            if (e != cudaSuccess) return cuda_fail(c, e, "gravity pass");
+            join = c->ev_join;
+            c->launches += 1;
+        }
+        if (sp) {  // bounds of every chunk at the current positions, each group's near chunks, work items
             e = launch_chunk_bounds(c->a, c->sp, s);
             if (e == cudaSuccess) e = launch_chunk_lists(c->a, c->sp, p.H, s);
+            if (e == cudaSuccess) e = launch_work_items(c->a, c->sp, s);
             if (e != cudaSuccess) return cuda_fail(c, e, "chunk lists");
-            c->launches += 2;
+            c->launches += 3;
         }
         if (!has(p, GSPH_INTEGRATE_DENSITY)) {
             e = launch_density(c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_DENSITY), sp);
@@ -213,20 +233,19 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
             c->launches += 1;
         }
         const bool vgrad = has(p, GSPH_SOLIDS) || has(p, GSPH_INTEGRATE_DENSITY) || has(p, GSPH_BALSARA_SWITCH);
-        const bool grav_kernel = sp && has(p, GSPH_SELF_GRAVITY);
-        const KTimer* tg = grav_kernel ? slot_timer(c, GSPH_KSLOT_GRAVITY) : nullptr;
+        const int gnseg = grav_kernel ? c->L.grav_nseg : 0;
         if (vgrad && has(p, GSPH_BALSARA_SWITCH)) {
             e = launch_pairs(PASS_VGRAD, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_VGRAD), sp);
             if (e != cudaSuccess) return cuda_fail(c, e, "velocity-gradient pass");
-            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, tg);
+            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, gnseg, join);
             if (e != cudaSuccess) return cuda_fail(c, e, "acceleration pass");
             c->launches += 4;
         } else {
-            e = launch_pairs(vgrad ? PASS_FUSED : PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, tg);
+            e = launch_pairs(vgrad ? PASS_FUSED : PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, gnseg,
+                             join);
             if (e != cudaSuccess) return cuda_fail(c, e, "pair pass");
             c->launches += 2;
         }
-        if (grav_kernel) c->launches += 1;
     } else {
         e = launch_gravity(c->a, p, c->L, s,
                            has(p, GSPH_SELF_GRAVITY) ? slot_timer(c, GSPH_KSLOT_GRAVITY) : nullptr);
@@ -415,6 +434,12 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
+        sp.item_chunks = static_cast<int>(std::max<int64_t>(4, (nchunks + kMaxItemsPerGroup - 1) / kMaxItemsPerGroup));
+        sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 1) * sizeof(int), ae));
+        // worst case fields per item: fused solids pass without gravity, compensated (x2)
+        const size_t kk = 2 * static_cast<size_t>(popc_c(field_mask<PASS_FUSED, false, true>()));
+        sp.item_part = static_cast<float*>(dalloc(c, ngroups * kMaxItemsPerGroup * kk * kGroup * sizeof(float), ae));
+        L.item_grid = c->sm_count * 6;
         sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));
@@ -444,6 +469,11 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (e == cudaSuccess) e = cudaMemset(a.status, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = launch_init_padding(a, 0);
     if (e == cudaSuccess && L.cull) e = launch_identity_order(c->sp, n_pad, 0);
+    if (e == cudaSuccess && L.cull) {
+        e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         release(c);

@@ -66,12 +66,52 @@ __device__ __forceinline__ bool in_open_closed(float x, uint32_t lo_bits, uint32
 // ================================================================================================
 // density
 // ================================================================================================
-// LIST: the block is one i-group of kGroup particles and visits only its near chunks (spatial.cuh)
-template <bool COMP, bool LIST>
+// Where the partial sums of particle i live: j-segments [seg][field][n_pad] (all-pairs kernels) or
+// work items [w][field][kGroup] (culled kernels); KK = fields per slot (2K when compensated).
+struct PartView {
+    const float* part;
+    int64_t n_pad;
+    int nseg;
+    const int* item_start;  // non-null: item layout
+    int KK;
+    __device__ __forceinline__ void range(int64_t i, int& b, int& e) const {
+        if (item_start) {
+            const int64_t g = i / kGroup;
+            b = item_start[g];
+            e = item_start[g + 1];
+        } else {
+            b = 0;
+            e = nseg;
+        }
+    }
+    __device__ __forceinline__ float at(int slot, int o, int64_t i) const {
+        if (item_start) return part[(static_cast<int64_t>(slot) * KK + o) * kGroup + (i % kGroup)];
+        return part[(static_cast<int64_t>(slot) * KK + o) * n_pad + i];
+    }
+};
+
+// one tile of the density sum: rho += m_j W~(q) over 0 < r^2 <= H^2 (self term excluded), the
+// spline prefactor applied by the finish kernel
+__device__ __forceinline__ float density_tile(const float4* __restrict__ J, int nj, float4 pi, uint32_t span,
+                                              float inv_h) {
+    float rho = 0.0f;
+#pragma unroll 8
+    for (int j = 0; j < nj; ++j) {
+        const float4 q = J[j];
+        const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        if (in_open_closed(r2, 0u, span)) {  // calcDensity: r2 <= H2 && r2 > 0 (computeDerivatives.h:72)
+            const float r = r2 * rsqrtf(r2);
+            rho = fmaf(q.w, w_poly(r * inv_h), rho);
+        }
+    }
+    return rho;
+}
+
+// all-pairs density sum: blockIdx.x = i-block, blockIdx.y = j-segment
+template <bool COMP>
 __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm, float* __restrict__ part,
-                                                  int64_t n_pad, int jt, int nseg, DevParams p, int* status,
-                                                  const int* __restrict__ list, const int* __restrict__ count,
-                                                  int64_t list_stride) {
+                                                  int64_t n_pad, int jt, int nseg, DevParams p, int* status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     JTilePipe<1> pipe;
     pipe.buf = reinterpret_cast<float4*>(smem_raw);
@@ -79,55 +119,69 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm
     pipe.src[0] = posm;
     pipe.jt = jt;
     pipe.status = status;
-    if (LIST) {
-        pipe.list = list + blockIdx.x * list_stride;
-        pipe.t_begin = 0;
-        pipe.t_end = count[blockIdx.x];
-    } else {
-        segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
-    }
-
+    segment_tiles(n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const float4 pi = posm[i];
     const uint32_t span = __float_as_uint(p.H2);
     float rho_s = 0.0f, rho_c = 0.0f;
-
     pipe.start();
     pipe.run([&](const float4* J) {
-        float rho_t = 0.0f;
-#pragma unroll 8
-        for (int j = 0; j < jt; ++j) {
-            const float4 q = J[j];
-            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            if (in_open_closed(r2, 0u, span)) {  // calcDensity: r2 <= H2 && r2 > 0
-                const float r = r2 * rsqrtf(r2);
-                rho_t = fmaf(q.w, w_poly(r * p.inv_h), rho_t);
-            }
-        }
-        if (COMP) fold(rho_s, rho_c, rho_t);
-        else rho_s += rho_t;
+        const float t = density_tile(J, jt, pi, span, p.inv_h);
+        if (COMP) fold(rho_s, rho_c, t);
+        else rho_s += t;
     });
     const int64_t seg = blockIdx.y;
     part[(seg * (COMP ? 2 : 1)) * n_pad + i] = rho_s;
     if (COMP) part[(seg * 2 + 1) * n_pad + i] = rho_c;
 }
 
-// sum the segments, apply the prefactor and the optional floor (computeDerivatives.h:85-88), then
+// culled density sum over the near-chunk work items (persistent grid)
+template <bool COMP>
+__global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restrict__ posm, DevParams p, CullView cv,
+                                                          int* status) {
+    constexpr int SJ = kStageChunks * kChunk;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ItemPipe<1> pipe;
+    pipe.buf = reinterpret_cast<float4*>(smem_raw);
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * SJ * sizeof(float4));
+    pipe.src[0] = posm;
+    pipe.status = status;
+    pipe.init();
+    const uint32_t span = __float_as_uint(p.H2);
+    const int total = cv.item_start[cv.ngroups];
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        int g, c0, c1;
+        cv.item(w, g, c0, c1);
+        const float4 pi = posm[static_cast<int64_t>(g) * kGroup + threadIdx.x];
+        float rho_s = 0.0f, rho_c = 0.0f;
+        if (!pipe.run(cv.list + static_cast<int64_t>(g) * cv.nchunks + c0, c1 - c0, [&](const float4* J, int nj) {
+                const float t = density_tile(J, nj, pi, span, p.inv_h);
+                if (COMP) fold(rho_s, rho_c, t);
+                else rho_s += t;
+            }))
+            return;
+        float* out = cv.part + static_cast<int64_t>(w) * (COMP ? 2 : 1) * kGroup + threadIdx.x;
+        out[0] = rho_s;
+        if (COMP) out[kGroup] = rho_c;
+    }
+}
+
+// sum the slots, apply the prefactor and the optional floor (computeDerivatives.h:85-88), then
 // build the j-record sigma/rho^2 of the new density
 template <bool COMP>
-__global__ void k_density_finish(DevArrays a, DevParams p, int nseg) {
+__global__ void k_density_finish(DevArrays a, DevParams p, PartView pv) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    int b, e;
+    pv.range(i, b, e);
     float rho;
     if (COMP) {
         double s = 0.0;
-        for (int k = 0; k < nseg; ++k)
-            s += static_cast<double>(a.part[(2 * k) * a.n_pad + i]) + static_cast<double>(a.part[(2 * k + 1) * a.n_pad + i]);
+        for (int k = b; k < e; ++k) s += static_cast<double>(pv.at(k, 0, i)) + static_cast<double>(pv.at(k, 1, i));
         rho = static_cast<float>(s * static_cast<double>(p.w_pref));
     } else {
         float s = 0.0f;
-        for (int k = 0; k < nseg; ++k) s += a.part[k * a.n_pad + i];
+        for (int k = b; k < e; ++k) s += pv.at(k, 0, i);
         rho = s * p.w_pref;
     }
     if (has(p, GSPH_DEAL_WITH_NO_PARTNERS) && rho < 0.001f) rho = p.rho0 * 0.01f;
@@ -157,15 +211,171 @@ struct PairAcc {
     float f[F_COUNT];
 };
 
-// GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: the self pair must contribute 0)
-template <int PASS, int GRAV, bool SOLIDS, bool COMP, bool LIST>
-__global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt, int nseg, const int* __restrict__ list,
-                                               const int* __restrict__ count, int64_t list_stride) {
+// Per-i state of the SPH pair passes and the run-time switches the pair body reads.
+struct ISph {
+    float4 pi, vi, jAi, jBi;
+    float bi;
+    float ai_xx, ai_yy, ai_zz, ai_xy, ai_xz, ai_yz;  // artificial stress of i (computeDerivatives.h:210-217)
+    bool bals, av, xsph, arts, curl, divv_on;
+    float eps2;           // added to r^2 when gravity shares the squared distance
+    uint32_t lo, span;    // neighbour window 0 < r^2 <= H^2 on the bit patterns of r^2 + eps2
+};
+
+template <int PASS, bool SOLIDS>
+__device__ __forceinline__ ISph load_isph(const DevArrays& a, const DevParams& p, int64_t i, float eps2) {
+    constexpr bool DO_A = PASS != PASS_VGRAD;
+    ISph s;
+    s.pi = a.posm[i];
+    s.vi = a.velrho[i];
+    s.jAi = make_float4(0, 0, 0, 0);
+    s.jBi = make_float4(0, 0, 0, 0);
+    if (DO_A) {
+        s.jAi = a.jA[i];
+        s.jBi = a.jB[i];
+    }
+    s.bals = has(p, GSPH_BALSARA_SWITCH);
+    s.av = has(p, GSPH_ARTIFICIAL_VISCOSITY);
+    s.xsph = has(p, GSPH_XSPH);
+    s.arts = has(p, GSPH_ARTIFICIAL_STRESS);
+    s.curl = !SOLIDS && s.bals;
+    s.divv_on = s.bals || has(p, GSPH_INTEGRATE_DENSITY);
+    s.bi = s.bals ? s.jBi.z : 1.0f;
+    s.ai_xx = art(p.mateps, s.jAi.x); s.ai_yy = art(p.mateps, s.jAi.y); s.ai_zz = art(p.mateps, s.jAi.z);
+    s.ai_xy = art(p.mateps, s.jAi.w); s.ai_xz = art(p.mateps, s.jBi.x); s.ai_yz = art(p.mateps, s.jBi.y);
+    s.eps2 = eps2;
+    s.lo = __float_as_uint(eps2);
+    s.span = __float_as_uint(p.H2 + eps2) - s.lo;
+    return s;
+}
+
+// The pair body of the SPH jobs over nj staged j-records (P: posm, V: velrho, JA/JB: sigma/rho^2):
+// gravity when GRAV != 0 (computeDerivatives.h:229-235, G applied by the finish kernel), then for
+// 0 < r <= H the velocity-gradient terms (:118-141) and the acceleration terms (:237-295).
+// GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: the self pair must contribute 0).
+template <int PASS, int GRAV, bool SOLIDS>
+__device__ __forceinline__ void pair_tile(PairAcc& T, float& maxv, const ISph& I, const float4* __restrict__ P,
+                                          const float4* __restrict__ V, const float4* __restrict__ JA,
+                                          const float4* __restrict__ JB, int nj, const DevParams& p) {
+    constexpr bool DO_V = PASS != PASS_ACC;
+    constexpr bool DO_A = PASS != PASS_VGRAD;
+    const float eps2 = I.eps2;
+#pragma unroll 4
+    for (int j = 0; j < nj; ++j) {
+        const float4 q = P[j];
+        const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;  // d = x_j - x_i = -r_ij
+        const float r2e = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+        if (GRAV != 0) {
+            float inv = rsqrtf(r2e);
+            if (GRAV == 2) inv = fminf(inv, 1e12f);
+            const float s = q.w * inv * (inv * inv);
+            T.f[F_GX] = fmaf(dx, s, T.f[F_GX]);
+            T.f[F_GY] = fmaf(dy, s, T.f[F_GY]);
+            T.f[F_GZ] = fmaf(dz, s, T.f[F_GZ]);
+        }
+        if (in_open_closed(r2e, I.lo, I.span)) {  // 0 < r2 <= H2
+            const float r2 = r2e - eps2;
+            const float inv_r = rsqrtf(r2);
+            const float r = r2 * inv_r;
+            const float qq = r * p.inv_h;
+            // grad_i W = (dW/r) r_ij with r_ij = -d:  g = -(dW/r) d
+            const float gf = -p.dw_pref * dw_poly(qq) * inv_r;
+            const float gx = gf * dx, gy = gf * dy, gz = gf * dz;
+            const float4 vj = V[j];
+            const float vx = I.vi.x - vj.x, vy = I.vi.y - vj.y, vz = I.vi.z - vj.z;  // v_ij
+            const float mj = q.w, rhoj = vj.w;
+            if (DO_V) {
+                const float mr = mj / rhoj;
+                if (SOLIDS) {  // addStrainRateAndRotationRate (models.h:225-248)
+                    const float t = -0.5f * mr;
+                    T.f[F_E00] = fmaf(t, vx * gx + vx * gx, T.f[F_E00]);
+                    T.f[F_E11] = fmaf(t, vy * gy + vy * gy, T.f[F_E11]);
+                    T.f[F_E22] = fmaf(t, vz * gz + vz * gz, T.f[F_E22]);
+                    T.f[F_E01] = fmaf(t, vx * gy + vy * gx, T.f[F_E01]);
+                    T.f[F_E02] = fmaf(t, vx * gz + vz * gx, T.f[F_E02]);
+                    T.f[F_E12] = fmaf(t, vy * gz + vz * gy, T.f[F_E12]);
+                    T.f[F_W01] = fmaf(t, vx * gy - vy * gx, T.f[F_W01]);
+                    T.f[F_W02] = fmaf(t, vx * gz - vz * gx, T.f[F_W02]);
+                    T.f[F_W12] = fmaf(t, vy * gz - vz * gy, T.f[F_W12]);
+                } else if (I.curl) {
+                    T.f[F_C0] = fmaf(mr, vy * gz - vz * gy, T.f[F_C0]);
+                    T.f[F_C1] = fmaf(mr, vz * gx - vx * gz, T.f[F_C1]);
+                    T.f[F_C2] = fmaf(mr, vx * gy - vy * gx, T.f[F_C2]);
+                }
+                if (I.divv_on) T.f[F_DIVV] = fmaf(-mr, vx * gx + vy * gy + vz * gz, T.f[F_DIVV]);
+            }
+            if (DO_A) {
+                const float4 ja = JA[j];
+                const float4 jb = JB[j];
+                float sxx = I.jAi.x + ja.x, syy = I.jAi.y + ja.y, szz = I.jAi.z + ja.z;
+                float sxy = I.jAi.w + ja.w, sxz = I.jBi.x + jb.x, syz = I.jBi.y + jb.y;
+                if (I.arts) {
+                    const float f = powf(p.w_pref * w_poly(qq) * p.inv_w_normalsep, p.matexp);
+                    sxx += f * (I.ai_xx + art(p.mateps, ja.x));
+                    syy += f * (I.ai_yy + art(p.mateps, ja.y));
+                    szz += f * (I.ai_zz + art(p.mateps, ja.z));
+                    sxy += f * (I.ai_xy + art(p.mateps, ja.w));
+                    sxz += f * (I.ai_xz + art(p.mateps, jb.x));
+                    syz += f * (I.ai_yz + art(p.mateps, jb.y));
+                }
+                T.f[F_AX] = fmaf(mj, sxx * gx + sxy * gy + sxz * gz, T.f[F_AX]);
+                T.f[F_AY] = fmaf(mj, sxy * gx + syy * gy + syz * gz, T.f[F_AY]);
+                T.f[F_AZ] = fmaf(mj, sxz * gx + syz * gy + szz * gz, T.f[F_AZ]);
+                if (I.av) {  // artificialViscosity (models.h:158-185)
+                    const float w = -(dx * vx + dy * vy + dz * vz) * inv_r;  // r_ij . v_ij / r
+                    if (w < 0.0f) {
+                        const float vsig = p.c + p.c - p.beta * w;
+                        const float rhoij = (I.vi.w + rhoj) * 0.5f;
+                        const float bj = I.bals ? jb.z : 1.0f;
+                        const float II = -0.25f * (I.bi + bj) * p.alpha * w * vsig / rhoij;
+                        const float m2 = -mj * II;
+                        T.f[F_AX] = fmaf(m2, gx, T.f[F_AX]);
+                        T.f[F_AY] = fmaf(m2, gy, T.f[F_AY]);
+                        T.f[F_AZ] = fmaf(m2, gz, T.f[F_AZ]);
+                        if (I.bals) maxv = fmaxf(maxv, vsig);
+                    }
+                }
+                if (I.xsph) {
+                    const float f = 2.0f * mj / (I.vi.w + rhoj) * (p.w_pref * w_poly(qq));
+                    T.f[F_XV0] = fmaf(f, -vx, T.f[F_XV0]);
+                    T.f[F_XV1] = fmaf(f, -vy, T.f[F_XV1]);
+                    T.f[F_XV2] = fmaf(f, -vz, T.f[F_XV2]);
+                }
+            }
+        }
+    }
+}
+
+template <uint32_t MASK, bool COMP>
+__device__ __forceinline__ void fold_tile(PairAcc& S, PairAcc& C, const PairAcc& T) {
+#pragma unroll
+    for (int f = 0; f < F_COUNT; ++f) {
+        if (!((MASK >> f) & 1u) || f == F_MAXV) continue;
+        if (COMP) fold(S.f[f], C.f[f], T.f[f]);
+        else S.f[f] += T.f[f];
+    }
+}
+
+// store one thread's partial sums: field o at out[o * stride] (sums) and out[(K + o) * stride]
+// (compensation terms)
+template <uint32_t MASK, bool COMP>
+__device__ __forceinline__ void store_partials(float* out, int64_t stride, const PairAcc& S, const PairAcc& C,
+                                               float maxv) {
+    constexpr int K = popc_c(MASK);
+#pragma unroll
+    for (int f = 0; f < F_COUNT; ++f) {
+        if (!((MASK >> f) & 1u)) continue;
+        const int o = field_offset<MASK>(f);
+        out[o * stride] = (f == F_MAXV) ? maxv : S.f[f];
+        if (COMP) out[(K + o) * stride] = (f == F_MAXV) ? 0.0f : C.f[f];
+    }
+}
+
+// All-pairs SPH pass: blockIdx.x = i-block, blockIdx.y = j-segment (partials [seg][field][n_pad]).
+template <int PASS, int GRAV, bool SOLIDS, bool COMP>
+__global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt, int nseg) {
     constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
     constexpr int K = popc_c(MASK);
     constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
-    constexpr bool DO_V = PASS != PASS_ACC;
-    constexpr bool DO_A = PASS != PASS_VGRAD;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     JTilePipe<NS> pipe;
@@ -179,179 +389,91 @@ __global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt,
     }
     pipe.jt = jt;
     pipe.status = a.status;
-    if (LIST) {
-        pipe.list = list + blockIdx.x * list_stride;
-        pipe.t_begin = 0;
-        pipe.t_end = count[blockIdx.x];
-    } else {
-        segment_tiles(a.n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
-    }
+    segment_tiles(a.n_pad / jt, blockIdx.y, nseg, pipe.t_begin, pipe.t_end);
 
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const float4 pi = a.posm[i];
-    const float4 vi = a.velrho[i];
-    float4 jAi = make_float4(0, 0, 0, 0), jBi = make_float4(0, 0, 0, 0);
-    if (DO_A) {
-        jAi = a.jA[i];
-        jBi = a.jB[i];
-    }
-    const bool bals = has(p, GSPH_BALSARA_SWITCH);
-    const bool av = has(p, GSPH_ARTIFICIAL_VISCOSITY);
-    const bool xsph = has(p, GSPH_XSPH);
-    const bool arts = has(p, GSPH_ARTIFICIAL_STRESS);
-    const bool curl = !SOLIDS && bals;
-    const bool divv_on = bals || has(p, GSPH_INTEGRATE_DENSITY);
-    const float bi = bals ? jBi.z : 1.0f;
-    // artificial stress of i (computeDerivatives.h:210-217)
-    const float ai_xx = art(p.mateps, jAi.x), ai_yy = art(p.mateps, jAi.y), ai_zz = art(p.mateps, jAi.z),
-                ai_xy = art(p.mateps, jAi.w), ai_xz = art(p.mateps, jBi.x), ai_yz = art(p.mateps, jBi.y);
-
-    // neighbour window on r2 (+eps^2 when gravity shares the squared distance)
-    const float eps2 = (GRAV == 1) ? p.eps2 : 0.0f;
-    const uint32_t lo = __float_as_uint(eps2);
-    const uint32_t span = __float_as_uint(p.H2 + eps2) - lo;
-
+    const ISph I = load_isph<PASS, SOLIDS>(a, p, i, (GRAV == 1) ? p.eps2 : 0.0f);
     PairAcc S, C;
 #pragma unroll
-    for (int f = 0; f < F_COUNT; ++f) {
-        S.f[f] = 0.0f;
-        C.f[f] = 0.0f;
-    }
+    for (int f = 0; f < F_COUNT; ++f) S.f[f] = C.f[f] = 0.0f;
     float maxv = 0.0f;
 
     pipe.start();
     pipe.run([&](const float4* stage) {
-        const float4* P = stage;
-        const float4* V = stage + jt;
-        const float4* JA = stage + 2 * jt;
-        const float4* JB = stage + 3 * jt;
         PairAcc T;
 #pragma unroll
         for (int f = 0; f < F_COUNT; ++f) T.f[f] = 0.0f;
-#pragma unroll 4
-        for (int j = 0; j < jt; ++j) {
-            const float4 q = P[j];
-            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;  // d = x_j - x_i = -r_ij
-            const float r2e = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-            if (GRAV != 0) {  // computeDerivatives.h:229-235 (G applied by the finish kernel)
-                float inv = rsqrtf(r2e);
-                if (GRAV == 2) inv = fminf(inv, 1e12f);
-                const float s = q.w * inv * (inv * inv);
-                T.f[F_GX] = fmaf(dx, s, T.f[F_GX]);
-                T.f[F_GY] = fmaf(dy, s, T.f[F_GY]);
-                T.f[F_GZ] = fmaf(dz, s, T.f[F_GZ]);
-            }
-            if (in_open_closed(r2e, lo, span)) {  // 0 < r2 <= H2
-                const float r2 = r2e - eps2;
-                const float inv_r = rsqrtf(r2);
-                const float r = r2 * inv_r;
-                const float qq = r * p.inv_h;
-                const float gf = -p.dw_pref * dw_poly(qq) * inv_r;  // gradW = -gf * r_ij... see below
-                // grad_i W = (dW/r) r_ij with r_ij = -d:  g = -(dW/r) d
-                const float gx = gf * dx, gy = gf * dy, gz = gf * dz;
-                const float4 vj = V[j];
-                const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;  // v_ij
-                const float mj = q.w, rhoj = vj.w;
-                if (DO_V) {  // calcBalsaraDensityDTDStressDT pair body (:118-141)
-                    const float mr = mj / rhoj;
-                    if (SOLIDS) {  // addStrainRateAndRotationRate (models.h:225-248)
-                        const float t = -0.5f * mr;
-                        T.f[F_E00] = fmaf(t, vx * gx + vx * gx, T.f[F_E00]);
-                        T.f[F_E11] = fmaf(t, vy * gy + vy * gy, T.f[F_E11]);
-                        T.f[F_E22] = fmaf(t, vz * gz + vz * gz, T.f[F_E22]);
-                        T.f[F_E01] = fmaf(t, vx * gy + vy * gx, T.f[F_E01]);
-                        T.f[F_E02] = fmaf(t, vx * gz + vz * gx, T.f[F_E02]);
-                        T.f[F_E12] = fmaf(t, vy * gz + vz * gy, T.f[F_E12]);
-                        T.f[F_W01] = fmaf(t, vx * gy - vy * gx, T.f[F_W01]);
-                        T.f[F_W02] = fmaf(t, vx * gz - vz * gx, T.f[F_W02]);
-                        T.f[F_W12] = fmaf(t, vy * gz - vz * gy, T.f[F_W12]);
-                    } else if (curl) {
-                        T.f[F_C0] = fmaf(mr, vy * gz - vz * gy, T.f[F_C0]);
-                        T.f[F_C1] = fmaf(mr, vz * gx - vx * gz, T.f[F_C1]);
-                        T.f[F_C2] = fmaf(mr, vx * gy - vy * gx, T.f[F_C2]);
-                    }
-                    if (divv_on) T.f[F_DIVV] = fmaf(-mr, vx * gx + vy * gy + vz * gz, T.f[F_DIVV]);
-                }
-                if (DO_A) {  // calcAcceleration SPH body (:237-295)
-                    const float4 ja = JA[j];
-                    const float4 jb = JB[j];
-                    float sxx = jAi.x + ja.x, syy = jAi.y + ja.y, szz = jAi.z + ja.z;
-                    float sxy = jAi.w + ja.w, sxz = jBi.x + jb.x, syz = jBi.y + jb.y;
-                    if (arts) {
-                        const float f = powf(p.w_pref * w_poly(qq) * p.inv_w_normalsep, p.matexp);
-                        sxx += f * (ai_xx + art(p.mateps, ja.x));
-                        syy += f * (ai_yy + art(p.mateps, ja.y));
-                        szz += f * (ai_zz + art(p.mateps, ja.z));
-                        sxy += f * (ai_xy + art(p.mateps, ja.w));
-                        sxz += f * (ai_xz + art(p.mateps, jb.x));
-                        syz += f * (ai_yz + art(p.mateps, jb.y));
-                    }
-                    T.f[F_AX] = fmaf(mj, sxx * gx + sxy * gy + sxz * gz, T.f[F_AX]);
-                    T.f[F_AY] = fmaf(mj, sxy * gx + syy * gy + syz * gz, T.f[F_AY]);
-                    T.f[F_AZ] = fmaf(mj, sxz * gx + syz * gy + szz * gz, T.f[F_AZ]);
-                    if (av) {  // artificialViscosity (models.h:158-185)
-                        const float w = -(dx * vx + dy * vy + dz * vz) * inv_r;  // r_ij . v_ij / r
-                        if (w < 0.0f) {
-                            const float vsig = p.c + p.c - p.beta * w;
-                            const float rhoij = (vi.w + rhoj) * 0.5f;
-                            const float bj = bals ? jb.z : 1.0f;
-                            const float II = -0.25f * (bi + bj) * p.alpha * w * vsig / rhoij;
-                            const float m2 = -mj * II;
-                            T.f[F_AX] = fmaf(m2, gx, T.f[F_AX]);
-                            T.f[F_AY] = fmaf(m2, gy, T.f[F_AY]);
-                            T.f[F_AZ] = fmaf(m2, gz, T.f[F_AZ]);
-                            if (bals) maxv = fmaxf(maxv, vsig);
-                        }
-                    }
-                    if (xsph) {
-                        const float f = 2.0f * mj / (vi.w + rhoj) * (p.w_pref * w_poly(qq));
-                        T.f[F_XV0] = fmaf(f, -vx, T.f[F_XV0]);
-                        T.f[F_XV1] = fmaf(f, -vy, T.f[F_XV1]);
-                        T.f[F_XV2] = fmaf(f, -vz, T.f[F_XV2]);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int f = 0; f < F_COUNT; ++f) {
-            if (!((MASK >> f) & 1u) || f == F_MAXV) continue;
-            if (COMP) fold(S.f[f], C.f[f], T.f[f]);
-            else S.f[f] += T.f[f];
-        }
+        pair_tile<PASS, GRAV, SOLIDS>(T, maxv, I, stage, stage + jt, stage + 2 * jt, stage + 3 * jt, jt, p);
+        fold_tile<MASK, COMP>(S, C, T);
     });
+    store_partials<MASK, COMP>(a.part + static_cast<int64_t>(blockIdx.y) * (COMP ? 2 * K : K) * a.n_pad + i, a.n_pad,
+                               S, C, maxv);
+}
 
-    const int64_t seg = blockIdx.y;
-    float* out = a.part + seg * static_cast<int64_t>(COMP ? 2 * K : K) * a.n_pad + i;
+// Culled SPH pass (no gravity): a persistent grid walks the work items; item w covers up to
+// `item_chunks` near chunks of one i-group and writes its partials to part[w][field][kGroup].
+template <int PASS, bool SOLIDS, bool COMP>
+__global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p, CullView cv) {
+    constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
+    constexpr int K = popc_c(MASK);
+    constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
+    constexpr int SJ = kStageChunks * kChunk;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ItemPipe<NS> pipe;
+    pipe.buf = reinterpret_cast<float4*>(smem_raw);
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * NS * SJ * sizeof(float4));
+    pipe.src[0] = a.posm;
+    pipe.src[1] = a.velrho;
+    if constexpr (NS == 4) {
+        pipe.src[2] = a.jA;
+        pipe.src[3] = a.jB;
+    }
+    pipe.status = a.status;
+    pipe.init();
+    const int total = cv.item_start[cv.ngroups];
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        int g, c0, c1;
+        cv.item(w, g, c0, c1);
+        const int64_t i = static_cast<int64_t>(g) * kGroup + threadIdx.x;
+        const ISph I = load_isph<PASS, SOLIDS>(a, p, i, 0.0f);
+        PairAcc S, C;
 #pragma unroll
-    for (int f = 0; f < F_COUNT; ++f) {
-        if (!((MASK >> f) & 1u)) continue;
-        const int o = field_offset<MASK>(f);
-        out[o * a.n_pad] = (f == F_MAXV) ? maxv : S.f[f];
-        if (COMP) out[(K + o) * a.n_pad] = (f == F_MAXV) ? 0.0f : C.f[f];
+        for (int f = 0; f < F_COUNT; ++f) S.f[f] = C.f[f] = 0.0f;
+        float maxv = 0.0f;
+        if (!pipe.run(cv.list + static_cast<int64_t>(g) * cv.nchunks + c0, c1 - c0, [&](const float4* stage, int nj) {
+                PairAcc T;
+#pragma unroll
+                for (int f = 0; f < F_COUNT; ++f) T.f[f] = 0.0f;
+                pair_tile<PASS, 0, SOLIDS>(T, maxv, I, stage, stage + SJ, stage + 2 * SJ, stage + 3 * SJ, nj, p);
+                fold_tile<MASK, COMP>(S, C, T);
+            }))
+            return;
+        store_partials<MASK, COMP>(cv.part + static_cast<int64_t>(w) * (COMP ? 2 * K : K) * kGroup + threadIdx.x,
+                                   kGroup, S, C, maxv);
     }
 }
 
-// Sum the segments of one field (fixed order): FP32 in plain mode, FP64 of (sum + error) in
-// compensated mode. The max signal velocity is a max over segments.
+
+// Sum the slots of one field in a fixed order: FP32 in plain mode, FP64 of (sum + error) in
+// compensated mode. The max signal velocity is a max over slots.
 template <uint32_t MASK, bool COMP>
-__device__ __forceinline__ float seg_sum(const DevArrays& a, int nseg, int64_t i, int f) {
+__device__ __forceinline__ float seg_sum(const PartView& v, int64_t i, int f) {
     constexpr int K = popc_c(MASK);
     const int o = field_offset<MASK>(f);
-    const int64_t stride = static_cast<int64_t>(COMP ? 2 * K : K) * a.n_pad;
+    int b, e;
+    v.range(i, b, e);
     if (f == F_MAXV) {
         float m = 0.0f;
-        for (int k = 0; k < nseg; ++k) m = fmaxf(m, a.part[k * stride + o * a.n_pad + i]);
+        for (int k = b; k < e; ++k) m = fmaxf(m, v.at(k, o, i));
         return m;
     }
     if (COMP) {
         double s = 0.0;
-        for (int k = 0; k < nseg; ++k)
-            s += static_cast<double>(a.part[k * stride + o * a.n_pad + i]) +
-                 static_cast<double>(a.part[k * stride + (K + o) * a.n_pad + i]);
+        for (int k = b; k < e; ++k) s += static_cast<double>(v.at(k, o, i)) + static_cast<double>(v.at(k, K + o, i));
         return static_cast<float>(s);
     }
     float s = 0.0f;
-    for (int k = 0; k < nseg; ++k) s += a.part[k * stride + o * a.n_pad + i];
+    for (int k = b; k < e; ++k) s += v.at(k, o, i);
     return s;
 }
 
@@ -391,7 +513,7 @@ __device__ __forceinline__ float gpart_sum(const DevArrays& a, int gnseg, int64_
 }
 
 template <int PASS, bool GRAV, bool SOLIDS, bool COMP>
-__global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
+__global__ void k_pairs_finish(DevArrays a, DevParams p, PartView pv, int gnseg) {
     constexpr uint32_t MASK = field_mask<PASS, GRAV, SOLIDS>();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (PASS != PASS_VGRAD && has(p, GSPH_VARIABLE_TIMESTEP) && i == 0)
@@ -399,14 +521,14 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
     if (i >= a.n) return;
     const float4 vi = a.velrho[i];
     if (PASS != PASS_ACC) {  // calcBalsaraDensityDTDStressDT::do_after (:144-161)
-        const float divv = seg_sum<MASK, COMP>(a, nseg, i, F_DIVV);
+        const float divv = seg_sum<MASK, COMP>(pv, i, F_DIVV);
         float c0 = 0, c1 = 0, c2 = 0;
         if (SOLIDS) {
-            const float e[6] = {seg_sum<MASK, COMP>(a, nseg, i, F_E00), seg_sum<MASK, COMP>(a, nseg, i, F_E11),
-                                seg_sum<MASK, COMP>(a, nseg, i, F_E22), seg_sum<MASK, COMP>(a, nseg, i, F_E01),
-                                seg_sum<MASK, COMP>(a, nseg, i, F_E02), seg_sum<MASK, COMP>(a, nseg, i, F_E12)};
-            const float w01 = seg_sum<MASK, COMP>(a, nseg, i, F_W01), w02 = seg_sum<MASK, COMP>(a, nseg, i, F_W02),
-                        w12 = seg_sum<MASK, COMP>(a, nseg, i, F_W12);
+            const float e[6] = {seg_sum<MASK, COMP>(pv, i, F_E00), seg_sum<MASK, COMP>(pv, i, F_E11),
+                                seg_sum<MASK, COMP>(pv, i, F_E22), seg_sum<MASK, COMP>(pv, i, F_E01),
+                                seg_sum<MASK, COMP>(pv, i, F_E02), seg_sum<MASK, COMP>(pv, i, F_E12)};
+            const float w01 = seg_sum<MASK, COMP>(pv, i, F_W01), w02 = seg_sum<MASK, COMP>(pv, i, F_W02),
+                        w12 = seg_sum<MASK, COMP>(pv, i, F_W12);
             const float E[3][3] = {{e[0], e[3], e[4]}, {e[3], e[1], e[5]}, {e[4], e[5], e[2]}};
             const float R[3][3] = {{0.0f, w01, w02}, {-w01, 0.0f, w12}, {-w02, -w12, 0.0f}};
             const float4 sa = a.sA[i], sb = a.sB[i];
@@ -430,9 +552,9 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
             c1 = -2.0f * R[2][0];
             c2 = -2.0f * R[0][1];
         } else {
-            c0 = seg_sum<MASK, COMP>(a, nseg, i, F_C0);
-            c1 = seg_sum<MASK, COMP>(a, nseg, i, F_C1);
-            c2 = seg_sum<MASK, COMP>(a, nseg, i, F_C2);
+            c0 = seg_sum<MASK, COMP>(pv, i, F_C0);
+            c1 = seg_sum<MASK, COMP>(pv, i, F_C1);
+            c2 = seg_sum<MASK, COMP>(pv, i, F_C2);
         }
         a.rhodot[i] = has(p, GSPH_INTEGRATE_DENSITY) ? -vi.w * divv : 0.0f;
         float bal = 0.0f;
@@ -447,13 +569,13 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
         a.balsara[i] = bal;
     }
     if (PASS != PASS_VGRAD) {  // calcAcceleration::do_after (:301-312)
-        float ax = seg_sum<MASK, COMP>(a, nseg, i, F_AX);
-        float ay = seg_sum<MASK, COMP>(a, nseg, i, F_AY);
-        float az = seg_sum<MASK, COMP>(a, nseg, i, F_AZ);
+        float ax = seg_sum<MASK, COMP>(pv, i, F_AX);
+        float ay = seg_sum<MASK, COMP>(pv, i, F_AY);
+        float az = seg_sum<MASK, COMP>(pv, i, F_AZ);
         if (GRAV) {
-            ax = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GX), ax);
-            ay = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GY), ay);
-            az = fmaf(p.G, seg_sum<MASK, COMP>(a, nseg, i, F_GZ), az);
+            ax = fmaf(p.G, seg_sum<MASK, COMP>(pv, i, F_GX), ax);
+            ay = fmaf(p.G, seg_sum<MASK, COMP>(pv, i, F_GY), ay);
+            az = fmaf(p.G, seg_sum<MASK, COMP>(pv, i, F_GZ), az);
         }
         if (gnseg > 0) {
             ax = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 0), ax);
@@ -462,9 +584,9 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, int nseg, int gnseg) {
         }
         const float4 x = a.posm[i];
         environment(p, x, vi, ax, ay, az);
-        a.acc[i] = make_float4(ax, ay, az, seg_sum<MASK, COMP>(a, nseg, i, F_MAXV));
-        a.xvel[i] = make_float4(seg_sum<MASK, COMP>(a, nseg, i, F_XV0), seg_sum<MASK, COMP>(a, nseg, i, F_XV1),
-                                seg_sum<MASK, COMP>(a, nseg, i, F_XV2), 0.0f);
+        a.acc[i] = make_float4(ax, ay, az, seg_sum<MASK, COMP>(pv, i, F_MAXV));
+        a.xvel[i] = make_float4(seg_sum<MASK, COMP>(pv, i, F_XV0), seg_sum<MASK, COMP>(pv, i, F_XV1),
+                                seg_sum<MASK, COMP>(pv, i, F_XV2), 0.0f);
     }
 }
 
@@ -692,44 +814,93 @@ cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s) {
         }                                                  \
     } while (0)
 
+namespace {
+CullView cull_view(const DevArrays& a, const SpatialArrays& sp) {
+    CullView cv;
+    cv.list = sp.list;
+    cv.count = sp.count;
+    cv.item_start = sp.item_start;
+    cv.ngroups = static_cast<int>(a.n_pad / kGroup);
+    cv.nchunks = a.n_pad / kChunk;
+    cv.item_chunks = sp.item_chunks;
+    cv.part = sp.item_part;
+    return cv;
+}
+PartView seg_view(const DevArrays& a, int nseg, int KK) { return PartView{a.part, a.n_pad, nseg, nullptr, KK}; }
+PartView item_view(const DevArrays& a, const SpatialArrays& sp, int KK) {
+    return PartView{sp.item_part, a.n_pad, 0, sp.item_start, KK};
+}
+
+// exclusive scan of the per-group item counts ceil(count / item_chunks), one block, fixed order
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_work_items(const int* __restrict__ count, int* __restrict__ start,
+                                                             int ngroups, int item_chunks) {
+    __shared__ int warp_sums[kScanThreads / 32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < ngroups; base += kScanThreads) {
+        const int g = base + threadIdx.x;
+        const int v = (g < ngroups) ? (count[g] + item_chunks - 1) / item_chunks : 0;
+        int x = v;  // inclusive warp scan
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = warp_sums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sums[lane] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = carry + (warp ? warp_sums[warp - 1] : 0) + x - v;
+        if (g < ngroups) start[g] = before;
+        __syncthreads();
+        if (threadIdx.x == kScanThreads - 1) carry = before + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[ngroups] = carry;
+}
+}  // namespace
+
+cudaError_t launch_work_items(const DevArrays& a, const SpatialArrays& sp, cudaStream_t s) {
+    k_work_items<<<1, kScanThreads, 0, s>>>(sp.count, sp.item_start, static_cast<int>(a.n_pad / kGroup), sp.item_chunks);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
                            const SpatialArrays* sp) {
     const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
-    const int nseg = sp ? 1 : L.nseg;
     GSPH_TIMER_MARK(t, start);
     if (sp) {
-        const dim3 grid(static_cast<unsigned>(a.n_pad / kGroup), 1);
-        const size_t smem = pipe_smem_bytes(1, kChunk);
-        const int64_t stride = a.n_pad / kChunk;
-        if (comp)
-            k_density<true, true><<<grid, kGroup, smem, s>>>(a.posm, a.part, a.n_pad, kChunk, 1, p, a.status, sp->list,
-                                                             sp->count, stride);
-        else
-            k_density<false, true><<<grid, kGroup, smem, s>>>(a.posm, a.part, a.n_pad, kChunk, 1, p, a.status, sp->list,
-                                                              sp->count, stride);
+        const size_t smem = pipe_smem_bytes(1, kStageChunks * kChunk);
+        const CullView cv = cull_view(a, *sp);
+        if (comp) k_density_items<true><<<L.item_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
+        else k_density_items<false><<<L.item_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
     } else {
         const int T = 256;
         const dim3 grid(static_cast<unsigned>(a.n_pad / T), static_cast<unsigned>(L.nseg));
         const size_t smem = pipe_smem_bytes(1, L.jt);
-        if (comp)
-            k_density<true, false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status, nullptr,
-                                                          nullptr, 0);
-        else
-            k_density<false, false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status, nullptr,
-                                                           nullptr, 0);
+        if (comp) k_density<true><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status);
+        else k_density<false><<<grid, T, smem, s>>>(a.posm, a.part, a.n_pad, L.jt, L.nseg, p, a.status);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
-    if (comp)
-        k_density_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, nseg);
-    else
-        k_density_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, nseg);
+    const int KK = comp ? 2 : 1;
+    const PartView pv = sp ? item_view(a, *sp, KK) : seg_view(a, L.nseg, KK);
+    if (comp) k_density_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, pv);
+    else k_density_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, pv);
     return cudaGetLastError();
 }
-
-cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                                    const KTimer* t);
 
 cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s) {
     k_prepare<<<blocks_for(a.n, 256), 256, 0, s>>>(a, p);
@@ -739,78 +910,77 @@ cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t 
 namespace {
 template <int PASS, int GRAV, bool SOLIDS, bool COMP>
 cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
-                    const SpatialArrays* sp, const KTimer* tg) {
+                    const SpatialArrays* sp, int gnseg, cudaEvent_t join) {
     constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
-    int gnseg = 0;
-    if (sp) {
-        // SPH terms over the near-chunk lists; gravity (acceleration passes) from the all-pairs kernel
-        const size_t smem = pipe_smem_bytes(NS, kChunk);
+    if (sp) {  // SPH terms over the near-chunk work items; gravity partials come from elsewhere
+        constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
+        constexpr int K = popc_c(MASK);
+        const size_t smem = pipe_smem_bytes(NS, kStageChunks * kChunk);
         GSPH_TIMER_MARK(t, start);
-        k_pairs<PASS, 0, SOLIDS, COMP, true><<<static_cast<unsigned>(a.n_pad / kGroup), kGroup, smem, s>>>(
-            a, p, kChunk, 1, sp->list, sp->count, a.n_pad / kChunk);
+        k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cull_view(a, *sp));
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         GSPH_TIMER_MARK(t, stop);
-        if (PASS != PASS_VGRAD && GRAV != 0) {
-            e = launch_gravity_partials(a, p, L, s, tg);
+        if (join) {
+            e = cudaStreamWaitEvent(s, join, 0);
             if (e != cudaSuccess) return e;
-            gnseg = L.grav_nseg;
         }
-        k_pairs_finish<PASS, false, SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 1, gnseg);
+        k_pairs_finish<PASS, false, SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(
+            a, p, item_view(a, *sp, COMP ? 2 * K : K), PASS == PASS_VGRAD ? 0 : gnseg);
         return cudaGetLastError();
     }
+    constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
+    constexpr int K = popc_c(MASK);
     const size_t smem = pipe_smem_bytes(NS, L.jt);
-    auto kern = k_pairs<PASS, GRAV, SOLIDS, COMP, false>;
+    auto kern = k_pairs<PASS, GRAV, SOLIDS, COMP>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
     }
     const dim3 grid(static_cast<unsigned>(a.n_pad / L.threads), static_cast<unsigned>(L.nseg));
     GSPH_TIMER_MARK(t, start);
-    kern<<<grid, L.threads, smem, s>>>(a, p, L.jt, L.nseg, nullptr, nullptr, 0);
+    kern<<<grid, L.threads, smem, s>>>(a, p, L.jt, L.nseg);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
-    k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.nseg, 0);
+    k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(
+        a, p, seg_view(a, L.nseg, COMP ? 2 * K : K), 0);
     return cudaGetLastError();
 }
 
 template <int PASS, int GRAV>
 cudaError_t pairs_g(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
-                    const SpatialArrays* sp, const KTimer* tg) {
+                    const SpatialArrays* sp, int gnseg, cudaEvent_t join) {
     const bool solids = has(p, GSPH_SOLIDS);
     const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
     if (solids)
-        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t, sp, tg)
-                    : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t, sp, tg);
-    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t, sp, tg)
-                : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t, sp, tg);
+        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t, sp, gnseg, join)
+                    : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t, sp, gnseg, join);
+    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t, sp, gnseg, join)
+                : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t, sp, gnseg, join);
 }
 }  // namespace
 
 cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                         const KTimer* t, const SpatialArrays* sp, const KTimer* tg) {
-    const int grav = !has(p, GSPH_SELF_GRAVITY) ? 0 : (p.eps2 > 0.0f ? 1 : 2);
-    if (sp) {  // the culled kernels carry no gravity; any nonzero GRAV just requests the gravity pass
+                         const KTimer* t, const SpatialArrays* sp, int gnseg, cudaEvent_t join) {
+    if (sp) {  // the culled kernels carry no gravity
         switch (pass) {
-            case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, sp, tg);
-            case PASS_ACC:
-                return grav ? pairs_g<PASS_ACC, 1>(a, p, L, s, t, sp, tg) : pairs_g<PASS_ACC, 0>(a, p, L, s, t, sp, tg);
-            default:
-                return grav ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t, sp, tg)
-                            : pairs_g<PASS_FUSED, 0>(a, p, L, s, t, sp, tg);
+            case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, sp, 0, join);
+            case PASS_ACC: return pairs_g<PASS_ACC, 0>(a, p, L, s, t, sp, gnseg, join);
+            default: return pairs_g<PASS_FUSED, 0>(a, p, L, s, t, sp, gnseg, join);
         }
     }
+    const int grav = !has(p, GSPH_SELF_GRAVITY) ? 0 : (p.eps2 > 0.0f ? 1 : 2);
     switch (pass) {
-        case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, nullptr, nullptr);
+        case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, nullptr, 0, nullptr);
         case PASS_ACC:
-            return grav == 0 ? pairs_g<PASS_ACC, 0>(a, p, L, s, t, nullptr, nullptr)
-                             : (grav == 1 ? pairs_g<PASS_ACC, 1>(a, p, L, s, t, nullptr, nullptr)
-                                          : pairs_g<PASS_ACC, 2>(a, p, L, s, t, nullptr, nullptr));
+            return grav == 0 ? pairs_g<PASS_ACC, 0>(a, p, L, s, t, nullptr, 0, nullptr)
+                             : (grav == 1 ? pairs_g<PASS_ACC, 1>(a, p, L, s, t, nullptr, 0, nullptr)
+                                          : pairs_g<PASS_ACC, 2>(a, p, L, s, t, nullptr, 0, nullptr));
         default:
-            return grav == 0 ? pairs_g<PASS_FUSED, 0>(a, p, L, s, t, nullptr, nullptr)
-                             : (grav == 1 ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t, nullptr, nullptr)
-                                          : pairs_g<PASS_FUSED, 2>(a, p, L, s, t, nullptr, nullptr));
+            return grav == 0 ? pairs_g<PASS_FUSED, 0>(a, p, L, s, t, nullptr, 0, nullptr)
+                             : (grav == 1 ? pairs_g<PASS_FUSED, 1>(a, p, L, s, t, nullptr, 0, nullptr)
+                                          : pairs_g<PASS_FUSED, 2>(a, p, L, s, t, nullptr, 0, nullptr));
     }
 }
 

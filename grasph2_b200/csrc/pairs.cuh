@@ -84,6 +84,88 @@ struct JTilePipe {
     }
 };
 
+// ---- culled passes: work items over the near-chunk lists ------------------------------------------
+constexpr int kStageChunks = 4;  // chunks staged per pipeline stage (256 j-particles)
+
+// Work item w of the culled passes: i-group g, positions [c0, c1) of g's near-chunk list. Items are
+// numbered group by group (item_start[g] .. item_start[g+1]-1), at most item_chunks chunks each.
+struct CullView {
+    const int* list;
+    const int* count;
+    const int* item_start;  // [ngroups + 1], last entry = number of items
+    int ngroups;
+    int64_t nchunks;        // row stride of `list`
+    int item_chunks;
+    float* part;            // [item][field][kGroup]
+    __device__ __forceinline__ void item(int w, int& g, int& c0, int& c1) const {
+        int lo = 0, hi = ngroups;  // item_start[lo] <= w < item_start[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (item_start[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        g = lo;
+        c0 = (w - item_start[g]) * item_chunks;
+        c1 = min(c0 + item_chunks, count[g]);
+    }
+};
+
+// Two-stage pipeline over a list of chunks, kStageChunks chunks per stage; the stage counter runs on
+// across items so the mbarrier phases stay in step.
+template <int NS>
+struct ItemPipe {
+    static constexpr int SJ = kStageChunks * kChunk;
+    float4* buf;     // shared: [2][NS][SJ]
+    uint64_t* bar;   // shared: [2]
+    const float4* src[NS];
+    int* status;
+    uint32_t kst = 0;
+
+    __device__ __forceinline__ void init() {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+            fence_barrier_init();
+        }
+        __syncthreads();
+    }
+    __device__ __forceinline__ void issue(int b, const int* chunks, int first, int nc) {
+        mbar_expect_tx(&bar[b], static_cast<uint32_t>(NS * nc * kChunk * sizeof(float4)));
+        for (int c = 0; c < nc; ++c) {
+            const int64_t ch = chunks[first + c];
+#pragma unroll
+            for (int s = 0; s < NS; ++s)
+                bulk_g2s(buf + (static_cast<int64_t>(b) * NS + s) * SJ + c * kChunk, src[s] + ch * kChunk,
+                         static_cast<uint32_t>(kChunk * sizeof(float4)), &bar[b]);
+        }
+    }
+    // body(stage, nj) for every stage of the n chunks chunks[0..n); false if a wait gave up
+    template <typename Body>
+    __device__ __forceinline__ bool run(const int* chunks, int n, Body&& body) {
+        const int nst = (n + kStageChunks - 1) / kStageChunks;
+        if (threadIdx.x == 0)
+            for (int st = 0; st < 2 && st < nst; ++st)
+                issue((kst + st) & 1, chunks, st * kStageChunks, min(kStageChunks, n - st * kStageChunks));
+        for (int st = 0; st < nst; ++st) {
+            const int b = kst & 1;
+            const bool ok = mbar_wait_bounded(&bar[b], (kst >> 1) & 1, status);
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0 && st + 1 < nst)
+                    mbar_wait_bounded(&bar[(kst + 1) & 1], ((kst + 1) >> 1) & 1, status);
+                __syncthreads();
+                return false;
+            }
+            const int nc = min(kStageChunks, n - st * kStageChunks);
+            body(buf + static_cast<int64_t>(b) * NS * SJ, nc * kChunk);
+            __syncthreads();
+            if (threadIdx.x == 0 && st + 2 < nst)
+                issue(b, chunks, (st + 2) * kStageChunks, min(kStageChunks, n - (st + 2) * kStageChunks));
+            ++kst;
+        }
+        return true;
+    }
+};
+
 // shared-memory bytes of a pipeline: 2 stages of NS streams plus the two barriers
 __host__ __device__ inline size_t pipe_smem_bytes(int ns, int jt) {
     return static_cast<size_t>(2) * ns * jt * sizeof(float4) + 2 * sizeof(uint64_t);
@@ -154,15 +236,22 @@ struct Launch {
     bool grav_x2;    // paired FP32 (f32x2) form of the gravity kernel
     int grav_nseg;
     int accum;       // GSPH_ACCUM_*
+    int item_grid;   // persistent grid of the culled kernels
 };
 
 cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                            const KTimer* t = nullptr, const SpatialArrays* sp = nullptr);
+// near-chunk work items of the culled passes (item_start scan); needs launch_chunk_lists first
+cudaError_t launch_work_items(const DevArrays& a, const SpatialArrays& sp, cudaStream_t s);
 cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s);
-// With `sp`, the SPH terms come from the near-chunk lists and the gravity of an acceleration pass
-// from a separate all-pairs gravity kernel (timer `tg`) whose partials the finish kernel adds.
+// With `sp`, the SPH terms come from the near-chunk work items; the finish kernel then adds `gnseg`
+// segments of gravity partials (a.gpart, from launch_gravity_partials), after waiting for `join`
+// when it is given (the gravity kernel may run on another stream).
 cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                         const KTimer* t = nullptr, const SpatialArrays* sp = nullptr, const KTimer* tg = nullptr);
+                         const KTimer* t = nullptr, const SpatialArrays* sp = nullptr, int gnseg = 0,
+                         cudaEvent_t join = nullptr);
+cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
+                                    const KTimer* t = nullptr);
 cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                            const KTimer* t = nullptr);
 cudaError_t launch_fp32_peak(int sm_count, int iters, float* sink, cudaStream_t s);

@@ -1,4 +1,4 @@
-// spatial.cu -- chunk bounding boxes, per-group near-chunk lists, and the Morton reorder.
+// spatial.cu -- chunk bounding boxes, per-group near-chunk lists, and the Hilbert-curve reorder.
 #include <cub/device/device_radix_sort.cuh>
 
 #include "spatial.cuh"
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(kListThreads) k_chunk_lists(const float4* __re
     if (threadIdx.x == 0) count[g] = base_sh;
 }
 
-// ---- Morton reorder -----------------------------------------------------------------------------
+// ---- space-filling-curve reorder ----------------------------------------------------------------
 __device__ __forceinline__ int f2o(float f) {  // float -> int with the same order
     const int i = __float_as_int(f);
     return i >= 0 ? i : i ^ 0x7fffffff;
@@ -138,7 +138,36 @@ __device__ __forceinline__ unsigned spread10(unsigned v) {  // 10 bits -> every 
     return v;
 }
 
-__global__ void k_morton(DevArrays a, const int* bb, unsigned* keys, int* vals) {
+// 30-bit Hilbert index of a point on a 1024^3 grid: J. Skilling, "Programming the Hilbert curve",
+// AIP Conf. Proc. 707 (2004): the axes are transformed in place into the transposed index
+// (inverse undo + Gray encoding), whose bits interleaved from the top give the index. Consecutive
+// indices are neighbouring cells, so runs of particles in this order are spatially compact.
+__device__ __forceinline__ unsigned hilbert3(unsigned x0, unsigned x1, unsigned x2) {
+    unsigned X[3] = {x0, x1, x2};
+    constexpr unsigned M = 1u << 9;
+    for (unsigned Q = M; Q > 1; Q >>= 1) {
+        const unsigned P = Q - 1;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (X[i] & Q) {
+                X[0] ^= P;
+            } else {
+                const unsigned t = (X[0] ^ X[i]) & P;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    X[1] ^= X[0];
+    X[2] ^= X[1];
+    unsigned t = 0;
+    for (unsigned Q = M; Q > 1; Q >>= 1)
+        if (X[2] & Q) t ^= Q - 1;
+    X[0] ^= t; X[1] ^= t; X[2] ^= t;
+    return (spread10(X[0]) << 2) | (spread10(X[1]) << 1) | spread10(X[2]);
+}
+
+__global__ void k_curve_keys(DevArrays a, const int* bb, unsigned* keys, int* vals) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n_pad) return;
     vals[i] = static_cast<int>(i);
@@ -157,7 +186,7 @@ __global__ void k_morton(DevArrays a, const int* bb, unsigned* keys, int* vals) 
         t = fminf(fmaxf(t, 0.0f), 1.0f);
         q[d] = static_cast<unsigned>(t * 1023.0f);
     }
-    keys[i] = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
+    keys[i] = hilbert3(q[0], q[1], q[2]);
 }
 
 template <typename T>
@@ -213,7 +242,7 @@ cudaError_t reorder_particles(const DevArrays& a, const SpatialArrays& s, cudaSt
     const int64_t np = a.n_pad;
     k_bbox_init<<<1, 32, 0, st>>>(s.bbox);
     k_bbox<<<256, 256, 0, st>>>(a, s.bbox);
-    k_morton<<<blocks_for(np, 256), 256, 0, st>>>(a, s.bbox, s.keys, s.order);
+    k_curve_keys<<<blocks_for(np, 256), 256, 0, st>>>(a, s.bbox, s.keys, s.order);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     launches += 3;

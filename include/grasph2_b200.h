@@ -163,10 +163,10 @@ typedef struct gsph_options {
     int32_t i_per_thread;    /* register blocking of the gravity-only kernel: 1, 2, 4 or 8 (0 = default) */
     int32_t threads;         /* threads per CTA of the pair kernels (0 = default) */
     int32_t check_finite;    /* nonzero: scan inputs at upload for NaN/Inf and fail with GSPH_E_NUMERIC */
-    int32_t no_cull;         /* 0 (default): particles are kept in Morton order on the device and the SPH
+    int32_t no_cull;         /* 0 (default): particles are kept in Hilbert-curve order on the device and the SPH
                                 passes visit only chunks within H of each particle group, gravity covering
                                 all pairs in its own kernel; nonzero: every SPH pass sweeps all N^2 pairs */
-    int32_t resort_interval; /* re-sort the Morton order every this many gsph_step steps (0: only when
+    int32_t resort_interval; /* re-sort the curve order every this many gsph_step steps (0: only when
                                 positions are uploaded) */
     int32_t scalar_fp32;     /* nonzero: scalar FP32 gravity kernel instead of the paired f32x2 form
                                 (identical results; for comparison) */
@@ -232,7 +232,7 @@ int gsph_diagnostics(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stre
 
 /* Number of particles of the context. */
 int gsph_size(gsph_ctx* ctx, int64_t* n);
-/* Re-sort the device-side particle order along a Morton curve of the current positions (a no-op
+/* Re-sort the device-side particle order along a Hilbert curve of the current positions (a no-op
  * with no_cull set). Results do not depend on the order except for floating-point summation order. */
 int gsph_reorder(gsph_ctx* ctx, void* stream);
 /* Text of the last failure on `ctx` (or of the last failed gsph_create when ctx is NULL). */

@@ -307,14 +307,15 @@ def test_profile_and_launch_count():
         pb.step(1)
         pb.profile_collect()
         pr = pb.profile_read()
-        # chunk bounds + lists, density + finish, SPH pass + gravity + finish, leapfrog
-        assert pb.launch_count() - c0 == 8
+        # gravity (side stream), chunk bounds + lists + work items, density + finish, SPH pass + finish,
+        # leapfrog
+        assert pb.launch_count() - c0 == 9
         assert pr["pairs"][1] == 1 and pr["pairs"][0] > 0 and pr["density"][1] == 1 and pr["gravity"][1] == 1
         assert pr["step"][0] >= pr["pairs"][0] + pr["gravity"][0]
 
 
 def test_device_order_is_invisible():
-    """The Morton order on the device never shows: every transfer is in the caller's order."""
+    """The curve order on the device never shows: every transfer is in the caller's order."""
     p = variant_params("solid_mc")
     st = _edge_state("solid_mc", 3001, seed=21)
     with DeviceParticleBuffer(p, 3001) as pb:
