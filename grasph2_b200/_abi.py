@@ -144,6 +144,8 @@ _SIGNATURES = {
     "gsph_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GsphProfile)]),
     "gsph_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "gsph_measure_fp32_peak": (ctypes.c_int, [ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+    "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 

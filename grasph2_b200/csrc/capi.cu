@@ -50,6 +50,13 @@ namespace {
 
 thread_local std::string g_create_error;
 
+}  // namespace
+
+// message of a failed call that has no context (read back with gsph_last_error(NULL))
+void set_global_error(const std::string& msg) { g_create_error = msg; }
+
+namespace {
+
 int fail(gsph_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     else g_create_error = msg;

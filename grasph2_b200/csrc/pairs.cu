@@ -1043,6 +1043,24 @@ cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, cons
     return gravity_any(a, p, L, s, t, false);
 }
 
+// Gravity partials of caller-provided, already padded j-records into caller-provided partials
+// (the allocation-free entry point, noalloc.cu): the plain-FP32 paired kernel.
+cudaError_t launch_gravity_raw(const float4* posm_padded, float* part, int64_t n_pad, int ipt, int jt, int nseg,
+                               float eps2, int* status, cudaStream_t s) {
+    const int T = 128;
+    const dim3 grid(static_cast<unsigned>(n_pad / (static_cast<int64_t>(T) * ipt)), static_cast<unsigned>(nseg));
+    const size_t smem = pipe_smem_bytes(1, jt);
+    const bool soft = eps2 > 0.0f;
+    if (ipt == 4) {
+        if (soft) k_gravity_x2<4, 1, false><<<grid, T, smem, s>>>(posm_padded, part, n_pad, jt, nseg, eps2, status);
+        else k_gravity_x2<4, 2, false><<<grid, T, smem, s>>>(posm_padded, part, n_pad, jt, nseg, eps2, status);
+    } else {
+        if (soft) k_gravity_x2<2, 1, false><<<grid, T, smem, s>>>(posm_padded, part, n_pad, jt, nseg, eps2, status);
+        else k_gravity_x2<2, 2, false><<<grid, T, smem, s>>>(posm_padded, part, n_pad, jt, nseg, eps2, status);
+    }
+    return cudaGetLastError();
+}
+
 // ---- FP32 FFMA throughput probe (roofline denominator) -------------------------------------------
 namespace {
 constexpr int kPeakThreads = 256;

@@ -255,6 +255,8 @@ cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, cons
 cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                            const KTimer* t = nullptr);
 cudaError_t launch_fp32_peak(int sm_count, int iters, float* sink, cudaStream_t s);
+cudaError_t launch_gravity_raw(const float4* posm_padded, float* part, int64_t n_pad, int ipt, int jt, int nseg,
+                               float eps2, int* status, cudaStream_t s);
 int64_t fp32_peak_flops(int sm_count, int iters);
 size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad);
 size_t gravity_partial_floats(const Launch& L, int64_t n_pad);

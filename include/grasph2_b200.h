@@ -273,6 +273,23 @@ int gsph_profile_collect(gsph_ctx* ctx);
 int gsph_profile_read(gsph_ctx* ctx, gsph_profile* out);
 int gsph_profile_reset(gsph_ctx* ctx);
 
+/* Softened all-pairs gravitational accelerations that allocate nothing (no counterpart in the
+ * reference, whose hot path always runs on buffers it allocated itself).
+ * For callers that may not allocate device memory: a host program that hands out all device memory
+ * from a pool fixed at start-up, where a library allocating on its own breaks the budget, or a loop
+ * that must never stall, since cudaMalloc / cudaFree can synchronise the whole device.
+ *   posm: device array of n float4 (x, y, z, m), 16-byte aligned (input)
+ *   acc:  device array of n float4, written as (ax, ay, az, 0) (output)
+ *   a_i = -G sum_{j != i} m_j r_ij / (r_ij^2 + eps^2)^(3/2), plain FP32, as the gravity pass of
+ *   gsph_compute_derivatives.
+ * The scratch (padded j-records and partial sums) is one 16 MiB file-scope device array that every
+ * GPU loading the library holds until exit; hence n <= 524288, larger n is rejected with
+ * GSPH_E_INVALID and a message in gsph_last_error(NULL). The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call on a device shares the array and leaves the last call's data in it: calls whose
+ * kernels may overlap on the GPU (different streams without ordering) race. Asynchronous on `stream`. */
+int gsph_gravity_accel_static(const void* posm, int64_t n, double G, double eps, void* acc, void* stream);
+
 /* FP32 FFMA throughput of the current device, measured by a dependent-chain-free FMA kernel
  * running for about `seconds` (the roofline denominator of the FP32-bound pair kernels).
  * Reports TFLOP/s counting an FMA as 2 flops. */
