@@ -226,7 +226,7 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
         if (sp) {  // bounds of every chunk at the current positions, each group's near chunks, work items
             e = launch_chunk_bounds(c->a, c->sp, s);
             if (e == cudaSuccess) e = launch_chunk_lists(c->a, c->sp, p.H, s);
-            if (e == cudaSuccess) e = launch_work_items(c->a, c->sp, s);
+            if (e == cudaSuccess) e = launch_work_items(c->a, c->sp, c->sp.item_target, s);
             if (e != cudaSuccess) return cuda_fail(c, e, "chunk lists");
             c->launches += 3;
         }
@@ -441,12 +441,14 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
-        sp.item_chunks = static_cast<int>(std::max<int64_t>(4, (nchunks + kMaxItemsPerGroup - 1) / kMaxItemsPerGroup));
-        sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 1) * sizeof(int), ae));
-        // worst case fields per item: fused solids pass without gravity, compensated (x2)
-        const size_t kk = 2 * static_cast<size_t>(popc_c(field_mask<PASS_FUSED, false, true>()));
-        sp.item_part = static_cast<float*>(dalloc(c, ngroups * kMaxItemsPerGroup * kk * kGroup * sizeof(float), ae));
         L.item_grid = c->sm_count * 6;
+        sp.item_target = 4 * L.item_grid;
+        sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 2) * sizeof(int), ae));
+        // worst case fields per item: fused solids pass without gravity, compensated (x2); items are at
+        // most target + one per group (rounding up per group)
+        const size_t kk = 2 * static_cast<size_t>(popc_c(field_mask<PASS_FUSED, false, true>()));
+        const size_t cap = static_cast<size_t>(sp.item_target) + static_cast<size_t>(ngroups);
+        sp.item_part = static_cast<float*>(dalloc(c, cap * kk * kGroup * sizeof(float), ae));
         sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));

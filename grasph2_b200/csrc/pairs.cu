@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restri
     pipe.status = status;
     pipe.init();
     const uint32_t span = __float_as_uint(p.H2);
-    const int total = cv.item_start[cv.ngroups];
+    const int total = cv.items();
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
         int g, c0, c1;
         cv.item(w, g, c0, c1);
@@ -248,15 +248,86 @@ __device__ __forceinline__ ISph load_isph(const DevArrays& a, const DevParams& p
     return s;
 }
 
-// The pair body of the SPH jobs over nj staged j-records (P: posm, V: velrho, JA/JB: sigma/rho^2):
-// gravity when GRAV != 0 (computeDerivatives.h:229-235, G applied by the finish kernel), then for
-// 0 < r <= H the velocity-gradient terms (:118-141) and the acceleration terms (:237-295).
-// GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: the self pair must contribute 0).
+// The SPH terms of one neighbour pair (0 < r <= H): velocity-gradient terms
+// (computeDerivatives.h:118-141) and acceleration terms (:237-295). d = x_j - x_i, r2 = |d|^2.
+template <int PASS, bool SOLIDS>
+__device__ __forceinline__ void sph_neighbour(PairAcc& T, float& maxv, const ISph& I, float mj, float dx, float dy,
+                                              float dz, float r2, float4 vj, float4 ja, float4 jb, const DevParams& p) {
+    constexpr bool DO_V = PASS != PASS_ACC;
+    constexpr bool DO_A = PASS != PASS_VGRAD;
+    const float inv_r = rsqrtf(r2);
+    const float r = r2 * inv_r;
+    const float qq = r * p.inv_h;
+    // grad_i W = (dW/r) r_ij with r_ij = -d:  g = -(dW/r) d
+    const float gf = -p.dw_pref * dw_poly(qq) * inv_r;
+    const float gx = gf * dx, gy = gf * dy, gz = gf * dz;
+    const float vx = I.vi.x - vj.x, vy = I.vi.y - vj.y, vz = I.vi.z - vj.z;  // v_ij
+    const float rhoj = vj.w;
+    if (DO_V) {
+        const float mr = mj / rhoj;
+        if (SOLIDS) {  // addStrainRateAndRotationRate (models.h:225-248)
+            const float t = -0.5f * mr;
+            T.f[F_E00] = fmaf(t, vx * gx + vx * gx, T.f[F_E00]);
+            T.f[F_E11] = fmaf(t, vy * gy + vy * gy, T.f[F_E11]);
+            T.f[F_E22] = fmaf(t, vz * gz + vz * gz, T.f[F_E22]);
+            T.f[F_E01] = fmaf(t, vx * gy + vy * gx, T.f[F_E01]);
+            T.f[F_E02] = fmaf(t, vx * gz + vz * gx, T.f[F_E02]);
+            T.f[F_E12] = fmaf(t, vy * gz + vz * gy, T.f[F_E12]);
+            T.f[F_W01] = fmaf(t, vx * gy - vy * gx, T.f[F_W01]);
+            T.f[F_W02] = fmaf(t, vx * gz - vz * gx, T.f[F_W02]);
+            T.f[F_W12] = fmaf(t, vy * gz - vz * gy, T.f[F_W12]);
+        } else if (I.curl) {
+            T.f[F_C0] = fmaf(mr, vy * gz - vz * gy, T.f[F_C0]);
+            T.f[F_C1] = fmaf(mr, vz * gx - vx * gz, T.f[F_C1]);
+            T.f[F_C2] = fmaf(mr, vx * gy - vy * gx, T.f[F_C2]);
+        }
+        if (I.divv_on) T.f[F_DIVV] = fmaf(-mr, vx * gx + vy * gy + vz * gz, T.f[F_DIVV]);
+    }
+    if (DO_A) {
+        float sxx = I.jAi.x + ja.x, syy = I.jAi.y + ja.y, szz = I.jAi.z + ja.z;
+        float sxy = I.jAi.w + ja.w, sxz = I.jBi.x + jb.x, syz = I.jBi.y + jb.y;
+        if (I.arts) {
+            const float f = powf(p.w_pref * w_poly(qq) * p.inv_w_normalsep, p.matexp);
+            sxx += f * (I.ai_xx + art(p.mateps, ja.x));
+            syy += f * (I.ai_yy + art(p.mateps, ja.y));
+            szz += f * (I.ai_zz + art(p.mateps, ja.z));
+            sxy += f * (I.ai_xy + art(p.mateps, ja.w));
+            sxz += f * (I.ai_xz + art(p.mateps, jb.x));
+            syz += f * (I.ai_yz + art(p.mateps, jb.y));
+        }
+        T.f[F_AX] = fmaf(mj, sxx * gx + sxy * gy + sxz * gz, T.f[F_AX]);
+        T.f[F_AY] = fmaf(mj, sxy * gx + syy * gy + syz * gz, T.f[F_AY]);
+        T.f[F_AZ] = fmaf(mj, sxz * gx + syz * gy + szz * gz, T.f[F_AZ]);
+        if (I.av) {  // artificialViscosity (models.h:158-185)
+            const float w = -(dx * vx + dy * vy + dz * vz) * inv_r;  // r_ij . v_ij / r
+            if (w < 0.0f) {
+                const float vsig = p.c + p.c - p.beta * w;
+                const float rhoij = (I.vi.w + rhoj) * 0.5f;
+                const float bj = I.bals ? jb.z : 1.0f;
+                const float II = -0.25f * (I.bi + bj) * p.alpha * w * vsig / rhoij;
+                const float m2 = -mj * II;
+                T.f[F_AX] = fmaf(m2, gx, T.f[F_AX]);
+                T.f[F_AY] = fmaf(m2, gy, T.f[F_AY]);
+                T.f[F_AZ] = fmaf(m2, gz, T.f[F_AZ]);
+                if (I.bals) maxv = fmaxf(maxv, vsig);
+            }
+        }
+        if (I.xsph) {
+            const float f = 2.0f * mj / (I.vi.w + rhoj) * (p.w_pref * w_poly(qq));
+            T.f[F_XV0] = fmaf(f, -vx, T.f[F_XV0]);
+            T.f[F_XV1] = fmaf(f, -vy, T.f[F_XV1]);
+            T.f[F_XV2] = fmaf(f, -vz, T.f[F_XV2]);
+        }
+    }
+}
+
+// The all-pairs body over nj staged j-records (P: posm, V: velrho, JA/JB: sigma/rho^2): gravity when
+// GRAV != 0 (computeDerivatives.h:229-235, G applied by the finish kernel), then the SPH terms of
+// every neighbour. GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: self pair gives 0).
 template <int PASS, int GRAV, bool SOLIDS>
 __device__ __forceinline__ void pair_tile(PairAcc& T, float& maxv, const ISph& I, const float4* __restrict__ P,
                                           const float4* __restrict__ V, const float4* __restrict__ JA,
                                           const float4* __restrict__ JB, int nj, const DevParams& p) {
-    constexpr bool DO_V = PASS != PASS_ACC;
     constexpr bool DO_A = PASS != PASS_VGRAD;
     const float eps2 = I.eps2;
 #pragma unroll 4
@@ -272,76 +343,51 @@ __device__ __forceinline__ void pair_tile(PairAcc& T, float& maxv, const ISph& I
             T.f[F_GY] = fmaf(dy, s, T.f[F_GY]);
             T.f[F_GZ] = fmaf(dz, s, T.f[F_GZ]);
         }
-        if (in_open_closed(r2e, I.lo, I.span)) {  // 0 < r2 <= H2
-            const float r2 = r2e - eps2;
-            const float inv_r = rsqrtf(r2);
-            const float r = r2 * inv_r;
-            const float qq = r * p.inv_h;
-            // grad_i W = (dW/r) r_ij with r_ij = -d:  g = -(dW/r) d
-            const float gf = -p.dw_pref * dw_poly(qq) * inv_r;
-            const float gx = gf * dx, gy = gf * dy, gz = gf * dz;
-            const float4 vj = V[j];
-            const float vx = I.vi.x - vj.x, vy = I.vi.y - vj.y, vz = I.vi.z - vj.z;  // v_ij
-            const float mj = q.w, rhoj = vj.w;
-            if (DO_V) {
-                const float mr = mj / rhoj;
-                if (SOLIDS) {  // addStrainRateAndRotationRate (models.h:225-248)
-                    const float t = -0.5f * mr;
-                    T.f[F_E00] = fmaf(t, vx * gx + vx * gx, T.f[F_E00]);
-                    T.f[F_E11] = fmaf(t, vy * gy + vy * gy, T.f[F_E11]);
-                    T.f[F_E22] = fmaf(t, vz * gz + vz * gz, T.f[F_E22]);
-                    T.f[F_E01] = fmaf(t, vx * gy + vy * gx, T.f[F_E01]);
-                    T.f[F_E02] = fmaf(t, vx * gz + vz * gx, T.f[F_E02]);
-                    T.f[F_E12] = fmaf(t, vy * gz + vz * gy, T.f[F_E12]);
-                    T.f[F_W01] = fmaf(t, vx * gy - vy * gx, T.f[F_W01]);
-                    T.f[F_W02] = fmaf(t, vx * gz - vz * gx, T.f[F_W02]);
-                    T.f[F_W12] = fmaf(t, vy * gz - vz * gy, T.f[F_W12]);
-                } else if (I.curl) {
-                    T.f[F_C0] = fmaf(mr, vy * gz - vz * gy, T.f[F_C0]);
-                    T.f[F_C1] = fmaf(mr, vz * gx - vx * gz, T.f[F_C1]);
-                    T.f[F_C2] = fmaf(mr, vx * gy - vy * gx, T.f[F_C2]);
-                }
-                if (I.divv_on) T.f[F_DIVV] = fmaf(-mr, vx * gx + vy * gy + vz * gz, T.f[F_DIVV]);
-            }
-            if (DO_A) {
-                const float4 ja = JA[j];
-                const float4 jb = JB[j];
-                float sxx = I.jAi.x + ja.x, syy = I.jAi.y + ja.y, szz = I.jAi.z + ja.z;
-                float sxy = I.jAi.w + ja.w, sxz = I.jBi.x + jb.x, syz = I.jBi.y + jb.y;
-                if (I.arts) {
-                    const float f = powf(p.w_pref * w_poly(qq) * p.inv_w_normalsep, p.matexp);
-                    sxx += f * (I.ai_xx + art(p.mateps, ja.x));
-                    syy += f * (I.ai_yy + art(p.mateps, ja.y));
-                    szz += f * (I.ai_zz + art(p.mateps, ja.z));
-                    sxy += f * (I.ai_xy + art(p.mateps, ja.w));
-                    sxz += f * (I.ai_xz + art(p.mateps, jb.x));
-                    syz += f * (I.ai_yz + art(p.mateps, jb.y));
-                }
-                T.f[F_AX] = fmaf(mj, sxx * gx + sxy * gy + sxz * gz, T.f[F_AX]);
-                T.f[F_AY] = fmaf(mj, sxy * gx + syy * gy + syz * gz, T.f[F_AY]);
-                T.f[F_AZ] = fmaf(mj, sxz * gx + syz * gy + szz * gz, T.f[F_AZ]);
-                if (I.av) {  // artificialViscosity (models.h:158-185)
-                    const float w = -(dx * vx + dy * vy + dz * vz) * inv_r;  // r_ij . v_ij / r
-                    if (w < 0.0f) {
-                        const float vsig = p.c + p.c - p.beta * w;
-                        const float rhoij = (I.vi.w + rhoj) * 0.5f;
-                        const float bj = I.bals ? jb.z : 1.0f;
-                        const float II = -0.25f * (I.bi + bj) * p.alpha * w * vsig / rhoij;
-                        const float m2 = -mj * II;
-                        T.f[F_AX] = fmaf(m2, gx, T.f[F_AX]);
-                        T.f[F_AY] = fmaf(m2, gy, T.f[F_AY]);
-                        T.f[F_AZ] = fmaf(m2, gz, T.f[F_AZ]);
-                        if (I.bals) maxv = fmaxf(maxv, vsig);
-                    }
-                }
-                if (I.xsph) {
-                    const float f = 2.0f * mj / (I.vi.w + rhoj) * (p.w_pref * w_poly(qq));
-                    T.f[F_XV0] = fmaf(f, -vx, T.f[F_XV0]);
-                    T.f[F_XV1] = fmaf(f, -vy, T.f[F_XV1]);
-                    T.f[F_XV2] = fmaf(f, -vz, T.f[F_XV2]);
-                }
+        if (in_open_closed(r2e, I.lo, I.span))  // 0 < r2 <= H2
+            sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2e - eps2, V[j],
+                                        DO_A ? JA[j] : make_float4(0, 0, 0, 0), DO_A ? JB[j] : make_float4(0, 0, 0, 0),
+                                        p);
+    }
+}
+
+// The culled body (no gravity), lane-dense: each 64-j sub-tile is scanned first and every lane
+// appends the indices of its own neighbours to `nb` (this warp's [64][32] byte slots); then the warp
+// walks those lists, so the SPH terms run with all lanes busy instead of once per j any lane needs.
+template <int PASS, bool SOLIDS>
+__device__ __forceinline__ void pair_tile_compact(PairAcc& T, float& maxv, const ISph& I, const float4* __restrict__ P,
+                                                  const float4* __restrict__ V, const float4* __restrict__ JA,
+                                                  const float4* __restrict__ JB, int nj, const DevParams& p,
+                                                  uint8_t* __restrict__ nb) {
+    constexpr bool DO_A = PASS != PASS_VGRAD;
+    const int lane = threadIdx.x & 31;
+    for (int j0 = 0; j0 < nj; j0 += 64) {
+        int cnt = 0;
+#pragma unroll 8
+        for (int jj = 0; jj < 64; ++jj) {
+            const float4 q = P[j0 + jj];
+            const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (in_open_closed(r2, 0u, I.span)) {
+                nb[cnt * 32 + lane] = static_cast<uint8_t>(jj);
+                ++cnt;
             }
         }
+        int m = cnt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        __syncwarp();
+        for (int k = 0; k < m; ++k) {
+            if (k < cnt) {
+                const int j = j0 + nb[k * 32 + lane];
+                const float4 q = P[j];
+                const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, V[j],
+                                            DO_A ? JA[j] : make_float4(0, 0, 0, 0),
+                                            DO_A ? JB[j] : make_float4(0, 0, 0, 0), p);
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -429,8 +475,9 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
         pipe.src[3] = a.jB;
     }
     pipe.status = a.status;
+    uint8_t* nb = reinterpret_cast<uint8_t*>(smem_raw + pipe_smem_bytes(NS, SJ)) + (threadIdx.x >> 5) * (64 * 32);
     pipe.init();
-    const int total = cv.item_start[cv.ngroups];
+    const int total = cv.items();
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
         int g, c0, c1;
         cv.item(w, g, c0, c1);
@@ -444,7 +491,7 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
                 PairAcc T;
 #pragma unroll
                 for (int f = 0; f < F_COUNT; ++f) T.f[f] = 0.0f;
-                pair_tile<PASS, 0, SOLIDS>(T, maxv, I, stage, stage + SJ, stage + 2 * SJ, stage + 3 * SJ, nj, p);
+                pair_tile_compact<PASS, SOLIDS>(T, maxv, I, stage, stage + SJ, stage + 2 * SJ, stage + 3 * SJ, nj, p, nb);
                 fold_tile<MASK, COMP>(S, C, T);
             }))
             return;
@@ -822,7 +869,6 @@ CullView cull_view(const DevArrays& a, const SpatialArrays& sp) {
     cv.item_start = sp.item_start;
     cv.ngroups = static_cast<int>(a.n_pad / kGroup);
     cv.nchunks = a.n_pad / kChunk;
-    cv.item_chunks = sp.item_chunks;
     cv.part = sp.item_part;
     return cv;
 }
@@ -831,24 +877,40 @@ PartView item_view(const DevArrays& a, const SpatialArrays& sp, int KK) {
     return PartView{sp.item_part, a.n_pad, 0, sp.item_start, KK};
 }
 
-// exclusive scan of the per-group item counts ceil(count / item_chunks), one block, fixed order
+// One block: chunks per item ic = ceil(total near chunks / target) so that items carry equal work,
+// then the exclusive scan of the per-group item counts ceil(count / ic) in a fixed order.
 constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads) k_work_items(const int* __restrict__ count, int* __restrict__ start,
-                                                             int ngroups, int item_chunks) {
+                                                             int ngroups, int target) {
     __shared__ int warp_sums[kScanThreads / 32];
     __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
+    __shared__ int ic_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int part = 0;  // total near chunks
+    for (int g = threadIdx.x; g < ngroups; g += kScanThreads) part += count[g];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if (lane == 0) warp_sums[warp] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long total = 0;
+        for (int w = 0; w < kScanThreads / 32; ++w) total += warp_sums[w];
+        const long long ic = (total + target - 1) / target;
+        ic_sh = static_cast<int>(ic < 1 ? 1 : ic);
+        carry = 0;
+    }
+    __syncthreads();
+    const int ic = ic_sh;
     for (int base = 0; base < ngroups; base += kScanThreads) {
         const int g = base + threadIdx.x;
-        const int v = (g < ngroups) ? (count[g] + item_chunks - 1) / item_chunks : 0;
+        const int v = (g < ngroups) ? (count[g] + ic - 1) / ic : 0;
         int x = v;  // inclusive warp scan
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
+        __syncthreads();
         if (lane == 31) warp_sums[warp] = x;
         __syncthreads();
         if (warp == 0) {
@@ -867,12 +929,15 @@ __global__ void __launch_bounds__(kScanThreads) k_work_items(const int* __restri
         if (threadIdx.x == kScanThreads - 1) carry = before + v;
         __syncthreads();
     }
-    if (threadIdx.x == 0) start[ngroups] = carry;
+    if (threadIdx.x == 0) {
+        start[ngroups] = carry;
+        start[ngroups + 1] = ic;
+    }
 }
 }  // namespace
 
-cudaError_t launch_work_items(const DevArrays& a, const SpatialArrays& sp, cudaStream_t s) {
-    k_work_items<<<1, kScanThreads, 0, s>>>(sp.count, sp.item_start, static_cast<int>(a.n_pad / kGroup), sp.item_chunks);
+cudaError_t launch_work_items(const DevArrays& a, const SpatialArrays& sp, int target, cudaStream_t s) {
+    k_work_items<<<1, kScanThreads, 0, s>>>(sp.count, sp.item_start, static_cast<int>(a.n_pad / kGroup), target);
     return cudaGetLastError();
 }
 
@@ -915,7 +980,8 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
     if (sp) {  // SPH terms over the near-chunk work items; gravity partials come from elsewhere
         constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
         constexpr int K = popc_c(MASK);
-        const size_t smem = pipe_smem_bytes(NS, kStageChunks * kChunk);
+        // pipeline stages, then per warp the [64][32] neighbour slots of the compacted body
+        const size_t smem = pipe_smem_bytes(NS, kStageChunks * kChunk) + (kGroup / 32) * 64 * 32;
         GSPH_TIMER_MARK(t, start);
         k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cull_view(a, *sp));
         cudaError_t e = cudaGetLastError();

@@ -92,11 +92,12 @@ constexpr int kStageChunks = 4;  // chunks staged per pipeline stage (256 j-part
 struct CullView {
     const int* list;
     const int* count;
-    const int* item_start;  // [ngroups + 1], last entry = number of items
+    const int* item_start;  // [ngroups + 2]: first item of each group, the number of items, the
+                            // chunks per item (chosen on the device from the total near-chunk count)
     int ngroups;
     int64_t nchunks;        // row stride of `list`
-    int item_chunks;
     float* part;            // [item][field][kGroup]
+    __device__ __forceinline__ int items() const { return item_start[ngroups]; }
     __device__ __forceinline__ void item(int w, int& g, int& c0, int& c1) const {
         int lo = 0, hi = ngroups;  // item_start[lo] <= w < item_start[hi]
         while (hi - lo > 1) {
@@ -105,8 +106,9 @@ struct CullView {
             else hi = mid;
         }
         g = lo;
-        c0 = (w - item_start[g]) * item_chunks;
-        c1 = min(c0 + item_chunks, count[g]);
+        const int ic = item_start[ngroups + 1];
+        c0 = (w - item_start[g]) * ic;
+        c1 = min(c0 + ic, count[g]);
     }
 };
 
@@ -241,8 +243,9 @@ struct Launch {
 
 cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                            const KTimer* t = nullptr, const SpatialArrays* sp = nullptr);
-// near-chunk work items of the culled passes (item_start scan); needs launch_chunk_lists first
-cudaError_t launch_work_items(const DevArrays& a, const SpatialArrays& sp, cudaStream_t s);
+// near-chunk work items of the culled passes (item_start scan); needs launch_chunk_lists first.
+// `target` items in total (plus at most one per group for rounding).
+cudaError_t launch_work_items(const DevArrays& a, const SpatialArrays& sp, int target, cudaStream_t s);
 cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t s);
 // With `sp`, the SPH terms come from the near-chunk work items; the finish kernel then adds `gnseg`
 // segments of gravity partials (a.gpart, from launch_gravity_partials), after waiting for `join`

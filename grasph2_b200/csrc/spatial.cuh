@@ -16,15 +16,14 @@ namespace gsph {
 constexpr int kChunk = 64;     // particles per j-chunk (one bounding box)
 constexpr int kGroup = 128;    // particles per i-group (threads of a culled SPH block)
 constexpr float kMargin = 1e-3f;
-constexpr int kMaxItemsPerGroup = 16;
 
 struct SpatialArrays {
     float4* box_lo;    // [n_pad / kChunk]  chunk bounds (x, y, z, unused)
     float4* box_hi;
     int* list;         // [n_pad / kGroup][n_pad / kChunk] near chunks of each i-group
     int* count;        // [n_pad / kGroup]
-    int* item_start;   // [n_pad / kGroup + 1] first work item of each group; last = number of items
-    int item_chunks;   // chunks per work item (at most kMaxItemsPerGroup items per group)
+    int* item_start;   // [n_pad / kGroup + 2] first work item of each group, number of items, chunks per item
+    int item_target;   // items aimed at per pass (the item buffer holds item_target + groups items)
     float* item_part;  // [items][fields][kGroup] partial sums of the culled passes
     int* ext_of_int;   // [n_pad] caller's index of the particle stored at each internal slot
     int* order;        // [n_pad] scratch: sort values / gather map
