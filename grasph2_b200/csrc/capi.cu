@@ -441,8 +441,9 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
-        L.item_grid = c->sm_count * 6;
-        sp.item_target = 4 * L.item_grid;
+        L.item_grid = c->sm_count * 4;      // 56 KB of shared memory per block: 4 resident per SM
+        L.density_grid = c->sm_count * 8;
+        sp.item_target = 6 * L.item_grid;
         sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 2) * sizeof(int), ae));
         // worst case fields per item: fused solids pass without gravity, compensated (x2); items are at
         // most target + one per group (rounding up per group)

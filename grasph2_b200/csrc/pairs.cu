@@ -350,47 +350,6 @@ __device__ __forceinline__ void pair_tile(PairAcc& T, float& maxv, const ISph& I
     }
 }
 
-// The culled body (no gravity), lane-dense: each 64-j sub-tile is scanned first and every lane
-// appends the indices of its own neighbours to `nb` (this warp's [64][32] byte slots); then the warp
-// walks those lists, so the SPH terms run with all lanes busy instead of once per j any lane needs.
-template <int PASS, bool SOLIDS>
-__device__ __forceinline__ void pair_tile_compact(PairAcc& T, float& maxv, const ISph& I, const float4* __restrict__ P,
-                                                  const float4* __restrict__ V, const float4* __restrict__ JA,
-                                                  const float4* __restrict__ JB, int nj, const DevParams& p,
-                                                  uint8_t* __restrict__ nb) {
-    constexpr bool DO_A = PASS != PASS_VGRAD;
-    const int lane = threadIdx.x & 31;
-    for (int j0 = 0; j0 < nj; j0 += 64) {
-        int cnt = 0;
-#pragma unroll 8
-        for (int jj = 0; jj < 64; ++jj) {
-            const float4 q = P[j0 + jj];
-            const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            if (in_open_closed(r2, 0u, I.span)) {
-                nb[cnt * 32 + lane] = static_cast<uint8_t>(jj);
-                ++cnt;
-            }
-        }
-        int m = cnt;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        __syncwarp();
-        for (int k = 0; k < m; ++k) {
-            if (k < cnt) {
-                const int j = j0 + nb[k * 32 + lane];
-                const float4 q = P[j];
-                const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
-                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, V[j],
-                                            DO_A ? JA[j] : make_float4(0, 0, 0, 0),
-                                            DO_A ? JB[j] : make_float4(0, 0, 0, 0), p);
-            }
-        }
-        __syncwarp();
-    }
-}
-
 template <uint32_t MASK, bool COMP>
 __device__ __forceinline__ void fold_tile(PairAcc& S, PairAcc& C, const PairAcc& T) {
 #pragma unroll
@@ -456,26 +415,26 @@ __global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt,
                                S, C, maxv);
 }
 
-// Culled SPH pass (no gravity): a persistent grid walks the work items; item w covers up to
-// `item_chunks` near chunks of one i-group and writes its partials to part[w][field][kGroup].
+// Culled SPH pass (no gravity): a persistent grid walks the work items; item w covers some near
+// chunks of one i-group and writes its partials to part[w][field][kGroup]. Phase 1 streams only the
+// positions of those chunks through shared memory and lets every lane record the indices of its own
+// neighbours (kNbCap per lane, flushed early when a lane's list is nearly full); phase 2 walks the
+// per-lane lists and gathers each neighbour's records from L2, so the SPH terms run lane-dense.
+constexpr int kNbCap = 96;
 template <int PASS, bool SOLIDS, bool COMP>
 __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p, CullView cv) {
     constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
     constexpr int K = popc_c(MASK);
-    constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
+    constexpr bool DO_A = PASS != PASS_VGRAD;
     constexpr int SJ = kStageChunks * kChunk;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ItemPipe<NS> pipe;
+    ItemPipe<1> pipe;
     pipe.buf = reinterpret_cast<float4*>(smem_raw);
-    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * NS * SJ * sizeof(float4));
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * SJ * sizeof(float4));
     pipe.src[0] = a.posm;
-    pipe.src[1] = a.velrho;
-    if constexpr (NS == 4) {
-        pipe.src[2] = a.jA;
-        pipe.src[3] = a.jB;
-    }
     pipe.status = a.status;
-    uint8_t* nb = reinterpret_cast<uint8_t*>(smem_raw + pipe_smem_bytes(NS, SJ)) + (threadIdx.x >> 5) * (64 * 32);
+    const int lane = threadIdx.x & 31;
+    int* nb = reinterpret_cast<int*>(smem_raw + pipe_smem_bytes(1, SJ)) + (threadIdx.x >> 5) * (kNbCap * 32);
     pipe.init();
     const int total = cv.items();
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -483,18 +442,53 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
         cv.item(w, g, c0, c1);
         const int64_t i = static_cast<int64_t>(g) * kGroup + threadIdx.x;
         const ISph I = load_isph<PASS, SOLIDS>(a, p, i, 0.0f);
-        PairAcc S, C;
+        PairAcc S, C, T;
 #pragma unroll
-        for (int f = 0; f < F_COUNT; ++f) S.f[f] = C.f[f] = 0.0f;
+        for (int f = 0; f < F_COUNT; ++f) S.f[f] = C.f[f] = T.f[f] = 0.0f;
         float maxv = 0.0f;
-        if (!pipe.run(cv.list + static_cast<int64_t>(g) * cv.nchunks + c0, c1 - c0, [&](const float4* stage, int nj) {
-                PairAcc T;
+        int cnt = 0;
+        // phase 2 over the lane lists collected so far
+        auto drain = [&]() {
+            int m = cnt;
 #pragma unroll
-                for (int f = 0; f < F_COUNT; ++f) T.f[f] = 0.0f;
-                pair_tile_compact<PASS, SOLIDS>(T, maxv, I, stage, stage + SJ, stage + 2 * SJ, stage + 3 * SJ, nj, p, nb);
-                fold_tile<MASK, COMP>(S, C, T);
+            for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+            for (int k = 0; k < m; ++k) {
+                if (k < cnt) {
+                    const int j = nb[k * 32 + lane];
+                    const float4 q = a.posm[j];
+                    const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
+                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, a.velrho[j],
+                                                DO_A ? a.jA[j] : make_float4(0, 0, 0, 0),
+                                                DO_A ? a.jB[j] : make_float4(0, 0, 0, 0), p);
+                }
+            }
+            cnt = 0;
+            __syncwarp();
+        };
+        const int* chunks = cv.list + static_cast<int64_t>(g) * cv.nchunks + c0;
+        int chunk_base = 0;  // position in `chunks` of the current stage
+        if (!pipe.run(chunks, c1 - c0, [&](const float4* J, int nj) {
+                for (int s0 = 0; s0 < nj; s0 += kChunk) {
+                    const int jbase = chunks[chunk_base + s0 / kChunk] * kChunk;
+#pragma unroll 8
+                    for (int jj = 0; jj < kChunk; ++jj) {
+                        const float4 q = J[s0 + jj];
+                        const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        if (in_open_closed(r2, 0u, I.span)) {
+                            nb[cnt * 32 + lane] = jbase + jj;
+                            ++cnt;
+                        }
+                    }
+                    // a lane could overflow on the next chunk: process the lists now
+                    if (__any_sync(0xffffffffu, cnt > kNbCap - kChunk)) drain();
+                }
+                chunk_base += nj / kChunk;
             }))
             return;
+        drain();
+        fold_tile<MASK, COMP>(S, C, T);
         store_partials<MASK, COMP>(cv.part + static_cast<int64_t>(w) * (COMP ? 2 * K : K) * kGroup + threadIdx.x,
                                    kGroup, S, C, maxv);
     }
@@ -948,8 +942,8 @@ cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch&
     if (sp) {
         const size_t smem = pipe_smem_bytes(1, kStageChunks * kChunk);
         const CullView cv = cull_view(a, *sp);
-        if (comp) k_density_items<true><<<L.item_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
-        else k_density_items<false><<<L.item_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
+        if (comp) k_density_items<true><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
+        else k_density_items<false><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
     } else {
         const int T = 256;
         const dim3 grid(static_cast<unsigned>(a.n_pad / T), static_cast<unsigned>(L.nseg));
@@ -980,8 +974,13 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
     if (sp) {  // SPH terms over the near-chunk work items; gravity partials come from elsewhere
         constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
         constexpr int K = popc_c(MASK);
-        // pipeline stages, then per warp the [64][32] neighbour slots of the compacted body
-        const size_t smem = pipe_smem_bytes(NS, kStageChunks * kChunk) + (kGroup / 32) * 64 * 32;
+        // position stages, then per warp the [kNbCap][32] neighbour-index lists
+        const size_t smem = pipe_smem_bytes(1, kStageChunks * kChunk) + (kGroup / 32) * kNbCap * 32 * sizeof(int);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_pairs_items<PASS, SOLIDS, COMP>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            if (e != cudaSuccess) return e;
+        }
         GSPH_TIMER_MARK(t, start);
         k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cull_view(a, *sp));
         cudaError_t e = cudaGetLastError();

@@ -238,7 +238,8 @@ struct Launch {
     bool grav_x2;    // paired FP32 (f32x2) form of the gravity kernel
     int grav_nseg;
     int accum;       // GSPH_ACCUM_*
-    int item_grid;   // persistent grid of the culled kernels
+    int item_grid;   // persistent grid of the culled SPH kernel (its resident capacity)
+    int density_grid;  // persistent grid of the culled density kernel
 };
 
 cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
