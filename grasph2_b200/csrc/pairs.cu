@@ -452,15 +452,26 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
             int m = cnt;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+            // software pipeline: the records of neighbour k+1 are in flight while k is computed
+            const float4 zero = make_float4(0, 0, 0, 0);
+            int jn = cnt > 0 ? nb[lane] : 0;
+            float4 qn = a.posm[jn], vn = a.velrho[jn];
+            float4 an = DO_A ? a.jA[jn] : zero, bn = DO_A ? a.jB[jn] : zero;
             for (int k = 0; k < m; ++k) {
+                const float4 q = qn, vj = vn, ja = an, jb = bn;
+                if (k + 1 < cnt) {
+                    jn = nb[(k + 1) * 32 + lane];
+                    qn = a.posm[jn];
+                    vn = a.velrho[jn];
+                    if (DO_A) {
+                        an = a.jA[jn];
+                        bn = a.jB[jn];
+                    }
+                }
                 if (k < cnt) {
-                    const int j = nb[k * 32 + lane];
-                    const float4 q = a.posm[j];
                     const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
                     const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, a.velrho[j],
-                                                DO_A ? a.jA[j] : make_float4(0, 0, 0, 0),
-                                                DO_A ? a.jB[j] : make_float4(0, 0, 0, 0), p);
+                    sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, vj, ja, jb, p);
                 }
             }
             cnt = 0;
@@ -471,15 +482,31 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
         if (!pipe.run(chunks, c1 - c0, [&](const float4* J, int nj) {
                 for (int s0 = 0; s0 < nj; s0 += kChunk) {
                     const int jbase = chunks[chunk_base + s0 / kChunk] * kChunk;
-#pragma unroll 8
-                    for (int jj = 0; jj < kChunk; ++jj) {
-                        const float4 q = J[s0 + jj];
-                        const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        if (in_open_closed(r2, 0u, I.span)) {
-                            nb[cnt * 32 + lane] = jbase + jj;
-                            ++cnt;
+                    // 64 independent tests into eight 8-bit masks (no serial chain), then the set bits
+                    unsigned m8[8];
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) {
+                        unsigned m = 0;
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) {
+                            const float4 q = J[s0 + b * 8 + t];
+                            const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
+                            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            m |= static_cast<unsigned>(in_open_closed(r2, 0u, I.span)) << t;
                         }
+                        m8[b] = m;
+                    }
+                    unsigned lo = m8[0] | (m8[1] << 8) | (m8[2] << 16) | (m8[3] << 24);
+                    unsigned hi = m8[4] | (m8[5] << 8) | (m8[6] << 16) | (m8[7] << 24);
+                    while (lo) {
+                        nb[cnt * 32 + lane] = jbase + __ffs(lo) - 1;
+                        ++cnt;
+                        lo &= lo - 1u;
+                    }
+                    while (hi) {
+                        nb[cnt * 32 + lane] = jbase + 32 + __ffs(hi) - 1;
+                        ++cnt;
+                        hi &= hi - 1u;
                     }
                     // a lane could overflow on the next chunk: process the lists now
                     if (__any_sync(0xffffffffu, cnt > kNbCap - kChunk)) drain();
