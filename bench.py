@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--n", type=int, default=0, help="particle count of the fluid / plummer workloads")
     ap.add_argument("--no-cull", action="store_true", help="all-pairs SPH sweeps (no chunk culling)")
     ap.add_argument("--scalar-fp32", action="store_true", help="scalar instead of paired f32x2 gravity kernel")
+    ap.add_argument("--drift-steps", type=int, default=-1,
+                    help="steps of the energy-drift comparison (plain, compensated, FP64); default 1000 on the "
+                         "impact workload, 0 (off) elsewhere")
+    ap.add_argument("--drift-every", type=int, default=100, help="steps between energy samples of the drift run")
     return ap.parse_args()
 
 
@@ -268,6 +272,59 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def total_energy(d):
+    return d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
+
+
+def energy_drift(params, st, steps, every, stream, forms=("plain", "compensated")):
+    """Total energy along `steps` steps of each FP32 form and of the double-precision form, all from
+    the same float32-representable state. Every `every` steps the derivatives are refreshed at the
+    current positions and the energy is taken at the synchronous velocity v + a dt/2. Returns, per
+    form, max_t |E(t) - E_fp64(t)| / |E_fp64(0)| (the drift against the FP64 trajectory), its own
+    max_t |E(t) - E(0)| / |E(0)|, and the simulated time per wall-second of its stepping (CUDA events
+    around the step launches, diagnostics excluded)."""
+    import torch
+    from grasph2_b200.params import make_options
+    from grasph2_b200.sim import DeviceParticleBuffer
+    from grasph2_b200.state import as_dtype
+    st = as_dtype(as_dtype(st, np.float32), np.float64)
+    n = st["mass"].shape[0]
+    dt = params.fixed_dt
+    runs = {}
+    for form in ("fp64",) + tuple(forms):
+        opt = make_options(precision="double") if form == "fp64" else make_options(accum=form)
+        energies, ms = [], 0.0
+        with DeviceParticleBuffer(params, n, opt) as pb:
+            pb.upload_f64(st, stream=stream)
+            done = 0
+            while True:
+                pb.compute_derivatives(stream)
+                energies.append(total_energy(pb.diagnostics(half_kick=0.5 * dt, stream=stream)))
+                if done >= steps:
+                    break
+                k = min(every, steps - done)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                pb.step(k, stream)
+                b.record(stream)
+                b.synchronize()
+                ms += a.elapsed_time(b)
+                done += k
+        runs[form] = (np.array(energies), ms)
+    e64 = runs["fp64"][0]
+    out = {"steps": steps, "sample_every": every, "reference": "double-precision GPU form",
+           "forms": {}}
+    for form, (e, ms) in runs.items():
+        out["forms"][form] = {
+            "rel_drift_vs_fp64": float(np.abs(e - e64).max() / abs(e64[0])),
+            "rel_energy_change": float(np.abs(e - e[0]).max() / abs(e[0])),
+            "sim_time_per_wall_s": steps * dt / (ms * 1e-3),
+            "steps_per_s": steps / (ms * 1e-3),
+        }
+    return out
+
+
 def flops_pairs(params, n):
     from grasph2_b200._abi import FLAG_BITS as F
     passes = 1
@@ -396,6 +453,12 @@ def main():
         rate, sdesc, cores, kind, _ = cpu_reference_sample(variant, st, args.cpu_budget)
         cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sdesc}
 
+    drift = None
+    if args.drift_steps < 0:
+        args.drift_steps = 1000 if args.workload == "impact" else 0
+    if args.drift_steps > 0:
+        drift = energy_drift(params, st, args.drift_steps, args.drift_every, stream)
+
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -416,6 +479,7 @@ def main():
         "e2e": ({"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                  "d2h_bytes_per_step": d2h} if e2e_steps else None),
         "gpu_launches": gpu_launches,
+        "energy_drift": drift,
     }
     print(json.dumps(line))
     pb.close()

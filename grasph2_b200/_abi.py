@@ -66,7 +66,7 @@ class GsphOptions(ctypes.Structure):
         ("accum", ctypes.c_int32), ("j_split", ctypes.c_int32), ("j_tile", ctypes.c_int32),
         ("i_per_thread", ctypes.c_int32), ("threads", ctypes.c_int32), ("check_finite", ctypes.c_int32),
         ("no_cull", ctypes.c_int32), ("resort_interval", ctypes.c_int32), ("scalar_fp32", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -80,9 +80,12 @@ class GsphHostParticles(ctypes.Structure):
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
-class OracleParticles(ctypes.Structure):
-    """FP64 twin of GsphHostParticles, used by the oracle bindings."""
+class GsphHostParticles64(ctypes.Structure):
+    """gsph_host_particles64: the double-precision host buffers."""
     _fields_ = [(name, _dp) for name, _, _ in ATTRIBUTES]
+
+
+OracleParticles = GsphHostParticles64  # same layout; the oracle bindings use it for their FP64 arrays
 
 
 class GsphDiag(ctypes.Structure):
@@ -126,6 +129,10 @@ _SIGNATURES = {
                                    ctypes.c_void_p]),
     "gsph_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
                                      ctypes.c_void_p]),
+    "gsph_upload_f64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles64),
+                                       ctypes.c_void_p]),
+    "gsph_download_f64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles64),
+                                         ctypes.c_void_p]),
     "gsph_upload_pos64": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_void_p]),
     "gsph_download_pos64": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_void_p]),
     "gsph_compute_derivatives": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "fp64.cuh"
 #include "integrate.cuh"
 #include "pairs.cuh"
 #include "spatial.cuh"
@@ -24,12 +25,16 @@ struct gsph_ctx {
     SpatialArrays sp{};
     int64_t steps_since_sort = 0;
     cudaStream_t side = nullptr;   // gravity runs here, concurrent with the SPH chain (culled path)
+    bool fp64 = false;             // GSPH_PRECISION_DOUBLE: every pass on a64 (fp64.cu)
+    DevArrays64 a64{};
+    DevParams64 dp64{};
+    double* diag64 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int device = 0;
     int sm_count = 148;
     std::vector<void*> allocations;
     float* staging = nullptr;     // 9 * n floats
-    double* staging64 = nullptr;  // 3 * n doubles
+    double* staging64 = nullptr;  // 9 * n doubles
     double* diag_out = nullptr;   // device, 12 doubles
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -210,6 +215,13 @@ const KTimer* slot_timer(gsph_ctx* c, int slot) {
 int derivatives(gsph_ctx* c, cudaStream_t s) {
     const DevParams& p = c->dp;
     cudaError_t e;
+    if (c->fp64) {
+        int launches = 0;
+        e = launch64_derivatives(c->a64, c->dp64, s, launches);
+        c->launches += launches;
+        if (e != cudaSuccess) return cuda_fail(c, e, "FP64 derivatives");
+        return GSPH_OK;
+    }
     if (has(p, GSPH_SPH)) {
         const SpatialArrays* sp = c->L.cull ? &c->sp : nullptr;
         const bool grav_kernel = sp && has(p, GSPH_SELF_GRAVITY);
@@ -275,6 +287,13 @@ int reorder(gsph_ctx* c, cudaStream_t s) {
 const int* ext_map(const gsph_ctx* c) { return c->L.cull ? c->sp.ext_of_int : nullptr; }
 
 int integrate(gsph_ctx* c, int not_first_step, cudaStream_t s) {
+    if (c->fp64) {
+        int launches = 0;
+        const cudaError_t e = launch64_leapfrog(c->a64, c->dp64, not_first_step, s, launches);
+        c->launches += launches;
+        if (e != cudaSuccess) return cuda_fail(c, e, "FP64 leapfrog");
+        return GSPH_OK;
+    }
     cudaError_t e = launch_leapfrog(c->a, c->dp, not_first_step, s);
     if (e != cudaSuccess) return cuda_fail(c, e, "leapfrog");
     c->launches += has(c->dp, GSPH_VARIABLE_TIMESTEP) ? 3 : 1;
@@ -374,6 +393,8 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (o.i_per_thread && o.i_per_thread != 1 && o.i_per_thread != 2 && o.i_per_thread != 4 && o.i_per_thread != 8)
         return fail(nullptr, GSPH_E_INVALID, "i_per_thread: 1, 2, 4 or 8");
     if (o.j_split < 0 || o.j_split > kMaxSplit) return fail(nullptr, GSPH_E_INVALID, "j_split out of range");
+    if (o.precision != GSPH_PRECISION_SINGLE && o.precision != GSPH_PRECISION_DOUBLE)
+        return fail(nullptr, GSPH_E_INVALID, "precision must be GSPH_PRECISION_SINGLE or GSPH_PRECISION_DOUBLE");
 
     gsph_ctx* c = new (std::nothrow) gsph_ctx();
     if (!c) return fail(nullptr, GSPH_E_NOMEM, "host allocation failed");
@@ -393,7 +414,8 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     // launch shape
     Launch& L = c->L;
     L.accum = o.accum;
-    L.cull = (p->flags & GSPH_SPH) && !o.no_cull;
+    c->fp64 = o.precision == GSPH_PRECISION_DOUBLE;
+    L.cull = (p->flags & GSPH_SPH) && !o.no_cull && !c->fp64;
     L.threads = o.threads ? o.threads : 128;
     L.jt = o.j_tile ? o.j_tile : 256;
     const int64_t ntiles = n_pad / L.jt;
@@ -467,8 +489,26 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     a.dt_state = static_cast<float*>(dalloc(c, 4 * sizeof(float), ae));
     a.diag = static_cast<double*>(dalloc(c, diag_scratch_doubles(n) * sizeof(double), ae));
     a.status = static_cast<int*>(dalloc(c, sizeof(int) * 4, ae));
+    if (c->fp64) {
+        DevArrays64& b = c->a64;
+        b.n = n;
+        b.n_pad = n_pad;
+        auto D4 = [&](void) { return static_cast<double4*>(dalloc(c, n_pad * sizeof(double4), ae)); };
+        b.posm = D4(); b.velrho = D4(); b.acc = D4(); b.xvel = D4(); b.sA = D4(); b.sB = D4();
+        b.dA = D4(); b.dB = D4(); b.jA = D4(); b.jB = D4();
+        b.rhodot = static_cast<double*>(dalloc(c, n_pad * sizeof(double), ae));
+        b.balsara = static_cast<double*>(dalloc(c, n_pad * sizeof(double), ae));
+        b.dt_state = static_cast<double*>(dalloc(c, 4 * sizeof(double), ae));
+        c->diag64 = static_cast<double*>(dalloc(c, diag64_scratch_doubles(n_pad) * sizeof(double), ae));
+        const double q = p->normalsep / p->H;
+        double wn = 0.0;
+        if (q <= 1.0) wn = (q < 0.5) ? (6 * q * q * q - 6 * q * q + 1) : 2 * (1 - q) * (1 - q) * (1 - q);
+        wn *= spline_prefactor(p->dimension, p->H);
+        c->dp64 = make_dev_params64(*p, spline_prefactor(p->dimension, p->H), dspline_prefactor(p->dimension, p->H),
+                                    wn > 0 ? 1.0 / wn : 0.0);
+    }
     c->staging = static_cast<float*>(dalloc(c, 9 * n * sizeof(float), ae));
-    c->staging64 = static_cast<double*>(dalloc(c, 3 * n * sizeof(double), ae));
+    c->staging64 = static_cast<double*>(dalloc(c, 9 * n * sizeof(double), ae));
     c->diag_out = static_cast<double*>(dalloc(c, 16 * sizeof(double), ae));
     if (ae != cudaSuccess) {
         release(c);
@@ -479,6 +519,10 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (e == cudaSuccess) e = cudaMemset(a.status, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = launch_init_padding(a, 0);
     if (e == cudaSuccess && L.cull) e = launch_identity_order(c->sp, n_pad, 0);
+    if (e == cudaSuccess && c->fp64) {
+        e = launch64_init(c->a64, 0);
+        if (e == cudaSuccess) e = cudaMemset(c->a64.dt_state, 0, 4 * sizeof(double));
+    }
     if (e == cudaSuccess && L.cull) {
         e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
@@ -516,7 +560,8 @@ int gsph_upload(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void
         if (!(mask >> k & 1u)) continue;
         GSPH_CK(c, cudaMemcpyAsync(c->staging, ptrs[k], comps[k] * c->a.n * sizeof(float), cudaMemcpyHostToDevice, s),
                 "upload copy");
-        GSPH_CK(c, launch_pack(c->a, k, c->staging, ext_map(c), s), "upload pack");
+        if (c->fp64) GSPH_CK(c, launch64_pack(c->a64, k, c->staging, s), "upload pack");
+        else GSPH_CK(c, launch_pack(c->a, k, c->staging, ext_map(c), s), "upload pack");
         c->launches += 1;
     }
     if (mask & GSPH_POS) {
@@ -543,9 +588,68 @@ int gsph_download(gsph_ctx* c, uint32_t mask, gsph_host_particles* dst, void* st
     cudaStream_t s = as_stream(stream);
     for (int k = 0; k < 11; ++k) {
         if (!(mask >> k & 1u)) continue;
-        GSPH_CK(c, launch_unpack(c->a, k, c->staging, ext_map(c), s), "download unpack");
+        if (c->fp64) GSPH_CK(c, launch64_unpack(c->a64, k, c->staging, s), "download unpack");
+        else GSPH_CK(c, launch_unpack(c->a, k, c->staging, ext_map(c), s), "download unpack");
         c->launches += 1;
         GSPH_CK(c, cudaMemcpyAsync(ptrs[k], c->staging, comps[k] * c->a.n * sizeof(float), cudaMemcpyDeviceToHost, s),
+                "download copy");
+    }
+    return check_status(c, s);
+}
+
+int gsph_upload_f64(gsph_ctx* c, uint32_t mask, const gsph_host_particles64* src, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!src) return fail(c, GSPH_E_INVALID, "src is NULL");
+    if (mask & ~GSPH_ALL_ATTRIBS) return fail(c, GSPH_E_INVALID, "unknown attribute bits in mask");
+    const double* ptrs[11] = {src->pos, src->mass, src->vel, src->acc, src->balsara, src->xvel,
+                              src->density, src->density_dt, src->dstress, src->dstress_dt, src->maxvsig};
+    static const int comps[11] = {3, 1, 3, 3, 1, 3, 1, 1, 9, 9, 1};
+    for (int k = 0; k < 11; ++k)
+        if ((mask >> k & 1u) && !ptrs[k]) return fail(c, GSPH_E_INVALID, "attribute pointer is NULL for a set mask bit");
+    cudaStream_t s = as_stream(stream);
+    for (int k = 0; k < 11; ++k) {
+        if (!(mask >> k & 1u)) continue;
+        const int64_t cnt = comps[k] * c->a.n;
+        GSPH_CK(c, cudaMemcpyAsync(c->staging64, ptrs[k], cnt * sizeof(double), cudaMemcpyHostToDevice, s),
+                "upload copy");
+        if (c->fp64) {
+            GSPH_CK(c, launch64_pack_f64(c->a64, k, c->staging64, s), "upload pack");
+        } else {
+            GSPH_CK(c, launch_narrow(c->staging64, c->staging, cnt, s), "upload narrow");
+            GSPH_CK(c, launch_pack(c->a, k, c->staging, ext_map(c), s), "upload pack");
+            if (k == 0) GSPH_CK(c, launch_pack_pos64(c->a, c->staging64, ext_map(c), s), "upload pack");
+            c->launches += 1 + (k == 0);
+        }
+        c->launches += 1;
+    }
+    if (mask & GSPH_POS) return reorder(c, s);
+    return GSPH_OK;
+}
+
+int gsph_download_f64(gsph_ctx* c, uint32_t mask, gsph_host_particles64* dst, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!dst) return fail(c, GSPH_E_INVALID, "dst is NULL");
+    if (mask & ~GSPH_ALL_ATTRIBS) return fail(c, GSPH_E_INVALID, "unknown attribute bits in mask");
+    double* ptrs[11] = {dst->pos, dst->mass, dst->vel, dst->acc, dst->balsara, dst->xvel,
+                        dst->density, dst->density_dt, dst->dstress, dst->dstress_dt, dst->maxvsig};
+    static const int comps[11] = {3, 1, 3, 3, 1, 3, 1, 1, 9, 9, 1};
+    for (int k = 0; k < 11; ++k)
+        if ((mask >> k & 1u) && !ptrs[k]) return fail(c, GSPH_E_INVALID, "attribute pointer is NULL for a set mask bit");
+    cudaStream_t s = as_stream(stream);
+    for (int k = 0; k < 11; ++k) {
+        if (!(mask >> k & 1u)) continue;
+        const int64_t cnt = comps[k] * c->a.n;
+        if (c->fp64) {
+            GSPH_CK(c, launch64_unpack_f64(c->a64, k, c->staging64, s), "download unpack");
+        } else if (k == 0) {
+            GSPH_CK(c, launch_unpack_pos64(c->a, c->staging64, ext_map(c), s), "download unpack");
+        } else {
+            GSPH_CK(c, launch_unpack(c->a, k, c->staging, ext_map(c), s), "download unpack");
+            GSPH_CK(c, launch_widen(c->staging, c->staging64, cnt, s), "download widen");
+            c->launches += 1;
+        }
+        c->launches += 1;
+        GSPH_CK(c, cudaMemcpyAsync(ptrs[k], c->staging64, cnt * sizeof(double), cudaMemcpyDeviceToHost, s),
                 "download copy");
     }
     return check_status(c, s);
@@ -556,7 +660,8 @@ int gsph_upload_pos64(gsph_ctx* c, const double* pos, void* stream) {
     if (!pos) return fail(c, GSPH_E_INVALID, "pos is NULL");
     cudaStream_t s = as_stream(stream);
     GSPH_CK(c, cudaMemcpyAsync(c->staging64, pos, 3 * c->a.n * sizeof(double), cudaMemcpyHostToDevice, s), "upload copy");
-    GSPH_CK(c, launch_pack_pos64(c->a, c->staging64, ext_map(c), s), "upload pack");
+    if (c->fp64) GSPH_CK(c, launch64_pack_pos(c->a64, c->staging64, s), "upload pack");
+    else GSPH_CK(c, launch_pack_pos64(c->a, c->staging64, ext_map(c), s), "upload pack");
     c->launches += 1;
     return reorder(c, s);
 }
@@ -565,7 +670,8 @@ int gsph_download_pos64(gsph_ctx* c, double* pos, void* stream) {
     if (!c) return GSPH_E_INVALID;
     if (!pos) return fail(c, GSPH_E_INVALID, "pos is NULL");
     cudaStream_t s = as_stream(stream);
-    GSPH_CK(c, launch_unpack_pos64(c->a, c->staging64, ext_map(c), s), "download unpack");
+    if (c->fp64) GSPH_CK(c, launch64_unpack_d(c->a64, 0, c->staging64, s), "download unpack");
+    else GSPH_CK(c, launch_unpack_pos64(c->a, c->staging64, ext_map(c), s), "download unpack");
     c->launches += 1;
     GSPH_CK(c, cudaMemcpyAsync(pos, c->staging64, 3 * c->a.n * sizeof(double), cudaMemcpyDeviceToHost, s), "download copy");
     return check_status(c, s);
@@ -657,11 +763,19 @@ int gsph_step(gsph_ctx* c, int32_t nsteps, void* stream) {
 int gsph_current_timestep(gsph_ctx* c, double* dt, void* stream) {
     if (!c || !dt) return c ? fail(c, GSPH_E_INVALID, "dt is NULL") : GSPH_E_INVALID;
     if (!(c->params.flags & GSPH_VARIABLE_TIMESTEP)) {
-        *dt = static_cast<float>(c->params.fixed_dt);  // f1_t fixed_timestep
+        // f1_t fixed_timestep: float, or double in the double-precision mode
+        *dt = c->fp64 ? c->params.fixed_dt : static_cast<float>(c->params.fixed_dt);
+        return GSPH_OK;
+    }
+    cudaStream_t s = as_stream(stream);
+    if (c->fp64) {
+        double d = 0.0;
+        GSPH_CK(c, cudaMemcpyAsync(&d, c->a64.dt_state, sizeof(double), cudaMemcpyDeviceToHost, s), "timestep read");
+        GSPH_CK(c, cudaStreamSynchronize(s), "stream synchronize");
+        *dt = d;
         return GSPH_OK;
     }
     float v = 0.0f;
-    cudaStream_t s = as_stream(stream);
     GSPH_CK(c, cudaMemcpyAsync(&v, c->a.dt_state, sizeof(float), cudaMemcpyDeviceToHost, s), "timestep read");
     GSPH_CK(c, cudaStreamSynchronize(s), "stream synchronize");
     *dt = v;
@@ -672,7 +786,8 @@ int gsph_diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream
     if (!c) return GSPH_E_INVALID;
     if (!out) return fail(c, GSPH_E_INVALID, "out is NULL");
     cudaStream_t s = as_stream(stream);
-    GSPH_CK(c, launch_diagnostics(c->a, c->dp, half_kick, c->diag_out, s), "diagnostics");
+    if (c->fp64) GSPH_CK(c, launch64_diagnostics(c->a64, c->dp64, half_kick, c->diag64, c->diag_out, s), "diagnostics");
+    else GSPH_CK(c, launch_diagnostics(c->a, c->dp, half_kick, c->diag_out, s), "diagnostics");
     c->launches += 2;
     double h[12];
     GSPH_CK(c, cudaMemcpyAsync(h, c->diag_out, sizeof h, cudaMemcpyDeviceToHost, s), "diagnostics read");

@@ -93,13 +93,14 @@ def params_to_dict(p):
 
 
 def make_options(accum="plain", j_split=0, j_tile=0, i_per_thread=0, threads=0, check_finite=0, cull=True,
-                 resort_interval=0, scalar_fp32=False):
+                 resort_interval=0, scalar_fp32=False, precision="single"):
     o = GsphOptions()
     o.accum = {"plain": ACCUM_PLAIN, "compensated": ACCUM_COMPENSATED}[accum] if isinstance(accum, str) else accum
     o.j_split, o.j_tile, o.i_per_thread, o.threads, o.check_finite = j_split, j_tile, i_per_thread, threads, check_finite
     o.no_cull = 0 if cull else 1
     o.resort_interval = resort_interval
     o.scalar_fp32 = 1 if scalar_fp32 else 0
+    o.precision = {"single": 0, "double": 1}[precision] if isinstance(precision, str) else int(precision)
     return o
 
 

@@ -111,6 +111,24 @@ class DeviceParticleBuffer:
         self._check(self.lib.gsph_download(self._ctx, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
         return {k: st[k] for k in names} if attributes is not None else st
 
+    def upload_f64(self, state, attributes=None, stream=None):
+        """Double-precision host buffers (the reference's DOUBLE_PRECISION layout)."""
+        names = [k for k in ATTR_BITS if k in state] if attributes is None else list(attributes)
+        st = {k: np.ascontiguousarray(state[k], dtype=np.float64) for k in names}
+        for k, v in st.items():
+            if v.shape[0] != self.n:
+                raise ValueError("attribute %s has %d rows, buffer holds %d" % (k, v.shape[0], self.n))
+        hp = pointer_struct(st, _abi.GsphHostParticles64, ctypes.c_double)
+        self._check(self.lib.gsph_upload_f64(self._ctx, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
+        return self
+
+    def download_f64(self, attributes=None, stream=None):
+        names = list(ATTR_BITS) if attributes is None else list(attributes)
+        st = new_state(self.n, np.float64)
+        hp = pointer_struct({k: st[k] for k in names}, _abi.GsphHostParticles64, ctypes.c_double)
+        self._check(self.lib.gsph_download_f64(self._ctx, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
+        return {k: st[k] for k in names}
+
     def upload_pos64(self, pos, stream=None):
         pos = np.ascontiguousarray(pos, dtype=np.float64)
         assert pos.shape == (self.n, 3)

@@ -170,8 +170,15 @@ typedef struct gsph_options {
                                 positions are uploaded) */
     int32_t scalar_fp32;     /* nonzero: scalar FP32 gravity kernel instead of the paired f32x2 form
                                 (identical results; for comparison) */
-    int32_t reserved[7];
+    int32_t precision;       /* GSPH_PRECISION_SINGLE (default) or GSPH_PRECISION_DOUBLE: the reference's
+                                SINGLE_PRECISION / DOUBLE_PRECISION switch (settings/precisionSettings.h:16-17).
+                                Double runs every pass in FP64 with plain all-pairs tiles (no culling,
+                                accum ignored); host transfers stay float, plus the FP64 position calls */
+    int32_t reserved[6];
 } gsph_options;
+
+#define GSPH_PRECISION_SINGLE 0
+#define GSPH_PRECISION_DOUBLE 1
 
 int gsph_options_defaults(gsph_options* o);
 
@@ -191,6 +198,25 @@ int gsph_destroy(gsph_ctx* ctx);
 int gsph_upload(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
 /* Copy device -> host for the attributes in `attr_mask`; synchronises `stream`. */
 int gsph_download(gsph_ctx* ctx, uint32_t attr_mask, gsph_host_particles* dst, void* stream);
+/* The same transfers in double precision: the host buffers of the reference's DOUBLE_PRECISION build
+ * (src/types.h:32-43, f1_t = double). With GSPH_PRECISION_DOUBLE the values pass unrounded; in single
+ * precision they are rounded to float on upload and widened on download. */
+typedef struct gsph_host_particles64 {
+    double* pos;        /* 3N */
+    double* mass;       /* N  */
+    double* vel;        /* 3N */
+    double* acc;        /* 3N */
+    double* balsara;    /* N  */
+    double* xvel;       /* 3N */
+    double* density;    /* N  */
+    double* density_dt; /* N  */
+    double* dstress;    /* 9N */
+    double* dstress_dt; /* 9N */
+    double* maxvsig;    /* N  */
+} gsph_host_particles64;
+int gsph_upload_f64(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles64* src, void* stream);
+int gsph_download_f64(gsph_ctx* ctx, uint32_t attr_mask, gsph_host_particles64* dst, void* stream);
+
 /* FP64 positions (3N, x0,y0,z0,...): upload overrides the FP32 positions; download reads the master. */
 int gsph_upload_pos64(gsph_ctx* ctx, const double* pos, void* stream);
 int gsph_download_pos64(gsph_ctx* ctx, double* pos, void* stream);
