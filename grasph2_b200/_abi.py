@@ -151,6 +151,24 @@ _SIGNATURES = {
     "gsph_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GsphProfile)]),
     "gsph_profile_reset": (ctypes.c_int, [ctypes.c_void_p]),
     "gsph_measure_fp32_peak": (ctypes.c_int, [ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+    "gsph_ensemble_create": (ctypes.c_int, [ctypes.POINTER(GsphParams), ctypes.POINTER(GsphOptions), ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_void_p)]),
+    "gsph_ensemble_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_ensemble_offsets": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_ensemble_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
+                                            ctypes.c_void_p]),
+    "gsph_ensemble_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
+                                              ctypes.c_void_p]),
+    "gsph_ensemble_upload_pos64": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "gsph_ensemble_download_pos64": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                                    ctypes.c_void_p]),
+    "gsph_ensemble_compute_derivatives": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_ensemble_integrate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "gsph_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "gsph_ensemble_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
+                                                 ctypes.c_void_p]),
+    "gsph_ensemble_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_void_p]),
 }

@@ -302,6 +302,9 @@ int integrate(gsph_ctx* c, int not_first_step, cudaStream_t s) {
 
 }  // namespace
 
+// the parameter block of the kernels, for the other translation units (ensemble.cu)
+DevParams gsph_dev_params(const gsph_params& p) { return make_dev_params(p); }
+
 extern "C" {
 
 int gsph_params_reference_defaults(gsph_params* p) {

@@ -3,92 +3,13 @@
 //
 // HBM-bound: each kernel touches each particle once with coalesced float4 / double streams.
 #include "integrate.cuh"
+#include "sph.cuh"
 
 namespace gsph {
 
 namespace {
 
 inline unsigned blocks_for(int64_t n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
-
-__device__ __forceinline__ float murnaghan(const DevParams& p, float rho) {
-    return p.bulk / p.dbulk * (powf(rho / p.rho0, p.dbulk) - 1.0f);
-}
-
-// plasticity (src/sph/models.h:194-205) on the six stored components of the symmetric S:
-// J2 = 1/2 sum_de S_de^2 counts each off-diagonal twice; S *= Y^2/(3 J2) when that is < 1
-__device__ __forceinline__ void plasticity(float4& a, float4& b, float Y) {
-    const float J2 = 0.5f * (a.x * a.x + a.y * a.y + a.z * a.z + 2.0f * (a.w * a.w + b.x * b.x + b.y * b.y));
-    const float f = Y * Y / (3.0f * J2);
-    if (f < 1.0f) {
-        a.x *= f; a.y *= f; a.z *= f; a.w *= f;
-        b.x *= f; b.y *= f;
-    }
-}
-
-// the per-particle update shared by fixedTsLeapfrog (integration.h:90-124) and
-// variableTsLeapfrog_useNewTimestep (:171-217): kick, drift (FP64 master position), density and
-// stress update, plasticity, box boundary
-__device__ __forceinline__ void kick_drift(const DevArrays& a, const DevParams& p, int64_t i, float kick_dt, float dt) {
-    float4 vr = a.velrho[i];
-    const float4 ac = a.acc[i];
-    vr.x = fmaf(ac.x, kick_dt, vr.x);
-    vr.y = fmaf(ac.y, kick_dt, vr.y);
-    vr.z = fmaf(ac.z, kick_dt, vr.z);
-    float ux = vr.x, uy = vr.y, uz = vr.z;
-    const bool sph = has(p, GSPH_SPH);
-    if (sph && has(p, GSPH_XSPH)) {
-        const float4 xv = a.xvel[i];
-        ux = fmaf(p.xsph, xv.x, ux);
-        uy = fmaf(p.xsph, xv.y, uy);
-        uz = fmaf(p.xsph, xv.z, uz);
-    }
-    const int64_t np = a.n_pad;
-    double x = a.pos64[i], y = a.pos64[np + i], z = a.pos64[2 * np + i];
-    x += static_cast<double>(ux) * static_cast<double>(dt);
-    y += static_cast<double>(uy) * static_cast<double>(dt);
-    z += static_cast<double>(uz) * static_cast<double>(dt);
-    if (sph) {
-        if (has(p, GSPH_INTEGRATE_DENSITY)) {
-            float rho = fmaf(a.rhodot[i], dt, vr.w);
-            if (rho < 0.0f) rho = 0.0f;
-            vr.w = rho;
-        }
-        if (has(p, GSPH_SOLIDS)) {
-            float4 sa = a.sA[i], sb = a.sB[i];
-            const float4 da = a.dA[i], db = a.dB[i];
-            sa.x = fmaf(da.x, dt, sa.x); sa.y = fmaf(da.y, dt, sa.y); sa.z = fmaf(da.z, dt, sa.z);
-            sa.w = fmaf(da.w, dt, sa.w); sb.x = fmaf(db.x, dt, sb.x); sb.y = fmaf(db.y, dt, sb.y);
-            if (has(p, GSPH_PLASTICITY_MC))  // doPlasticity (integration.h:24-31), updated density
-                plasticity(sa, sb, p.tanfr * murnaghan(p, vr.w) + p.cohesion);
-            else if (has(p, GSPH_PLASTICITY_MIESE))
-                plasticity(sa, sb, p.Y);
-            a.sA[i] = sa;
-            a.sB[i] = sb;
-        }
-    }
-    if (has(p, GSPH_SIMPLE_BOX_BOUNDARY)) {  // handleBoundaryConditions (integration.h:33-73)
-        const float m = 1.0f + p.box_refl;
-        double* xc[3] = {&x, &y, &z};
-        float* vc[3] = {&vr.x, &vr.y, &vr.z};
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            if (d == 2 && p.dim != 3) break;
-            if (*xc[d] > static_cast<double>(p.box_max[d])) {
-                *xc[d] = p.box_max[d];
-                *vc[d] -= m * *vc[d];
-            } else if (*xc[d] < static_cast<double>(p.box_min[d])) {
-                *xc[d] = p.box_min[d];
-                *vc[d] -= m * *vc[d];
-            }
-        }
-    }
-    a.pos64[i] = x;
-    a.pos64[np + i] = y;
-    a.pos64[2 * np + i] = z;
-    const float mass = a.posm[i].w;
-    a.posm[i] = make_float4(static_cast<float>(x), static_cast<float>(y), static_cast<float>(z), mass);
-    a.velrho[i] = vr;
-}
 
 __global__ void k_leapfrog_fixed(DevArrays a, DevParams p, float kick_dt) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -178,33 +99,9 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag(DevArrays a, DevParams p,
     for (int k = 0; k < kDiagFields; ++k) f[k] = 0.0;
     double xi = 0, yi = 0, zi = 0, mi = 0;
     if (i < a.n) {
-        const float4 pm = a.posm[i];
-        const float4 vr = a.velrho[i];
-        const float4 ac = a.acc[i];
-        mi = pm.w;
+        diag_terms(a, p, i, half_kick, f);
+        mi = a.posm[i].w;
         xi = a.pos64[i]; yi = a.pos64[np + i]; zi = a.pos64[2 * np + i];
-        const double vx = vr.x + half_kick * ac.x, vy = vr.y + half_kick * ac.y, vz = vr.z + half_kick * ac.z;
-        f[0] = 0.5 * mi * (vx * vx + vy * vy + vz * vz);
-        f[4] = mi * vx; f[5] = mi * vy; f[6] = mi * vz;
-        f[7] = mi * (yi * vz - zi * vy); f[8] = mi * (zi * vx - xi * vz); f[9] = mi * (xi * vy - yi * vx);
-        f[10] = mi;
-        if (has(p, GSPH_SPH)) {
-            const double rho = vr.w, r0 = p.rho0;
-            if (has(p, GSPH_SOLIDS)) {
-                const double K = p.bulk, nn = p.dbulk;
-                double u;
-                if (fabs(nn - 1.0) < 1e-12) u = K / r0 * (log(rho / r0) + r0 / rho - 1.0);
-                else u = K / nn * ((pow(rho, nn - 1.0) - pow(r0, nn - 1.0)) / ((nn - 1.0) * pow(r0, nn)) + (1.0 / rho - 1.0 / r0));
-                f[2] = mi * u;
-                const float4 sa = a.sA[i], sb = a.sB[i];
-                const double ss = double(sa.x) * sa.x + double(sa.y) * sa.y + double(sa.z) * sa.z +
-                                  2.0 * (double(sa.w) * sa.w + double(sb.x) * sb.x + double(sb.y) * sb.y);
-                f[3] = mi * ss / (4.0 * p.shear * rho);
-            } else {
-                const double c2 = double(p.c) * p.c;
-                f[2] = mi * c2 * (log(rho / r0) + r0 / rho - 1.0);
-            }
-        }
     }
     // pair potential: -G m_i sum_{j>i} m_j / sqrt(r^2 + eps^2), j-tiles of blockDim through shared memory
     if (has(p, GSPH_SELF_GRAVITY)) {

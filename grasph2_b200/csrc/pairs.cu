@@ -16,52 +16,11 @@
 #include <cfloat>
 
 #include "pairs.cuh"
+#include "sph.cuh"
 
 namespace gsph {
 
 namespace {
-
-// ---- SPH building blocks (src/sph/kernel.h, eos.h, models.h) ---------------------------------
-// spline polynomial of Wspline without its prefactor, q in [0,1] (kernel.h:130-136)
-__device__ __forceinline__ float w_poly(float q) {
-    if (q > 1.0f) return 0.0f;
-    if (q < 0.5f) return 6.0f * q * q * q - 6.0f * q * q + 1.0f;
-    const float a = 1.0f - q;
-    return 2.0f * a * a * a;
-}
-// polynomial of dWspline without its prefactor (kernel.h:169-175)
-__device__ __forceinline__ float dw_poly(float q) {
-    if (q > 1.0f) return 0.0f;
-    if (q < 0.5f) return 3.0f * q * q - 2.0f * q;
-    const float a = 1.0f - q;
-    return -a * a;
-}
-// pressure of the selected EOS (eos.h:88-96; computeDerivatives.h:200,205)
-__device__ __forceinline__ float eos_pressure(const DevParams& p, float rho) {
-    if (has(p, GSPH_SOLIDS)) return p.bulk / p.dbulk * (powf(rho / p.rho0, p.dbulk) - 1.0f);
-    return p.c2 * (rho - p.rho0);
-}
-// j-record of one particle: sigma/rho^2 in (A, B) with B.z = Balsara value
-__device__ __forceinline__ void make_jrecord(const DevParams& p, float rho, float4 sA, float4 sB, float bal,
-                                             float4& jA, float4& jB) {
-    const float pres = eos_pressure(p, rho);
-    if (has(p, GSPH_SOLIDS)) {
-        jA = make_float4((sA.x - pres) / (rho * rho), (sA.y - pres) / (rho * rho), (sA.z - pres) / (rho * rho),
-                         sA.w / (rho * rho));
-        jB = make_float4(sB.x / (rho * rho), sB.y / (rho * rho), bal, 0.0f);
-    } else {
-        const float s = -pres / (rho * rho);
-        jA = make_float4(s, s, s, 0.0f);
-        jB = make_float4(0.0f, 0.0f, bal, 0.0f);
-    }
-}
-// artificialStress / artificialPressure (models.h:212-223)
-__device__ __forceinline__ float art(float mateps, float s) { return s > 0.0f ? -mateps * s : 0.0f; }
-
-// neighbour test 0 < x <= hi for a non-negative float x, on the bit patterns: one add, one compare
-__device__ __forceinline__ bool in_open_closed(float x, uint32_t lo_bits, uint32_t span_bits) {
-    return (__float_as_uint(x) - lo_bits - 1u) < span_bits;
-}
 
 // ================================================================================================
 // density
@@ -207,120 +166,6 @@ __global__ void k_prepare(DevArrays a, DevParams p) {
 // ================================================================================================
 // SPH pair passes
 // ================================================================================================
-struct PairAcc {
-    float f[F_COUNT];
-};
-
-// Per-i state of the SPH pair passes and the run-time switches the pair body reads.
-struct ISph {
-    float4 pi, vi, jAi, jBi;
-    float bi;
-    float ai_xx, ai_yy, ai_zz, ai_xy, ai_xz, ai_yz;  // artificial stress of i (computeDerivatives.h:210-217)
-    bool bals, av, xsph, arts, curl, divv_on;
-    float eps2;           // added to r^2 when gravity shares the squared distance
-    uint32_t lo, span;    // neighbour window 0 < r^2 <= H^2 on the bit patterns of r^2 + eps2
-};
-
-template <int PASS, bool SOLIDS>
-__device__ __forceinline__ ISph load_isph(const DevArrays& a, const DevParams& p, int64_t i, float eps2) {
-    constexpr bool DO_A = PASS != PASS_VGRAD;
-    ISph s;
-    s.pi = a.posm[i];
-    s.vi = a.velrho[i];
-    s.jAi = make_float4(0, 0, 0, 0);
-    s.jBi = make_float4(0, 0, 0, 0);
-    if (DO_A) {
-        s.jAi = a.jA[i];
-        s.jBi = a.jB[i];
-    }
-    s.bals = has(p, GSPH_BALSARA_SWITCH);
-    s.av = has(p, GSPH_ARTIFICIAL_VISCOSITY);
-    s.xsph = has(p, GSPH_XSPH);
-    s.arts = has(p, GSPH_ARTIFICIAL_STRESS);
-    s.curl = !SOLIDS && s.bals;
-    s.divv_on = s.bals || has(p, GSPH_INTEGRATE_DENSITY);
-    s.bi = s.bals ? s.jBi.z : 1.0f;
-    s.ai_xx = art(p.mateps, s.jAi.x); s.ai_yy = art(p.mateps, s.jAi.y); s.ai_zz = art(p.mateps, s.jAi.z);
-    s.ai_xy = art(p.mateps, s.jAi.w); s.ai_xz = art(p.mateps, s.jBi.x); s.ai_yz = art(p.mateps, s.jBi.y);
-    s.eps2 = eps2;
-    s.lo = __float_as_uint(eps2);
-    s.span = __float_as_uint(p.H2 + eps2) - s.lo;
-    return s;
-}
-
-// The SPH terms of one neighbour pair (0 < r <= H): velocity-gradient terms
-// (computeDerivatives.h:118-141) and acceleration terms (:237-295). d = x_j - x_i, r2 = |d|^2.
-template <int PASS, bool SOLIDS>
-__device__ __forceinline__ void sph_neighbour(PairAcc& T, float& maxv, const ISph& I, float mj, float dx, float dy,
-                                              float dz, float r2, float4 vj, float4 ja, float4 jb, const DevParams& p) {
-    constexpr bool DO_V = PASS != PASS_ACC;
-    constexpr bool DO_A = PASS != PASS_VGRAD;
-    const float inv_r = rsqrtf(r2);
-    const float r = r2 * inv_r;
-    const float qq = r * p.inv_h;
-    // grad_i W = (dW/r) r_ij with r_ij = -d:  g = -(dW/r) d
-    const float gf = -p.dw_pref * dw_poly(qq) * inv_r;
-    const float gx = gf * dx, gy = gf * dy, gz = gf * dz;
-    const float vx = I.vi.x - vj.x, vy = I.vi.y - vj.y, vz = I.vi.z - vj.z;  // v_ij
-    const float rhoj = vj.w;
-    if (DO_V) {
-        const float mr = mj / rhoj;
-        if (SOLIDS) {  // addStrainRateAndRotationRate (models.h:225-248)
-            const float t = -0.5f * mr;
-            T.f[F_E00] = fmaf(t, vx * gx + vx * gx, T.f[F_E00]);
-            T.f[F_E11] = fmaf(t, vy * gy + vy * gy, T.f[F_E11]);
-            T.f[F_E22] = fmaf(t, vz * gz + vz * gz, T.f[F_E22]);
-            T.f[F_E01] = fmaf(t, vx * gy + vy * gx, T.f[F_E01]);
-            T.f[F_E02] = fmaf(t, vx * gz + vz * gx, T.f[F_E02]);
-            T.f[F_E12] = fmaf(t, vy * gz + vz * gy, T.f[F_E12]);
-            T.f[F_W01] = fmaf(t, vx * gy - vy * gx, T.f[F_W01]);
-            T.f[F_W02] = fmaf(t, vx * gz - vz * gx, T.f[F_W02]);
-            T.f[F_W12] = fmaf(t, vy * gz - vz * gy, T.f[F_W12]);
-        } else if (I.curl) {
-            T.f[F_C0] = fmaf(mr, vy * gz - vz * gy, T.f[F_C0]);
-            T.f[F_C1] = fmaf(mr, vz * gx - vx * gz, T.f[F_C1]);
-            T.f[F_C2] = fmaf(mr, vx * gy - vy * gx, T.f[F_C2]);
-        }
-        if (I.divv_on) T.f[F_DIVV] = fmaf(-mr, vx * gx + vy * gy + vz * gz, T.f[F_DIVV]);
-    }
-    if (DO_A) {
-        float sxx = I.jAi.x + ja.x, syy = I.jAi.y + ja.y, szz = I.jAi.z + ja.z;
-        float sxy = I.jAi.w + ja.w, sxz = I.jBi.x + jb.x, syz = I.jBi.y + jb.y;
-        if (I.arts) {
-            const float f = powf(p.w_pref * w_poly(qq) * p.inv_w_normalsep, p.matexp);
-            sxx += f * (I.ai_xx + art(p.mateps, ja.x));
-            syy += f * (I.ai_yy + art(p.mateps, ja.y));
-            szz += f * (I.ai_zz + art(p.mateps, ja.z));
-            sxy += f * (I.ai_xy + art(p.mateps, ja.w));
-            sxz += f * (I.ai_xz + art(p.mateps, jb.x));
-            syz += f * (I.ai_yz + art(p.mateps, jb.y));
-        }
-        T.f[F_AX] = fmaf(mj, sxx * gx + sxy * gy + sxz * gz, T.f[F_AX]);
-        T.f[F_AY] = fmaf(mj, sxy * gx + syy * gy + syz * gz, T.f[F_AY]);
-        T.f[F_AZ] = fmaf(mj, sxz * gx + syz * gy + szz * gz, T.f[F_AZ]);
-        if (I.av) {  // artificialViscosity (models.h:158-185)
-            const float w = -(dx * vx + dy * vy + dz * vz) * inv_r;  // r_ij . v_ij / r
-            if (w < 0.0f) {
-                const float vsig = p.c + p.c - p.beta * w;
-                const float rhoij = (I.vi.w + rhoj) * 0.5f;
-                const float bj = I.bals ? jb.z : 1.0f;
-                const float II = -0.25f * (I.bi + bj) * p.alpha * w * vsig / rhoij;
-                const float m2 = -mj * II;
-                T.f[F_AX] = fmaf(m2, gx, T.f[F_AX]);
-                T.f[F_AY] = fmaf(m2, gy, T.f[F_AY]);
-                T.f[F_AZ] = fmaf(m2, gz, T.f[F_AZ]);
-                if (I.bals) maxv = fmaxf(maxv, vsig);
-            }
-        }
-        if (I.xsph) {
-            const float f = 2.0f * mj / (I.vi.w + rhoj) * (p.w_pref * w_poly(qq));
-            T.f[F_XV0] = fmaf(f, -vx, T.f[F_XV0]);
-            T.f[F_XV1] = fmaf(f, -vy, T.f[F_XV1]);
-            T.f[F_XV2] = fmaf(f, -vz, T.f[F_XV2]);
-        }
-    }
-}
-
 // The all-pairs body over nj staged j-records (P: posm, V: velrho, JA/JB: sigma/rho^2): gravity when
 // GRAV != 0 (computeDerivatives.h:229-235, G applied by the finish kernel), then the SPH terms of
 // every neighbour. GRAV: 0 off, 1 softened (eps > 0), 2 unsoftened (eps == 0: self pair gives 0).
@@ -545,25 +390,6 @@ __device__ __forceinline__ float seg_sum(const PartView& v, int64_t i, int f) {
     return s;
 }
 
-// environmentAcceleration (computeDerivatives.h:33-47); the Clohessy-Wiltshire terms are scalars
-// added to all three components, as the reference's f3_t += f1_t does
-__device__ __forceinline__ void environment(const DevParams& p, float4 x, float4 v, float& ax, float& ay, float& az) {
-    if (has(p, GSPH_CLOHESSY_WILTSHIRE)) {
-        const float n = p.cw_n;
-        const float s1 = 3 * n * n * x.x + 2 * n * v.y;
-        ax += s1; ay += s1; az += s1;
-        const float s2 = -2 * n * v.x;
-        ax += s2; ay += s2; az += s2;
-        const float s3 = -n * n * x.z;
-        ax += s3; ay += s3; az += s3;
-    }
-    if (has(p, GSPH_CONSTANT_ACCELERATION)) {
-        ax += p.const_acc[0];
-        ay += p.const_acc[1];
-        az += p.const_acc[2];
-    }
-}
-
 // gravity partials of the separate all-pairs gravity kernel (culled path), summed like seg_sum
 template <bool COMP>
 __device__ __forceinline__ float gpart_sum(const DevArrays& a, int gnseg, int64_t i, int c) {
@@ -587,75 +413,20 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, PartView pv, int gnseg)
     if (PASS != PASS_VGRAD && has(p, GSPH_VARIABLE_TIMESTEP) && i == 0)
         a.dt_state[1] = p.max_dt;  // nextTS reset of calcAcceleration::do_after (:306-309)
     if (i >= a.n) return;
-    const float4 vi = a.velrho[i];
-    if (PASS != PASS_ACC) {  // calcBalsaraDensityDTDStressDT::do_after (:144-161)
-        const float divv = seg_sum<MASK, COMP>(pv, i, F_DIVV);
-        float c0 = 0, c1 = 0, c2 = 0;
-        if (SOLIDS) {
-            const float e[6] = {seg_sum<MASK, COMP>(pv, i, F_E00), seg_sum<MASK, COMP>(pv, i, F_E11),
-                                seg_sum<MASK, COMP>(pv, i, F_E22), seg_sum<MASK, COMP>(pv, i, F_E01),
-                                seg_sum<MASK, COMP>(pv, i, F_E02), seg_sum<MASK, COMP>(pv, i, F_E12)};
-            const float w01 = seg_sum<MASK, COMP>(pv, i, F_W01), w02 = seg_sum<MASK, COMP>(pv, i, F_W02),
-                        w12 = seg_sum<MASK, COMP>(pv, i, F_W12);
-            const float E[3][3] = {{e[0], e[3], e[4]}, {e[3], e[1], e[5]}, {e[4], e[5], e[2]}};
-            const float R[3][3] = {{0.0f, w01, w02}, {-w01, 0.0f, w12}, {-w02, -w12, 0.0f}};
-            const float4 sa = a.sA[i], sb = a.sB[i];
-            const float Sm[3][3] = {{sa.x, sa.w, sb.x}, {sa.w, sa.y, sb.y}, {sb.x, sb.y, sa.z}};
-            const float tr = E[0][0] + E[1][1] + E[2][2];
-            float D[3][3];
-            // dstress_dt (models.h:250-268): Hooke deviatoric rate + Jaumann rotation terms
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-#pragma unroll
-                for (int ee = 0; ee < 3; ++ee) {
-                    float v = 2.0f * p.shear * E[d][ee];
-                    if (d == ee) v -= 2.0f * p.shear * tr / 3.0f;
-#pragma unroll
-                    for (int f = 0; f < 3; ++f) v += Sm[d][f] * R[ee][f] + Sm[ee][f] * R[d][f];
-                    D[d][ee] = v;
-                }
-            a.dA[i] = make_float4(D[0][0], D[1][1], D[2][2], 0.5f * (D[0][1] + D[1][0]));
-            a.dB[i] = make_float4(0.5f * (D[0][2] + D[2][0]), 0.5f * (D[1][2] + D[2][1]), 0.0f, 0.0f);
-            c0 = -2.0f * R[1][2];
-            c1 = -2.0f * R[2][0];
-            c2 = -2.0f * R[0][1];
-        } else {
-            c0 = seg_sum<MASK, COMP>(pv, i, F_C0);
-            c1 = seg_sum<MASK, COMP>(pv, i, F_C1);
-            c2 = seg_sum<MASK, COMP>(pv, i, F_C2);
-        }
-        a.rhodot[i] = has(p, GSPH_INTEGRATE_DENSITY) ? -vi.w * divv : 0.0f;
-        float bal = 0.0f;
-        if (has(p, GSPH_BALSARA_SWITCH)) {  // balsaraSwitch (models.h:187-192)
-            const float absdiv = fabsf(divv);
-            const float abscurl = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
-            bal = absdiv / (absdiv + abscurl + p.balsara_floor);
-            float4 jb = a.jB[i];
-            jb.z = bal;
-            a.jB[i] = jb;
-        }
-        a.balsara[i] = bal;
-    }
-    if (PASS != PASS_VGRAD) {  // calcAcceleration::do_after (:301-312)
-        float ax = seg_sum<MASK, COMP>(pv, i, F_AX);
-        float ay = seg_sum<MASK, COMP>(pv, i, F_AY);
-        float az = seg_sum<MASK, COMP>(pv, i, F_AZ);
+    float g[3] = {0.0f, 0.0f, 0.0f};
+    bool grav = false;
+    if (PASS != PASS_VGRAD) {
         if (GRAV) {
-            ax = fmaf(p.G, seg_sum<MASK, COMP>(pv, i, F_GX), ax);
-            ay = fmaf(p.G, seg_sum<MASK, COMP>(pv, i, F_GY), ay);
-            az = fmaf(p.G, seg_sum<MASK, COMP>(pv, i, F_GZ), az);
+            g[0] = seg_sum<MASK, COMP>(pv, i, F_GX);
+            g[1] = seg_sum<MASK, COMP>(pv, i, F_GY);
+            g[2] = seg_sum<MASK, COMP>(pv, i, F_GZ);
+            grav = true;
+        } else if (gnseg > 0) {
+            for (int c = 0; c < 3; ++c) g[c] = gpart_sum<COMP>(a, gnseg, i, c);
+            grav = true;
         }
-        if (gnseg > 0) {
-            ax = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 0), ax);
-            ay = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 1), ay);
-            az = fmaf(p.G, gpart_sum<COMP>(a, gnseg, i, 2), az);
-        }
-        const float4 x = a.posm[i];
-        environment(p, x, vi, ax, ay, az);
-        a.acc[i] = make_float4(ax, ay, az, seg_sum<MASK, COMP>(pv, i, F_MAXV));
-        a.xvel[i] = make_float4(seg_sum<MASK, COMP>(pv, i, F_XV0), seg_sum<MASK, COMP>(pv, i, F_XV1),
-                                seg_sum<MASK, COMP>(pv, i, F_XV2), 0.0f);
     }
+    sph_finish<PASS, SOLIDS>(a, p, i, [&](int f) { return seg_sum<MASK, COMP>(pv, i, f); }, grav, g);
 }
 
 // ================================================================================================

@@ -188,6 +188,107 @@ class DeviceParticleBuffer:
 
 
 # reference-named free functions --------------------------------------------------------------
+class Ensemble:
+    """S independent simulations of uneven sizes with one parameter set (gsph_ensemble_*). Host states
+    hold the simulations back to back, simulation k in rows offsets[k]:offsets[k+1]."""
+
+    def __init__(self, params, counts, options=None):
+        self.lib = load_library()
+        self.params = params
+        counts = np.ascontiguousarray(counts, dtype=np.int64)
+        self.nsims = int(counts.shape[0])
+        self._h = ctypes.c_void_p()
+        opt = ctypes.byref(options) if options is not None else None
+        rc = self.lib.gsph_ensemble_create(ctypes.byref(params), opt, self.nsims,
+                                           counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(self._h))
+        if rc != 0:
+            raise GsphError(rc, self.lib.gsph_ensemble_last_error(None).decode())
+        off = np.zeros(self.nsims + 1, dtype=np.int64)
+        self._check(self.lib.gsph_ensemble_offsets(self._h, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        self.offsets = off
+        self.n = int(off[-1])
+
+    def close(self):
+        if self._h:
+            self.lib.gsph_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise GsphError(rc, self.lib.gsph_ensemble_last_error(self._h).decode())
+
+    def upload(self, state, attributes=None, stream=None):
+        names = [k for k in ATTR_BITS if k in state] if attributes is None else list(attributes)
+        st = {k: np.ascontiguousarray(state[k], dtype=np.float32) for k in names}
+        for k, v in st.items():
+            if v.shape[0] != self.n:
+                raise ValueError("attribute %s has %d rows, the ensemble holds %d" % (k, v.shape[0], self.n))
+        hp = pointer_struct(st, GsphHostParticles, ctypes.c_float)
+        self._check(self.lib.gsph_ensemble_upload(self._h, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
+        return self
+
+    def download(self, attributes=None, stream=None, out=None):
+        names = list(ATTR_BITS) if attributes is None else list(attributes)
+        st = out if out is not None else new_state(self.n, np.float32)
+        hp = pointer_struct({k: st[k] for k in names}, GsphHostParticles, ctypes.c_float)
+        self._check(self.lib.gsph_ensemble_download(self._h, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
+        return {k: st[k] for k in names}
+
+    def upload_pos64(self, pos, stream=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        if pos.shape != (self.n, 3):
+            raise ValueError("pos must have shape (%d, 3)" % self.n)
+        self._check(self.lib.gsph_ensemble_upload_pos64(self._h, pos.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                        _stream_handle(stream)))
+
+    def download_pos64(self, stream=None):
+        pos = np.empty((self.n, 3), dtype=np.float64)
+        self._check(self.lib.gsph_ensemble_download_pos64(self._h, pos.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                          _stream_handle(stream)))
+        return pos
+
+    def compute_derivatives(self, stream=None):
+        self._check(self.lib.gsph_ensemble_compute_derivatives(self._h, _stream_handle(stream)))
+
+    def integrate(self, not_first_step=True, stream=None):
+        self._check(self.lib.gsph_ensemble_integrate(self._h, int(bool(not_first_step)), _stream_handle(stream)))
+
+    def step(self, nsteps=1, stream=None):
+        self._check(self.lib.gsph_ensemble_step(self._h, int(nsteps), _stream_handle(stream)))
+
+    def diagnostics(self, half_kick=0.0, stream=None):
+        arr = (GsphDiag * self.nsims)()
+        self._check(self.lib.gsph_ensemble_diagnostics(self._h, float(half_kick), arr, _stream_handle(stream)))
+        return [d.as_dict() for d in arr]
+
+    def launch_count(self):
+        c = ctypes.c_int64()
+        self._check(self.lib.gsph_ensemble_launch_count(self._h, ctypes.byref(c)))
+        return c.value
+
+    def split(self, state):
+        """Per-simulation views of a packed state."""
+        return [{k: v[self.offsets[s]:self.offsets[s + 1]] for k, v in state.items()} for s in range(self.nsims)]
+
+
+def pack_states(states):
+    """Concatenate per-simulation states into the packed ensemble layout."""
+    keys = [k for k in states[0]]
+    return {k: np.concatenate([s[k] for s in states], axis=0) for k in keys}
+
+
 def computeDerivatives(pb, stream=None):  # noqa: N802 (reference name)
     pb.compute_derivatives(stream)
 

@@ -277,6 +277,37 @@ int gsph_device_view_get(gsph_ctx* ctx, gsph_device_view* v);
 int gsph_launch_count(gsph_ctx* ctx, int64_t* count);
 
 /* ---------------------------------------------------------------------------------------------
+ * batched ensemble: S independent simulations of uneven particle counts with one parameter set,
+ * advanced by one persistent launch per substep. No counterpart in the reference, which runs one
+ * simulation per process (src/main.cu:228-273); each simulation follows computeDerivatives /
+ * integrate exactly as a single context does (gravity, density and SPH terms only within its own
+ * particles). Host arrays hold the simulations back to back: simulation k is rows
+ * [offsets[k], offsets[k+1]) with offsets from gsph_ensemble_offsets. Fixed time step, single
+ * precision; BALSARA_SWITCH and VARIABLE_TIMESTEP give GSPH_E_UNSUPPORTED.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct gsph_ensemble gsph_ensemble;
+int gsph_ensemble_create(const gsph_params* p, const gsph_options* opt, int32_t nsims, const int64_t* counts,
+                         gsph_ensemble** out);
+int gsph_ensemble_destroy(gsph_ensemble* e);
+/* nsims + 1 row offsets of the packed host layout */
+int gsph_ensemble_offsets(const gsph_ensemble* e, int64_t* offsets);
+int gsph_ensemble_upload(gsph_ensemble* e, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
+/* synchronises `stream` */
+int gsph_ensemble_download(gsph_ensemble* e, uint32_t attr_mask, gsph_host_particles* dst, void* stream);
+/* FP64 positions (3N) of the master copy, as gsph_upload_pos64 / gsph_download_pos64 */
+int gsph_ensemble_upload_pos64(gsph_ensemble* e, const double* pos, void* stream);
+int gsph_ensemble_download_pos64(gsph_ensemble* e, double* pos, void* stream);
+int gsph_ensemble_compute_derivatives(gsph_ensemble* e, void* stream);
+int gsph_ensemble_integrate(gsph_ensemble* e, int32_t not_first_step, void* stream);
+/* nsteps x {computeDerivatives; integrate(true)} for every simulation, one captured graph per step */
+int gsph_ensemble_step(gsph_ensemble* e, int32_t nsteps, void* stream);
+/* FP64 diagnostics of every simulation into out[nsims] (as gsph_diagnostics); synchronises `stream` */
+int gsph_ensemble_diagnostics(gsph_ensemble* e, double half_kick, gsph_diag* out, void* stream);
+int gsph_ensemble_launch_count(const gsph_ensemble* e, int64_t* count);
+/* text of the last failure on `e` (or of the last failed gsph_ensemble_create when e is NULL) */
+const char* gsph_ensemble_last_error(const gsph_ensemble* e);
+
+/* ---------------------------------------------------------------------------------------------
  * measurement hooks (no reference counterpart: the reference has no kernel timers; its console
  * frontend prints wall-clock fps only, src/frontends/consoleFrontend.cpp:43-57)
  * ------------------------------------------------------------------------------------------- */
