@@ -51,7 +51,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["impact", "fluid", "plummer"], default="impact")
+    ap.add_argument("--workload", choices=["impact", "fluid", "plummer", "ensemble"], default="impact")
+    ap.add_argument("--nsims", type=int, default=512, help="simulations of the ensemble workload")
+    ap.add_argument("--no-sequential", action="store_true",
+                    help="ensemble: skip timing the simulations one by one in their own contexts")
     ap.add_argument("--accum", choices=["plain", "compensated"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU work for the CPU baseline")
@@ -233,6 +236,25 @@ def cpu_reference_sample(variant, st, budget_s, rows_hint=None):
 def run_reference_arm(args, rank, world):
     if world > 1 and rank != 0:
         return
+    if args.workload == "ensemble":  # the reference's host path on the largest simulation, scaled by sum N_k^2
+        params, sizes, states, desc = ensemble_workload(args.nsims)
+        big = int(np.argmax(sizes))
+        scale = float((sizes.astype(np.float64) ** 2).sum()) / float(sizes[big]) ** 2
+        rate, sdesc, cores, kind, _ = cpu_reference_sample("fluid", states[big], 20.0)
+        value = rate / scale
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "nsims": int(len(sizes)), "n_total": int(sizes.sum())},
+            "pair_interactions_per_s": float((sizes.astype(np.float64) ** 2).sum()) * value,
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
+                             "sample": "largest simulation N=%d: %s; scaled by sum N_k^2 / N^2 = %.1f"
+                                       % (int(sizes[big]), sdesc, scale)},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
     params, st, desc, variant = workload(args.workload, args.n)
     n = st["mass"].shape[0]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -336,6 +358,164 @@ def flops_pairs(params, n):
 
 
 # ---- our arm ----------------------------------------------------------------------------------------
+def ensemble_workload(nsims, seed=20261206):
+    """Batched ensemble: nsims self-gravitating SPH spheres with the fluid physics (h=0.15, eps=0.02,
+    c_s=1, rho0=0.239, dt=1e-3), each N a seeded log-uniform integer in [1024, 32768], radius 1,
+    rigid rotation omega ~ U[0, 0.5] about z."""
+    from grasph2_b200 import ics
+    from grasph2_b200.params import config0_params
+    sizes = ics.ensemble_sizes(nsims, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    states = [ics.uniform_sphere(int(n), radius=1.0, rho0=0.239, omega=(0.0, 0.0, rng.uniform(0.0, 0.5)),
+                                 seed=seed + 2 + k) for k, n in enumerate(sizes)]
+    desc = ("batched ensemble of %d self-gravitating SPH spheres, N_k log-uniform in [1024, 32768] (total %d), "
+            "radius 1, omega ~ U[0,0.5], h=0.15, eps=0.02, c_s=1, rho0=0.239, dt=1e-3" % (nsims, int(sizes.sum())))
+    return config0_params(), sizes, states, desc
+
+
+def run_ensemble(args, rank, world, local):
+    """One step = every simulation of the ensemble advanced once (one persistent launch)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    from grasph2_b200.params import make_options
+    from grasph2_b200.sim import DeviceParticleBuffer, Ensemble, measure_fp32_peak, pack_states
+    from grasph2_b200.state import new_state
+
+    params, sizes, states, desc = ensemble_workload(args.nsims)
+    packed = pack_states(states)
+    n_total = int(sizes.sum())
+    pairs = float((sizes.astype(np.float64) ** 2).sum())
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    peak_tflops = None if args.no_peak else measure_fp32_peak(0.5)
+    ens = Ensemble(params, sizes, make_options(accum=args.accum))
+    ens.upload(packed, stream=stream)
+    for _ in range(args.warmup):
+        flush.zero_()
+        ens.step(1, stream)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = ens.launch_count()
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(args.steps):
+        flush.zero_()
+        ev0[k].record(stream)
+        ens.step(1, stream)
+        ev1[k].record(stream)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    gpu_launches = ens.launch_count() - launches0
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+
+    # e2e through the public API with pinned host buffers: upload, one step, download
+    up_names = ["pos", "mass", "vel", "density"]
+    down_names = ["pos", "vel", "acc", "density"]
+    pinned_in = {k: torch.from_numpy(np.ascontiguousarray(packed[k], dtype=np.float32)).pin_memory().numpy()
+                 for k in up_names}
+    host_out = new_state(n_total, np.float32)
+    pinned_out = {k: torch.empty(host_out[k].shape, dtype=torch.float32).pin_memory().numpy() for k in down_names}
+    h2d = sum(a.nbytes for a in pinned_in.values())
+    d2h = sum(a.nbytes for a in pinned_out.values())
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 10))
+    e2e_ms = 0.0
+    with Ensemble(params, sizes, make_options(accum=args.accum)) as e2:
+        for k in range(e2e_steps + 2 if e2e_steps else 0):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e2.upload(pinned_in, stream=stream)
+            e2.step(1, stream)
+            e2.download(down_names, stream=stream, out=pinned_out)
+            b.record(stream)
+            b.synchronize()
+            if k >= 2:
+                e2e_ms += a.elapsed_time(b)
+
+    # the same simulations one after another, each in its own single-simulation context (plain path):
+    # every 8th simulation in size order, each standing for 8
+    seq_ms = None
+    if not args.no_sequential and rank == 0:
+        order = np.argsort(sizes)
+        stride = max(1, len(order) // 64)
+        pick = order[stride // 2::stride]
+        tot = 0.0
+        for k in pick:
+            with DeviceParticleBuffer(params, int(sizes[k]), make_options(accum=args.accum)) as pb:
+                pb.upload(states[k], stream=stream)
+                pb.step(2, stream)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                pb.step(5, stream)
+                b.record(stream)
+                b.synchronize()
+                tot += a.elapsed_time(b) / 5
+        seq_ms = tot * len(order) / len(pick)
+
+    if rank != 0:
+        ens.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    value = world / (ms_per_step * 1e-3)
+    nb = sum(neighbour_pairs(s["pos"], params.H, dev) for s in states[::8]) * 8
+    flops = FLOP_GRAV_PAIR * pairs + FLOP_DENS_PAIR * pairs + (FLOP_DENS_NB + FLOP_ACC_NB) * nb
+    achieved = flops / (ms_per_step * 1e-3) / 1e12
+    cpu = None
+    if not args.no_cpu_baseline:
+        big = int(np.argmax(sizes))
+        rate, sdesc, cores, kind, _ = cpu_reference_sample("fluid", states[big], args.cpu_budget)
+        scale = pairs / float(sizes[big]) ** 2
+        cpu = {"value": rate / scale, "unit": "steps/s", "cores": cores, "kind": kind,
+               "sample": "the largest simulation (N=%d): %s; the ensemble step scaled by sum N_k^2 / N^2 = %.1f"
+                         % (int(sizes[big]), sdesc, scale)}
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded initial conditions)",
+        "config": {"workload": desc, "nsims": int(len(sizes)), "n_total": n_total, "form": args.accum,
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "step": "every simulation: computeDerivatives + integrate, one persistent launch in a CUDA graph",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "simulation_steps_per_s": value * len(sizes),
+        "pair_interactions_per_s": pairs * value,
+        "sequential_plain_ms_per_step": seq_ms,
+        "speedup_vs_sequential": (seq_ms / ms_per_step) if seq_ms else None,
+        "roofline": {"bound": "fp32", "kernel": "k_ensemble", "achieved": achieved, "peak": peak_tflops,
+                     "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if peak_tflops else None, "traffic": None,
+                     "flops_per_launch": flops, "neighbour_pairs": nb,
+                     "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "e2e": ({"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                 "d2h_bytes_per_step": d2h} if e2e_steps else None),
+        "gpu_launches": gpu_launches,
+    }
+    print(json.dumps(line))
+    ens.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -345,6 +525,9 @@ def main():
         run_reference_arm(args, rank, world)
         return
 
+    if args.workload == "ensemble":
+        run_ensemble(args, rank, world, local)
+        return
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)

@@ -29,7 +29,10 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "integrate.cuh"
+#include "spatial.cuh"
 #include "sph.cuh"
 
 void set_global_error(const std::string& msg);                 // capi.cu
@@ -202,6 +205,7 @@ __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p
     }
     const float2 E2 = make_float2(p.eps2, p.eps2);
     const uint32_t span = __float_as_uint(p.H2);
+    const float H2 = p.H2;
     const float inv_h = p.inv_h;
 
     const bool ok = pipe.run(sm.x, static_cast<int64_t>(sm.x) + sm.y, [&](const float4* J, int nj, int64_t jb) {
@@ -216,10 +220,12 @@ __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p
             const float4 q = J[j];
             const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y), qz = make_float2(q.z, q.z),
                          qm = make_float2(q.w, q.w);
+            float2 R2[P];
 #pragma unroll
             for (int k = 0; k < P; ++k) {
                 const float2 dx = sub2(qx, X[k]), dy = sub2(qy, Y[k]), dz = sub2(qz, Z[k]);
                 const float2 r2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+                R2[k] = r2;
                 if (GRAV != 0) {
                     const float2 r2e = add2(r2, E2);
                     float2 inv = make_float2(rsqrtf(r2e.x), rsqrtf(r2e.y));
@@ -231,20 +237,31 @@ __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p
                         AX[k] = fma2(dx, s, AX[k]); AY[k] = fma2(dy, s, AY[k]); AZ[k] = fma2(dz, s, AZ[k]);
                     }
                 }
-                if (SPH) {
-                    // calcDensity's window 0 < r^2 <= H^2 (computeDerivatives.h:72), also the neighbour test
+            }
+            if (SPH) {
+                // one warp vote per j: particles of a group are close along the curve, so for most j no
+                // lane has a neighbour and the per-particle window tests are skipped
+                bool near = false;
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const float rr = h ? r2.y : r2.x;
-                        if (in_open_closed(rr, 0u, span)) {
-                            const int kk = 2 * k + h;
-                            const float r = rr * rsqrtf(rr);
-                            const float w = q.w * w_poly(r * inv_h);
-                            if (COMP) tr[kk] += w;
-                            else rho[kk] += w;
-                            if (valid[kk]) {
-                                if (cnt[kk] < kEnsCap) v.nb[static_cast<int64_t>(cnt[kk]) * v.n + idx[kk]] = static_cast<int>(jb + j);
-                                cnt[kk] = min(cnt[kk] + 1, kEnsCap + 1);
+                for (int k = 0; k < P; ++k) near |= (R2[k].x <= H2) | (R2[k].y <= H2);
+                if (__any_sync(0xffffffffu, near)) {
+#pragma unroll
+                    for (int k = 0; k < P; ++k) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            // calcDensity's window 0 < r^2 <= H^2 (computeDerivatives.h:72), also the neighbour test
+                            const float rr = h ? R2[k].y : R2[k].x;
+                            if (in_open_closed(rr, 0u, span)) {
+                                const int kk = 2 * k + h;
+                                const float r = rr * rsqrtf(rr);
+                                const float w = q.w * w_poly(r * inv_h);
+                                if (COMP) tr[kk] += w;
+                                else rho[kk] += w;
+                                if (valid[kk]) {
+                                    if (cnt[kk] < kEnsCap)
+                                        v.nb[static_cast<int64_t>(cnt[kk]) * v.n + idx[kk]] = static_cast<int>(jb + j);
+                                    cnt[kk] = min(cnt[kk] + 1, kEnsCap + 1);
+                                }
                             }
                         }
                     }
@@ -474,6 +491,71 @@ __global__ void k_ens_diag_reduce(EnsView v, const double* part, double* out) {
     out[static_cast<int64_t>(blockIdx.x) * kEnsDiagF + k] = s;
 }
 
+// ---- per-simulation curve order -------------------------------------------------------------------
+// bounds of each simulation's positions (one block per simulation): bbox[s] = lo xyz, hi xyz
+__global__ void k_ens_bbox(DevArrays a, EnsView v, float* bbox) {
+    __shared__ float red[6][32];
+    const int4 sm = v.sims[blockIdx.x];
+    float r[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x y z, -max x y z
+    for (int64_t i = static_cast<int64_t>(sm.x) + threadIdx.x; i < static_cast<int64_t>(sm.x) + sm.y; i += blockDim.x) {
+        const float4 p = a.posm[i];
+        const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (isfinite(c[d])) {
+                r[d] = fminf(r[d], c[d]);
+                r[3 + d] = fminf(r[3 + d], -c[d]);
+            }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r[d] = fminf(r[d], __shfl_xor_sync(0xffffffffu, r[d], o));
+        if (lane == 0) red[d][warp] = r[d];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float m = INFINITY;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fminf(m, red[threadIdx.x][w]);
+        bbox[blockIdx.x * 8 + threadIdx.x] = threadIdx.x < 3 ? m : -m;
+    }
+}
+
+// sort key of every slot: simulation index above the 30-bit Hilbert index of the position inside
+// that simulation's bounds; padding sorts last
+__global__ void k_ens_keys(DevArrays a, EnsView v, const float* bbox, unsigned long long* keys, int* vals) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n_pad) return;
+    vals[i] = static_cast<int>(i);
+    if (i >= a.n) {
+        keys[i] = ~0ull;
+        return;
+    }
+    int lo = 0, hi = v.nsims;  // sims[lo].x <= i < sims[hi].x (simulations are packed in index order)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (v.sims[mid].x <= i) lo = mid;
+        else hi = mid;
+    }
+    const float4 p = a.posm[i];
+    const float c[3] = {p.x, p.y, p.z};
+    unsigned q[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float l = bbox[lo * 8 + d], span = bbox[lo * 8 + 3 + d] - l;
+        float t = (span > 0.0f && isfinite(c[d])) ? (c[d] - l) / span : 0.0f;
+        t = fminf(fmaxf(t, 0.0f), 1.0f);
+        q[d] = static_cast<unsigned>(t * 1023.0f);
+    }
+    keys[i] = (static_cast<unsigned long long>(lo) << 32) | hilbert3(q[0], q[1], q[2]);
+}
+
+__global__ void k_ens_iota(int* v, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = static_cast<int>(i);
+}
+
 size_t ens_smem() { return pipe_smem_bytes(1, kEnsTile); }
 
 template <int GRAV, bool SPH, int PASS, bool SOLIDS, bool COMP>
@@ -539,6 +621,17 @@ struct gsph_ensemble {
     double* diag_out = nullptr;     // [S][kEnsDiagF]
     float* staging = nullptr;       // 9 n floats
     double* staging64 = nullptr;    // 3 n doubles
+    // per-simulation curve order: device slot i holds the caller's row ext[i]
+    int* ext = nullptr;
+    int* order = nullptr;
+    int* order_out = nullptr;
+    unsigned long long* keys = nullptr;  // [2 n_pad]
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    float4* tmp4 = nullptr;
+    double* tmp8 = nullptr;
+    float* bbox = nullptr;               // [S][8]
+    int steps_since_sort = 0;
     std::vector<void*> allocations;
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -631,6 +724,28 @@ int ens_status(gsph_ensemble* e, cudaStream_t s) {
     return GSPH_OK;
 }
 
+// sort every simulation's particles along its own Hilbert curve (positions as they are now)
+int ens_reorder(gsph_ensemble* e, cudaStream_t s) {
+    const int st[1] = {ST_DENS};
+    const EnsView v = view_of(e, st, 1);
+    const int64_t np = e->a.n_pad;
+    k_ens_bbox<<<e->nsims, 256, 0, s>>>(e->a, v, e->bbox);
+    k_ens_keys<<<static_cast<unsigned>((np + 255) / 256), 256, 0, s>>>(e->a, v, e->bbox, e->keys, e->order);
+    ENS_CK(e, cudaGetLastError(), "sort keys");
+    e->launches += 2;
+    int end_bit = 33;
+    while ((int64_t(1) << (end_bit - 32)) < e->nsims) ++end_bit;
+    size_t tb = e->sort_bytes;
+    ENS_CK(e, cub::DeviceRadixSort::SortPairs(e->sort_tmp, tb, e->keys, e->keys + np, e->order, e->order_out,
+                                              static_cast<int>(np), 0, end_bit, s), "radix sort");
+    e->launches += 4;
+    int launches = 0;
+    ENS_CK(e, permute_particles(e->a, e->order_out, e->tmp4, e->tmp8, e->ext, s, launches), "permute");
+    e->launches += launches;
+    e->steps_since_sort = 0;
+    return GSPH_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -715,9 +830,24 @@ int gsph_ensemble_create(const gsph_params* p, const gsph_options* opt, int32_t 
     e->diag_out = static_cast<double*>(ens_alloc(e, static_cast<size_t>(nsims) * kEnsDiagF * sizeof(double), ae));
     e->staging = static_cast<float*>(ens_alloc(e, 9 * n * sizeof(float), ae));
     e->staging64 = static_cast<double*>(ens_alloc(e, 3 * n * sizeof(double), ae));
+    e->ext = static_cast<int*>(ens_alloc(e, n_pad * sizeof(int), ae));
+    e->order = static_cast<int*>(ens_alloc(e, n_pad * sizeof(int), ae));
+    e->order_out = static_cast<int*>(ens_alloc(e, n_pad * sizeof(int), ae));
+    e->keys = static_cast<unsigned long long*>(ens_alloc(e, 2 * n_pad * sizeof(unsigned long long), ae));
+    cub::DeviceRadixSort::SortPairs(nullptr, e->sort_bytes, static_cast<const unsigned long long*>(nullptr),
+                                    static_cast<unsigned long long*>(nullptr), static_cast<const int*>(nullptr),
+                                    static_cast<int*>(nullptr), static_cast<int>(n_pad));
+    e->sort_tmp = ens_alloc(e, e->sort_bytes, ae);
+    e->tmp4 = static_cast<float4*>(ens_alloc(e, n_pad * sizeof(float4), ae));
+    e->tmp8 = static_cast<double*>(ens_alloc(e, n_pad * sizeof(double), ae));
+    e->bbox = static_cast<float*>(ens_alloc(e, static_cast<size_t>(nsims) * 8 * sizeof(float), ae));
     if (ae == cudaSuccess) ae = cudaMemcpy(e->groups, groups.data(), groups.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (ae == cudaSuccess) ae = cudaMemcpy(e->sims, sims.data(), sims.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (ae == cudaSuccess) ae = launch_init_padding(a, 0);
+    if (ae == cudaSuccess) {
+        k_ens_iota<<<static_cast<unsigned>((n_pad + 255) / 256), 256>>>(e->ext, n_pad);
+        ae = cudaGetLastError();
+    }
     if (ae == cudaSuccess) ae = cudaDeviceSynchronize();
     if (ae != cudaSuccess) {
         const std::string msg = std::string("ensemble allocation failed: ") + cudaGetErrorString(ae);
@@ -757,9 +887,10 @@ int gsph_ensemble_upload(gsph_ensemble* e, uint32_t mask, const gsph_host_partic
         if (!(mask >> k & 1u)) continue;
         ENS_CK(e, cudaMemcpyAsync(e->staging, ptrs[k], comps[k] * e->a.n * sizeof(float), cudaMemcpyHostToDevice, s),
                "upload copy");
-        ENS_CK(e, launch_pack(e->a, k, e->staging, nullptr, s), "upload pack");
+        ENS_CK(e, launch_pack(e->a, k, e->staging, e->ext, s), "upload pack");
         e->launches += 1;
     }
+    if (mask & GSPH_POS) return ens_reorder(e, s);
     return GSPH_OK;
 }
 
@@ -775,7 +906,7 @@ int gsph_ensemble_download(gsph_ensemble* e, uint32_t mask, gsph_host_particles*
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     for (int k = 0; k < 11; ++k) {
         if (!(mask >> k & 1u)) continue;
-        ENS_CK(e, launch_unpack(e->a, k, e->staging, nullptr, s), "download unpack");
+        ENS_CK(e, launch_unpack(e->a, k, e->staging, e->ext, s), "download unpack");
         e->launches += 1;
         ENS_CK(e, cudaMemcpyAsync(ptrs[k], e->staging, comps[k] * e->a.n * sizeof(float), cudaMemcpyDeviceToHost, s),
                "download copy");
@@ -788,7 +919,7 @@ int gsph_ensemble_upload_pos64(gsph_ensemble* e, const double* pos, void* stream
     if (!pos) return efail(e, GSPH_E_INVALID, "pos is NULL");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     ENS_CK(e, cudaMemcpyAsync(e->staging64, pos, 3 * e->a.n * sizeof(double), cudaMemcpyHostToDevice, s), "upload copy");
-    ENS_CK(e, launch_pack_pos64(e->a, e->staging64, nullptr, s), "upload pack");
+    ENS_CK(e, launch_pack_pos64(e->a, e->staging64, e->ext, s), "upload pack");
     e->launches += 1;
     return GSPH_OK;
 }
@@ -797,7 +928,7 @@ int gsph_ensemble_download_pos64(gsph_ensemble* e, double* pos, void* stream) {
     if (!e) return GSPH_E_INVALID;
     if (!pos) return efail(e, GSPH_E_INVALID, "pos is NULL");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    ENS_CK(e, launch_unpack_pos64(e->a, e->staging64, nullptr, s), "download unpack");
+    ENS_CK(e, launch_unpack_pos64(e->a, e->staging64, e->ext, s), "download unpack");
     e->launches += 1;
     ENS_CK(e, cudaMemcpyAsync(pos, e->staging64, 3 * e->a.n * sizeof(double), cudaMemcpyDeviceToHost, s), "download copy");
     return ens_status(e, s);
@@ -849,8 +980,13 @@ int gsph_ensemble_step(gsph_ensemble* e, int32_t nsteps, void* stream) {
         e->graph_exec = ex;
     }
     for (int32_t k = 0; k < nsteps; ++k) {
+        if (e->opt.resort_interval > 0 && e->steps_since_sort >= e->opt.resort_interval) {
+            const int rc = ens_reorder(e, s);  // permutes in place: the graph's pointers stay valid
+            if (rc != GSPH_OK) return rc;
+        }
         ENS_CK(e, cudaGraphLaunch(e->graph_exec, s), "graph launch");
         e->launches += 1;
+        e->steps_since_sort += 1;
     }
     return GSPH_OK;
 }

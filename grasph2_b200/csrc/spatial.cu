@@ -129,44 +129,6 @@ __global__ void k_bbox(DevArrays a, int* bb) {
     }
 }
 
-__device__ __forceinline__ unsigned spread10(unsigned v) {  // 10 bits -> every third bit
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-
-// 30-bit Hilbert index of a point on a 1024^3 grid: J. Skilling, "Programming the Hilbert curve",
-// AIP Conf. Proc. 707 (2004): the axes are transformed in place into the transposed index
-// (inverse undo + Gray encoding), whose bits interleaved from the top give the index. Consecutive
-// indices are neighbouring cells, so runs of particles in this order are spatially compact.
-__device__ __forceinline__ unsigned hilbert3(unsigned x0, unsigned x1, unsigned x2) {
-    unsigned X[3] = {x0, x1, x2};
-    constexpr unsigned M = 1u << 9;
-    for (unsigned Q = M; Q > 1; Q >>= 1) {
-        const unsigned P = Q - 1;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            if (X[i] & Q) {
-                X[0] ^= P;
-            } else {
-                const unsigned t = (X[0] ^ X[i]) & P;
-                X[0] ^= t;
-                X[i] ^= t;
-            }
-        }
-    }
-    X[1] ^= X[0];
-    X[2] ^= X[1];
-    unsigned t = 0;
-    for (unsigned Q = M; Q > 1; Q >>= 1)
-        if (X[2] & Q) t ^= Q - 1;
-    X[0] ^= t; X[1] ^= t; X[2] ^= t;
-    return (spread10(X[0]) << 2) | (spread10(X[1]) << 1) | spread10(X[2]);
-}
-
 __global__ void k_curve_keys(DevArrays a, const int* bb, unsigned* keys, int* vals) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n_pad) return;
@@ -251,21 +213,26 @@ cudaError_t reorder_particles(const DevArrays& a, const SpatialArrays& s, cudaSt
                                         static_cast<int>(np), 0, 32, st);
     if (e != cudaSuccess) return e;
     launches += 4;  // onesweep radix sort passes (approximate count for the launch counter)
-    const int* ord = s.order_out;
-    float4* t4 = s.tmp4;
+    return permute_particles(a, s.order_out, s.tmp4, s.tmp8, s.ext_of_int, st, launches);
+}
+
+cudaError_t permute_particles(const DevArrays& a, const int* ord, float4* t4, double* t8, int* ext_of_int,
+                              cudaStream_t st, int& launches) {
+    const int64_t np = a.n_pad;
+    cudaError_t e = cudaSuccess;
     float4* f4s[] = {a.posm, a.velrho, a.acc, a.xvel, a.sA, a.sB, a.dA, a.dB, a.jA, a.jB};
     for (float4* arr : f4s) {
         e = permute(arr, t4, ord, np, st, launches);
         if (e != cudaSuccess) return e;
     }
     for (int d = 0; d < 3; ++d) {
-        e = permute(a.pos64 + d * np, s.tmp8, ord, np, st, launches);
+        e = permute(a.pos64 + d * np, t8, ord, np, st, launches);
         if (e != cudaSuccess) return e;
     }
-    float* tf = reinterpret_cast<float*>(s.tmp4);
+    float* tf = reinterpret_cast<float*>(t4);
     e = permute(a.rhodot, tf, ord, np, st, launches);
     if (e == cudaSuccess) e = permute(a.balsara, tf, ord, np, st, launches);
-    if (e == cudaSuccess) e = permute(s.ext_of_int, reinterpret_cast<int*>(s.tmp4), ord, np, st, launches);
+    if (e == cudaSuccess) e = permute(ext_of_int, reinterpret_cast<int*>(t4), ord, np, st, launches);
     return e;
 }
 
