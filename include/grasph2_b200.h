@@ -173,7 +173,7 @@ typedef struct gsph_options {
     int32_t precision;       /* GSPH_PRECISION_SINGLE (default) or GSPH_PRECISION_DOUBLE: the reference's
                                 SINGLE_PRECISION / DOUBLE_PRECISION switch (settings/precisionSettings.h:16-17).
                                 Double runs every pass in FP64 with plain all-pairs tiles (no culling,
-                                accum ignored); host transfers stay float, plus the FP64 position calls */
+                                accum ignored); gsph_upload_f64 / gsph_download_f64 pass values unrounded */
     int32_t reserved[6];
 } gsph_options;
 
