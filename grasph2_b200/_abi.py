@@ -169,6 +169,8 @@ _SIGNATURES = {
                                                  ctypes.c_void_p]),
     "gsph_ensemble_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gsph_tc_gemm_check": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_void_p]),
 }

@@ -276,6 +276,12 @@ int gsph_device_view_get(gsph_ctx* ctx, gsph_device_view* v);
 /* Number of kernels this context launched since creation (host-side count). */
 int gsph_launch_count(gsph_ctx* ctx, int64_t* count);
 
+/* Tensor-core tile GEMM check (no counterpart in the reference): D[128][N] = A[128][K] * B[N][K]^T
+ * with bf16 row-major device inputs and FP32 output, each operand staged K-major (0) or MN-major (1)
+ * in shared memory as the surrogate's MLP kernels stage theirs. N, K multiples of 16 in [16, 128].
+ * Synchronises the device. */
+int gsph_tc_gemm_check(const void* A, const void* B, float* D, int32_t N, int32_t K, int32_t a_mn, int32_t b_mn);
+
 /* ---------------------------------------------------------------------------------------------
  * batched ensemble: S independent simulations of uneven particle counts with one parameter set,
  * advanced by one persistent launch per substep. No counterpart in the reference, which runs one
