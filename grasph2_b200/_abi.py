@@ -171,6 +171,19 @@ _SIGNATURES = {
     "gsph_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_tc_gemm_check": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "gsph_mlp_param_count": (ctypes.c_int64, []),
+    "gsph_mlp_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_void_p)]),
+    "gsph_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "gsph_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "gsph_mlp_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_void_p]),
+    "gsph_mlp_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_int64, ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "gsph_mlp_adam": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_void_p]),
+    "gsph_mlp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_void_p]),
 }

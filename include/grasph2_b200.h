@@ -283,6 +283,33 @@ int gsph_launch_count(gsph_ctx* ctx, int64_t* count);
 int gsph_tc_gemm_check(const void* A, const void* B, float* D, int32_t N, int32_t K, int32_t a_mn, int32_t b_mn);
 
 /* ---------------------------------------------------------------------------------------------
+ * the learned surrogate's per-particle MLP (no counterpart in the reference): 32 inputs, three
+ * hidden layers of 128 with SiLU, 13 outputs; BF16 weights and activations on the tensor cores with
+ * FP32 accumulation, FP32 master parameters and Adam state on the device. Parameters are one flat
+ * FP32 vector: W1[128][32] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] W4[13][128] b4[13].
+ * ------------------------------------------------------------------------------------------- */
+#define GSPH_MLP_IN  32
+#define GSPH_MLP_OUT 13
+typedef struct gsph_mlp gsph_mlp;
+int64_t gsph_mlp_param_count(void);
+/* params: host FP32 vector of gsph_mlp_param_count() values, or NULL for zeros */
+int gsph_mlp_create(const float* params, gsph_mlp** out);
+int gsph_mlp_destroy(gsph_mlp* m);
+int gsph_mlp_get_params(gsph_mlp* m, float* params);
+/* replaces the parameters and clears the Adam state */
+int gsph_mlp_set_params(gsph_mlp* m, const float* params);
+/* y[n][13] = MLP(x[n][32]); device pointers, asynchronous on `stream` */
+int gsph_mlp_forward(gsph_mlp* m, const float* x, float* y, int64_t n, void* stream);
+/* gradient of L = (1/n) sum_p sum_o wout[o] (y_po - target_po)^2 over the n device rows into the
+ * model's gradient buffer (deterministic); grad (host, param_count) and loss (host) may be NULL, else
+ * they are filled and `stream` synchronised. wout: 13 device floats */
+int gsph_mlp_gradient(gsph_mlp* m, const float* x, const float* target, const float* wout, int64_t n, float* grad,
+                      double* loss, void* stream);
+/* one Adam step (Kingma & Ba 2015) with the last gradient */
+int gsph_mlp_adam(gsph_mlp* m, float lr, float beta1, float beta2, float eps, void* stream);
+const char* gsph_mlp_last_error(const gsph_mlp* m);
+
+/* ---------------------------------------------------------------------------------------------
  * batched ensemble: S independent simulations of uneven particle counts with one parameter set,
  * advanced by one persistent launch per substep. No counterpart in the reference, which runs one
  * simulation per process (src/main.cu:228-273); each simulation follows computeDerivatives /
