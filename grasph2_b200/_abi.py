@@ -141,6 +141,8 @@ _SIGNATURES = {
     "gsph_current_timestep": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_void_p]),
     "gsph_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
                                         ctypes.c_void_p]),
+    "gsph_diagnostics_fast": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
+                                             ctypes.c_void_p]),
     "gsph_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_reorder": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "gsph_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -171,6 +173,11 @@ _SIGNATURES = {
     "gsph_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_tc_gemm_check": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "gsph_surrogate_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p]),
+    "gsph_surrogate_apply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int32, ctypes.c_void_p]),
+    "gsph_snapshot": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     "gsph_mlp_param_count": (ctypes.c_int64, []),
     "gsph_mlp_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_void_p)]),
     "gsph_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),

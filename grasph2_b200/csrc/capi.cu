@@ -10,11 +10,14 @@
 #include <vector>
 
 #include "fp64.cuh"
+#include "surrogate.cuh"
 #include "integrate.cuh"
 #include "pairs.cuh"
 #include "spatial.cuh"
 
 using namespace gsph;
+
+constexpr int kSnapSlots = 4;
 
 struct gsph_ctx {
     gsph_params params;
@@ -36,6 +39,7 @@ struct gsph_ctx {
     float* staging = nullptr;     // 9 * n floats
     double* staging64 = nullptr;  // 9 * n doubles
     double* diag_out = nullptr;   // device, 12 doubles
+    std::vector<void*> snap[4];    // gsph_snapshot slots: saved copies of the state arrays (allocated on first save)
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -189,6 +193,11 @@ void release(gsph_ctx* c) {
     if (c->capture_stream) cudaStreamDestroy(c->capture_stream);
     for (void* p : c->allocations) cudaFree(p);
     c->allocations.clear();
+    for (auto& sl : c->snap) {
+        for (void* p : sl)
+            if (p) cudaFree(p);
+        sl.clear();
+    }
 }
 
 int check_status(gsph_ctx* c, cudaStream_t s) {
@@ -785,11 +794,13 @@ int gsph_current_timestep(gsph_ctx* c, double* dt, void* stream) {
     return GSPH_OK;
 }
 
-int gsph_diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream) {
+namespace {
+int diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream, bool fast) {
     if (!c) return GSPH_E_INVALID;
     if (!out) return fail(c, GSPH_E_INVALID, "out is NULL");
     cudaStream_t s = as_stream(stream);
     if (c->fp64) GSPH_CK(c, launch64_diagnostics(c->a64, c->dp64, half_kick, c->diag64, c->diag_out, s), "diagnostics");
+    else if (fast) GSPH_CK(c, launch_diagnostics_fast(c->a, c->dp, half_kick, c->diag_out, s), "diagnostics");
     else GSPH_CK(c, launch_diagnostics(c->a, c->dp, half_kick, c->diag_out, s), "diagnostics");
     c->launches += 2;
     double h[12];
@@ -807,10 +818,82 @@ int gsph_diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream
     out->mass = h[10];
     return GSPH_OK;
 }
+}  // namespace
+
+int gsph_diagnostics(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream) {
+    return diagnostics(c, half_kick, out, stream, false);
+}
+
+int gsph_diagnostics_fast(gsph_ctx* c, double half_kick, gsph_diag* out, void* stream) {
+    return diagnostics(c, half_kick, out, stream, true);
+}
 
 int gsph_reorder(gsph_ctx* c, void* stream) {
     if (!c) return GSPH_E_INVALID;
     return reorder(c, as_stream(stream));
+}
+
+int gsph_surrogate_features(gsph_ctx* c, const float* mu, const float* sigma, float* feat, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (!feat || (!mu) != (!sigma)) return fail(c, GSPH_E_INVALID, "feat is NULL, or only one of mu / sigma given");
+    if (c->fp64 || !c->L.cull || !(c->params.flags & GSPH_SPH))
+        return fail(c, GSPH_E_UNSUPPORTED, "features need an SPH context in single precision with culling");
+    cudaStream_t s = as_stream(stream);
+    GSPH_CK(c, launch_chunk_bounds(c->a, c->sp, s), "chunk bounds");
+    GSPH_CK(c, launch_chunk_lists(c->a, c->sp, c->dp.H, s), "chunk lists");
+    GSPH_CK(c, launch_features(c->a, c->dp, c->sp, mu, sigma, feat, s), "features");
+    c->launches += 3;
+    return GSPH_OK;
+}
+
+int gsph_surrogate_apply(gsph_ctx* c, const float* delta, const float* out_mu, const float* out_sigma, int32_t K,
+                         void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (K < 1 || (delta && (!out_mu || !out_sigma))) return fail(c, GSPH_E_INVALID, "K < 1, or delta without scales");
+    if (c->fp64 || (c->params.flags & GSPH_VARIABLE_TIMESTEP))
+        return fail(c, GSPH_E_UNSUPPORTED, "proposals need the fixed step in single precision");
+    GSPH_CK(c, launch_apply(c->a, c->dp, ext_map(c), delta, out_mu, out_sigma, K, as_stream(stream)), "apply");
+    c->launches += 1;
+    return GSPH_OK;
+}
+
+int gsph_snapshot(gsph_ctx* c, int32_t slot, int32_t restore, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (c->fp64) return fail(c, GSPH_E_UNSUPPORTED, "snapshots are single-precision only");
+    if (slot < 0 || slot >= kSnapSlots) return fail(c, GSPH_E_INVALID, "snapshot slot out of range");
+    std::vector<void*>& snap = c->snap[slot];
+    const int64_t np = c->a.n_pad;
+    struct Arr { void* p; size_t bytes; };
+    const Arr arrs[] = {
+        {c->a.posm, np * sizeof(float4)}, {c->a.velrho, np * sizeof(float4)}, {c->a.acc, np * sizeof(float4)},
+        {c->a.xvel, np * sizeof(float4)}, {c->a.sA, np * sizeof(float4)}, {c->a.sB, np * sizeof(float4)},
+        {c->a.dA, np * sizeof(float4)}, {c->a.dB, np * sizeof(float4)}, {c->a.jA, np * sizeof(float4)},
+        {c->a.jB, np * sizeof(float4)}, {c->a.pos64, 3 * np * sizeof(double)}, {c->a.rhodot, np * sizeof(float)},
+        {c->a.balsara, np * sizeof(float)}, {c->a.dt_state, 4 * sizeof(float)},
+        {c->L.cull ? c->sp.ext_of_int : nullptr, np * sizeof(int)}};
+    const int na = static_cast<int>(sizeof(arrs) / sizeof(arrs[0]));
+    cudaStream_t s = as_stream(stream);
+    if (!restore && snap.empty()) {
+        for (int k = 0; k < na; ++k) {
+            void* p = nullptr;
+            if (arrs[k].p) {
+                const cudaError_t e = cudaMalloc(&p, arrs[k].bytes);
+                if (e != cudaSuccess) {
+                    for (void* q : snap) cudaFree(q);
+                    snap.clear();
+                    return fail(c, GSPH_E_NOMEM, "snapshot allocation failed");
+                }
+            }
+            snap.push_back(p);
+        }
+    }
+    if (restore && snap.empty()) return fail(c, GSPH_E_STATE, "no snapshot saved");
+    for (int k = 0; k < na; ++k) {
+        if (!arrs[k].p) continue;
+        GSPH_CK(c, cudaMemcpyAsync(restore ? arrs[k].p : snap[k], restore ? snap[k] : arrs[k].p, arrs[k].bytes,
+                                   cudaMemcpyDeviceToDevice, s), "snapshot copy");
+    }
+    return GSPH_OK;
 }
 
 int gsph_size(gsph_ctx* c, int64_t* n) {

@@ -10,6 +10,9 @@ int leapfrog_kernel_count(const DevParams& p);
 size_t diag_scratch_doubles(int64_t n);
 cudaError_t launch_diagnostics(const DevArrays& a, const DevParams& p, double half_kick, double* out_dev,
                                cudaStream_t s);
+// the same with the pair potential summed in FP32 (compensated across tiles, FP64 across particles)
+cudaError_t launch_diagnostics_fast(const DevArrays& a, const DevParams& p, double half_kick, double* out_dev,
+                                    cudaStream_t s);
 // `ext` (nullable) maps each device slot to the caller's particle index
 cudaError_t launch_pack(const DevArrays& a, int attr, const float* src_dev, const int* ext, cudaStream_t s);
 cudaError_t launch_unpack(const DevArrays& a, int attr, float* dst_dev, const int* ext, cudaStream_t s);

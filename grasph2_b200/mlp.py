@@ -4,6 +4,7 @@ pointers); the library fails loudly when it is missing.
 """
 
 import ctypes
+import math
 
 import numpy as np
 
@@ -19,6 +20,22 @@ def _ptr(a):
     if hasattr(a, "data_ptr"):
         return ctypes.c_void_p(a.data_ptr())
     return ctypes.c_void_p(int(a))
+
+
+SHAPES = [(128, 32), (128,), (128, 128), (128,), (128, 128), (128,), (13, 128), (13,)]
+
+
+def init_params(seed=0):
+    """Kaiming-uniform weights (bound sqrt(6 / fan_in), suited to SiLU), zero biases, as the flat vector."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for shape in SHAPES:
+        if len(shape) == 2:
+            b = math.sqrt(6.0 / shape[1])
+            parts.append(rng.uniform(-b, b, size=shape).ravel())
+        else:
+            parts.append(np.zeros(shape))
+    return np.concatenate(parts).astype(np.float32)
 
 
 class MLP:

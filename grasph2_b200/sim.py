@@ -156,9 +156,11 @@ class DeviceParticleBuffer:
         self._check(self.lib.gsph_current_timestep(self._ctx, ctypes.byref(dt), _stream_handle(stream)))
         return dt.value
 
-    def diagnostics(self, half_kick=0.0, stream=None):
+    def diagnostics(self, half_kick=0.0, stream=None, fast=False):
+        """FP64 energies, momentum, angular momentum; fast=True sums the pair potential in FP32 (compensated)."""
         d = GsphDiag()
-        self._check(self.lib.gsph_diagnostics(self._ctx, float(half_kick), ctypes.byref(d), _stream_handle(stream)))
+        f = self.lib.gsph_diagnostics_fast if fast else self.lib.gsph_diagnostics
+        self._check(f(self._ctx, float(half_kick), ctypes.byref(d), _stream_handle(stream)))
         return d.as_dict()
 
     def launch_count(self):

@@ -255,6 +255,9 @@ typedef struct gsph_diag {
  * 0.5*dt right after gsph_compute_derivatives to synchronise the leapfrog's half-step velocity
  * v_{n-1/2} to v_n. Synchronises `stream`. */
 int gsph_diagnostics(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stream);
+/* The same with the pair potential summed in FP32 (two-sum across j-tiles, FP64 across particles;
+ * relative error of e_grav ~1e-7): one FP32 N^2 sweep instead of an FP64 one, for frequent checks. */
+int gsph_diagnostics_fast(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stream);
 
 /* Number of particles of the context. */
 int gsph_size(gsph_ctx* ctx, int64_t* n);
@@ -308,6 +311,20 @@ int gsph_mlp_gradient(gsph_mlp* m, const float* x, const float* target, const fl
 /* one Adam step (Kingma & Ba 2015) with the last gradient */
 int gsph_mlp_adam(gsph_mlp* m, float lr, float beta1, float beta2, float eps, void* stream);
 const char* gsph_mlp_last_error(const gsph_mlp* m);
+
+/* Surrogate support on a context (no counterpart in the reference).
+ * gsph_surrogate_features: 32 neighbour-moment features of the current state per particle into
+ *   feat[n][32] (device, caller's order), standardised as (f - mu) / sigma when mu and sigma (32 device
+ *   floats each) are given. Needs SPH in single precision with culling.
+ * gsph_surrogate_apply: advance the state by a K-substep proposal: the fixed-step leapfrog with the
+ *   derivatives of the last gsph_compute_derivatives held constant, plus out_mu + out_sigma * delta
+ *   per particle (delta[n][13] device, caller's order: position 3, velocity 3, density, stress xx yy
+ *   zz xy xz yz; NULL for the extrapolation alone), then the plasticity limiter.
+ * gsph_snapshot: save (restore = 0) or restore (restore = 1) the whole device state in slot 0..3. */
+int gsph_surrogate_features(gsph_ctx* ctx, const float* mu, const float* sigma, float* feat, void* stream);
+int gsph_surrogate_apply(gsph_ctx* ctx, const float* delta, const float* out_mu, const float* out_sigma, int32_t K,
+                         void* stream);
+int gsph_snapshot(gsph_ctx* ctx, int32_t slot, int32_t restore, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
  * batched ensemble: S independent simulations of uneven particle counts with one parameter set,
