@@ -51,7 +51,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["impact", "fluid", "plummer", "ensemble"], default="impact")
+    ap.add_argument("--workload", choices=["impact", "fluid", "plummer", "ensemble", "surrogate"], default="impact")
+    ap.add_argument("--windows", type=int, default=8, help="surrogate: windows of M proposals")
+    ap.add_argument("--model", default=os.path.join(ROOT, "grasph2_b200", "data", "surrogate_impact_n262144.npz"),
+                    help="surrogate: trained model (grasph2_b200/train_surrogate.py)")
     ap.add_argument("--nsims", type=int, default=512, help="simulations of the ensemble workload")
     ap.add_argument("--no-sequential", action="store_true",
                     help="ensemble: skip timing the simulations one by one in their own contexts")
@@ -62,6 +65,7 @@ def parse():
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak probe (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="particle count of the fluid / plummer workloads")
     ap.add_argument("--no-cull", action="store_true", help="all-pairs SPH sweeps (no chunk culling)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--scalar-fp32", action="store_true", help="scalar instead of paired f32x2 gravity kernel")
     ap.add_argument("--drift-steps", type=int, default=-1,
                     help="steps of the energy-drift comparison (plain, compensated, FP64); default 1000 on the "
@@ -396,6 +400,7 @@ def run_ensemble(args, rank, world, local):
     peak_tflops = None if args.no_peak else measure_fp32_peak(0.5)
     ens = Ensemble(params, sizes, make_options(accum=args.accum))
     ens.upload(packed, stream=stream)
+    shape = {"tile": 512, "ctas_per_sm": 0} if args.no_autotune else ens.autotune(1, stream)
     for _ in range(args.warmup):
         flush.zero_()
         ens.step(1, stream)
@@ -495,6 +500,7 @@ def run_ensemble(args, rank, world, local):
         "config": {"workload": desc, "nsims": int(len(sizes)), "n_total": n_total, "form": args.accum,
                    "l2": "flushed between timed steps (256 MiB write)",
                    "step": "every simulation: computeDerivatives + integrate, one persistent launch in a CUDA graph",
+                   "launch_shape": dict(shape, autotuned=not args.no_autotune),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "simulation_steps_per_s": value * len(sizes),
         "pair_interactions_per_s": pairs * value,
@@ -516,6 +522,71 @@ def run_ensemble(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_surrogate(args, rank, world, local):
+    """The learned K-substep surrogate on the impact at N=262,144 (v=0.5, y-offset 0.3, a seed outside the
+    training set) against the plain solver over the same substeps: windows of M=4 proposals, the last
+    judged by the plain integrator (accepted at <= 1e-3 relative position error and <= 1e-4 energy
+    error). Reports simulated time per wall-second of both forms and of the extrapolation without the
+    network, the acceptance, and the energy of each trajectory against the plain one at the end."""
+    import torch
+    torch.cuda.set_device(local)
+    from grasph2_b200 import ics
+    from grasph2_b200 import surrogate as S
+    from grasph2_b200.params import CONFIG4_N_BIG, CONFIG4_N_SMALL, config4_params
+    from grasph2_b200.sim import DeviceParticleBuffer
+    if rank != 0:
+        return
+    if not os.path.exists(args.model):
+        print(json.dumps({"metric": METRIC, "error": "trained model missing: %s" % args.model}))
+        sys.exit(1)
+    sur = S.Surrogate.load(args.model)
+    p = config4_params()
+    n = CONFIG4_N_BIG + CONFIG4_N_SMALL
+    st = ics.two_sphere_impact(CONFIG4_N_BIG, CONFIG4_N_SMALL, v_rel=0.5, y_offset=0.3, seed=20261299)
+    M, K = 4, sur.K
+    substeps = args.windows * M * K
+    dt = float(np.float32(p.fixed_dt))
+    sampler = ClockSampler(local)
+    out = {}
+    energies = {}
+    for form in ("plain", "surrogate", "extrapolation"):
+        with DeviceParticleBuffer(p, n) as pb:
+            pb.upload(st)
+            pb.step(max(args.warmup, 1))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if form == "plain":
+                pb.step(substeps)
+                torch.cuda.synchronize()
+                r = {"wall_s": time.perf_counter() - t0, "accepted": None, "windows": args.windows}
+            else:
+                r = S.advance(pb, sur, args.windows, M=M, use_net=(form == "surrogate"))
+            d = pb.diagnostics(0.0, fast=True)
+            energies[form] = d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
+            errs = np.array(r.get("errors", [(np.nan, np.nan)]))
+            out[form] = {"sim_time_per_wall_s": substeps * dt / r["wall_s"], "substeps_per_s": substeps / r["wall_s"],
+                         "accepted_windows": r["accepted"], "windows": r["windows"],
+                         "mean_position_error": float(np.nanmean(errs[:, 0])),
+                         "mean_energy_error": float(np.nanmean(errs[:, 1]))}
+    clocks = sampler.stop()
+    for form in out:
+        out[form]["energy_vs_plain_at_end"] = abs(energies[form] - energies["plain"]) / abs(energies["plain"])
+    value = out["surrogate"]["substeps_per_s"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": 1, "steps": substeps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded initial conditions)",
+        "config": {"workload": "learned K=8 surrogate, elastic-plastic impact N=%d (v=0.5, y-offset 0.3), windows of "
+                               "M=4 proposals judged by the plain integrator (<=1e-3 position, <=1e-4 energy)" % n,
+                   "model": os.path.basename(args.model), "substeps": substeps, "form": "surrogate"},
+        "forms": out,
+        "speedup_vs_plain": value / out["plain"]["substeps_per_s"],
+        "clocks": clocks,
+        "gpu_launches": None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -527,6 +598,9 @@ def main():
 
     if args.workload == "ensemble":
         run_ensemble(args, rank, world, local)
+        return
+    if args.workload == "surrogate":
+        run_surrogate(args, rank, world, local)
         return
     import torch
     torch.cuda.set_device(local)
@@ -554,6 +628,7 @@ def main():
     opts = dict(accum=args.accum, cull=not args.no_cull, scalar_fp32=args.scalar_fp32)
     pb = DeviceParticleBuffer(params, n, make_options(**opts))
     pb.upload(st, stream=stream)
+    shape = pb.launch_shape() if args.no_autotune else pb.autotune(3, stream)
     pb.profile_enable(True)
     for _ in range(args.warmup):
         flush.zero_()
@@ -599,6 +674,9 @@ def main():
     e2e_steps = 0 if args.no_e2e else max(5, min(args.steps, 50))
     pb.profile_enable(False)
     pb2 = DeviceParticleBuffer(params, n, make_options(**opts))
+    if not args.no_autotune and e2e_steps:
+        pb2.upload(pinned_in, stream=stream)
+        pb2.autotune(3, stream)
     e2e_ms = 0.0
     for k in range(e2e_steps + 3 if e2e_steps else 0):
         flush.zero_()
@@ -650,6 +728,7 @@ def main():
                    "gravity_fp32": "scalar" if args.scalar_fp32 else "f32x2",
                    "l2": "flushed between timed steps (256 MiB write)",
                    "step": "computeDerivatives + integrate, one captured CUDA graph",
+                   "launch_shape": dict(shape, autotuned=not args.no_autotune),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "pair_interactions_per_s": pairs_per_step * value,
         "kernel_ms_per_step": {k: (v[0] / v[1] if v[1] else None) for k, v in prof.items()},

@@ -80,6 +80,14 @@ class GsphHostParticles(ctypes.Structure):
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
+class GsphLaunchShape(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("cull", "grav_ipt", "grav_jt", "grav_nseg", "grav_x2", "sph_threads",
+                                               "sph_jt", "sph_nseg", "items")] + [("reserved", ctypes.c_int32 * 7)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class GsphHostParticles64(ctypes.Structure):
     """gsph_host_particles64: the double-precision host buffers."""
     _fields_ = [(name, _dp) for name, _, _ in ATTRIBUTES]
@@ -143,6 +151,8 @@ _SIGNATURES = {
                                         ctypes.c_void_p]),
     "gsph_diagnostics_fast": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
                                              ctypes.c_void_p]),
+    "gsph_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "gsph_launch_shape_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(GsphLaunchShape)]),
     "gsph_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_reorder": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "gsph_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
@@ -169,6 +179,8 @@ _SIGNATURES = {
     "gsph_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     "gsph_ensemble_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(GsphDiag),
                                                  ctypes.c_void_p]),
+    "gsph_ensemble_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                              ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
     "gsph_ensemble_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_tc_gemm_check": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,

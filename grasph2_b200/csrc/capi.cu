@@ -39,6 +39,7 @@ struct gsph_ctx {
     float* staging = nullptr;     // 9 * n floats
     double* staging64 = nullptr;  // 9 * n doubles
     double* diag_out = nullptr;   // device, 12 doubles
+    size_t part_cap = 0, gpart_cap = 0, item_cap = 0;  // floats allocated for a.part, a.gpart, sp.item_part
     std::vector<void*> snap[4];    // gsph_snapshot slots: saved copies of the state arrays (allocated on first save)
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -163,6 +164,7 @@ int pick_split(int64_t iblocks, int slots, int cap) {
 bool is_pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
 void* dalloc(gsph_ctx* c, size_t bytes, cudaError_t& e) {
+    if (e != cudaSuccess) return nullptr;  // an earlier allocation failed: keep its error
     void* p = nullptr;
     e = cudaMalloc(&p, bytes == 0 ? 16 : bytes);
     if (e == cudaSuccess) c->allocations.push_back(p);
@@ -470,8 +472,10 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     a.pos64 = static_cast<double*>(dalloc(c, 3 * n_pad * sizeof(double), ae));
     a.rhodot = static_cast<float*>(dalloc(c, n_pad * sizeof(float), ae));
     a.balsara = static_cast<float*>(dalloc(c, n_pad * sizeof(float), ae));
-    a.part = static_cast<float*>(dalloc(c, partial_floats(c->dp, L, n_pad) * sizeof(float), ae));
-    a.gpart = static_cast<float*>(dalloc(c, (L.cull ? gravity_partial_floats(L, n_pad) : 4) * sizeof(float), ae));
+    c->part_cap = partial_floats(c->dp, L, n_pad);
+    c->gpart_cap = L.cull ? gravity_partial_floats(L, n_pad) : 4;
+    a.part = static_cast<float*>(dalloc(c, c->part_cap * sizeof(float), ae));
+    a.gpart = static_cast<float*>(dalloc(c, c->gpart_cap * sizeof(float), ae));
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
@@ -483,7 +487,8 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         // most target + one per group (rounding up per group)
         const size_t kk = 2 * static_cast<size_t>(popc_c(field_mask<PASS_FUSED, false, true>()));
         const size_t cap = static_cast<size_t>(sp.item_target) + static_cast<size_t>(ngroups);
-        sp.item_part = static_cast<float*>(dalloc(c, cap * kk * kGroup * sizeof(float), ae));
+        c->item_cap = cap * kk * kGroup;
+        sp.item_part = static_cast<float*>(dalloc(c, c->item_cap * sizeof(float), ae));
         sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));
@@ -893,6 +898,190 @@ int gsph_snapshot(gsph_ctx* c, int32_t slot, int32_t restore, void* stream) {
         GSPH_CK(c, cudaMemcpyAsync(restore ? arrs[k].p : snap[k], restore ? snap[k] : arrs[k].p, arrs[k].bytes,
                                    cudaMemcpyDeviceToDevice, s), "snapshot copy");
     }
+    return GSPH_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// replace the tracked allocation *p by one of `floats` floats when it holds fewer (contents are scratch)
+int grow(gsph_ctx* c, float** p, size_t& cap, size_t floats) {
+    if (floats <= cap) return GSPH_OK;
+    float* q = nullptr;
+    GSPH_CK(c, cudaMalloc(&q, floats * sizeof(float)), "autotune allocation");
+    for (auto& a : c->allocations)
+        if (a == *p) a = q;
+    cudaFree(*p);
+    *p = q;
+    cap = floats;
+    return GSPH_OK;
+}
+
+// median over `reps` launches of f(stream), in ms (events on the stream, after one warm-up)
+template <typename F>
+int time_ms(gsph_ctx* c, cudaStream_t s, int reps, F&& f, float& ms) {
+    cudaEvent_t e0, e1;
+    GSPH_CK(c, cudaEventCreate(&e0), "event");
+    GSPH_CK(c, cudaEventCreate(&e1), "event");
+    std::vector<float> t;
+    int rc = f();
+    for (int r = 0; r < reps && rc == GSPH_OK; ++r) {
+        cudaEventRecord(e0, s);
+        rc = f();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float x = 0.0f;
+        cudaEventElapsedTime(&x, e0, e1);
+        t.push_back(x);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != GSPH_OK) return rc;
+    std::sort(t.begin(), t.end());
+    ms = t.empty() ? 0.0f : t[t.size() / 2];
+    return check_status(c, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsph_autotune(gsph_ctx* c, int32_t reps, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (c->fp64) return GSPH_OK;  // the double-precision passes have a fixed shape
+    if (reps < 1) reps = 3;
+    cudaStream_t s = as_stream(stream);
+    Launch& L = c->L;
+    const int64_t np = c->a.n_pad;
+    const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
+    const bool sph = has(c->dp, GSPH_SPH), grav = has(c->dp, GSPH_SELF_GRAVITY);
+    const bool profiling = c->profiling;
+    c->profiling = false;
+    int rc = GSPH_OK;
+    // 1. the all-pairs gravity kernel (its own pass in the culled and the gravity-only paths)
+    if (grav && (L.cull || !sph)) {
+        Launch best = L;
+        float best_ms = 1e30f;
+        const int ipts[3] = {2, 4, 8};
+        const int jts[2] = {128, 256};
+        for (int ip : ipts)
+            for (int jt : jts) {
+                if (np % (int64_t(L.grav_threads) * ip) || np % jt) continue;
+                const int64_t iblocks = np / (int64_t(L.grav_threads) * ip);
+                const int gcap = static_cast<int>(std::min<int64_t>(kMaxSplit, np / jt));
+                const int slots = c->sm_count * gravity_blocks_per_sm(ip, L.grav_threads, jt, comp);
+                const int s0 = pick_split(iblocks, slots, gcap);
+                const int segs[3] = {std::max(1, s0 / 2), s0, std::min(gcap, 2 * s0)};
+                for (int k = 0; k < 3; ++k) {
+                    if (k > 0 && segs[k] == segs[k - 1]) continue;
+                    Launch t = L;
+                    t.grav_ipt = ip;
+                    t.grav_jt = jt;
+                    t.grav_nseg = segs[k];
+                    if (L.cull) rc = grow(c, &c->a.gpart, c->gpart_cap, gravity_partial_floats(t, np));
+                    else rc = grow(c, &c->a.part, c->part_cap, partial_floats(c->dp, t, np));
+                    if (rc != GSPH_OK) break;
+                    float ms = 0.0f;
+                    rc = time_ms(c, s, reps, [&]() {
+                        const cudaError_t e = L.cull ? launch_gravity_partials(c->a, c->dp, t, s)
+                                                     : launch_gravity(c->a, c->dp, t, s);
+                        return e == cudaSuccess ? GSPH_OK : cuda_fail(c, e, "autotune gravity");
+                    }, ms);
+                    if (rc != GSPH_OK) break;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                    }
+                }
+                if (rc != GSPH_OK) break;
+            }
+        if (rc == GSPH_OK) {
+            L.grav_ipt = best.grav_ipt;
+            L.grav_jt = best.grav_jt;
+            L.grav_nseg = best.grav_nseg;
+        }
+    }
+    // 2. the SPH passes: work items of the culled kernels, or the all-pairs tile shape
+    if (rc == GSPH_OK && sph) {
+        Launch best = L;
+        float best_ms = 1e30f;
+        std::vector<Launch> cands;
+        if (L.cull) {
+            for (int f : {3, 6, 12, 24}) {
+                Launch t = L;
+                t.item_grid = L.item_grid;
+                cands.push_back(t);
+                cands.back().nseg = -f;  // marks the item multiple (restored below)
+            }
+        } else {
+            for (int th : {64, 128, 256})
+                for (int jt : {128, 256, 512}) {
+                    if (np % jt || np % th) continue;
+                    const int cap = static_cast<int>(std::min<int64_t>(kMaxSplit, np / jt));
+                    const int s0 = pick_split(np / th, c->sm_count * 4, cap);
+                    for (int sg : {std::max(1, s0 / 2), s0, std::min(cap, 2 * s0)}) {
+                        Launch t = L;
+                        t.threads = th;
+                        t.jt = jt;
+                        t.nseg = sg;
+                        cands.push_back(t);
+                    }
+                }
+        }
+        const int ngroups = static_cast<int>(np / kGroup);
+        const size_t kk = 2 * static_cast<size_t>(popc_c(field_mask<PASS_FUSED, false, true>()));
+        for (Launch t : cands) {
+            const int target_mult = t.nseg < 0 ? -t.nseg : 0;
+            if (target_mult) {
+                t.nseg = L.nseg;
+                rc = grow(c, &c->sp.item_part, c->item_cap,
+                          (static_cast<size_t>(target_mult) * L.item_grid + ngroups) * kk * kGroup);
+                if (rc != GSPH_OK) break;
+                c->sp.item_target = target_mult * L.item_grid;
+            } else {
+                rc = grow(c, &c->a.part, c->part_cap, partial_floats(c->dp, t, np));
+                if (rc != GSPH_OK) break;
+            }
+            const Launch saved = L;
+            L = t;
+            float ms = 0.0f;
+            rc = time_ms(c, s, reps, [&]() { return derivatives(c, s); }, ms);
+            L = saved;
+            if (rc != GSPH_OK) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+                if (target_mult) best.item_grid = -target_mult;  // remembered as a multiple
+            }
+        }
+        if (rc == GSPH_OK) {
+            if (L.cull) {
+                c->sp.item_target = -best.item_grid * L.item_grid;
+            } else {
+                L.threads = best.threads;
+                L.jt = best.jt;
+                L.nseg = best.nseg;
+            }
+        }
+    }
+    c->profiling = profiling;
+    drop_graph(c);  // the next gsph_step captures the new shapes
+    return rc;
+}
+
+int gsph_launch_shape_get(gsph_ctx* c, gsph_launch_shape* out) {
+    if (!c || !out) return GSPH_E_INVALID;
+    std::memset(out, 0, sizeof *out);
+    out->cull = c->L.cull;
+    out->grav_ipt = c->L.grav_ipt;
+    out->grav_jt = c->L.grav_jt;
+    out->grav_nseg = c->L.grav_nseg;
+    out->grav_x2 = c->L.grav_x2;
+    out->sph_threads = c->L.threads;
+    out->sph_jt = c->L.jt;
+    out->sph_nseg = c->L.nseg;
+    out->items = c->L.cull ? c->sp.item_target : 0;
     return GSPH_OK;
 }
 

@@ -45,7 +45,7 @@ namespace {
 constexpr int kEnsThreads = 128;
 constexpr int kEnsIpt = 4;                    // particles per thread (two f32x2 pairs in the sweep)
 constexpr int kEnsGroup = kEnsThreads * kEnsIpt;    // particles per work item
-constexpr int kEnsTile = 512;                 // j-particles per shared-memory stage
+constexpr int kEnsTile = 512;                 // default j-particles per shared-memory stage (autotuned)
 constexpr int kEnsCap = 256;                  // neighbour-list slots per particle
 constexpr int kEnsDiagF = 12;                 // diagnostic fields (as gsph_diagnostics)
 
@@ -64,6 +64,7 @@ struct EnsView {
     int* nbcnt;          // [n] neighbour counts (kEnsCap + 1: the list overflowed)
     int64_t n;
     float kick_dt;
+    int tile;            // j-particles per shared-memory stage of the DENS sweep
 };
 
 // ---- paired FP32 (PTX ISA 8.6, sm_100+): two lanes per instruction, IEEE single precision ---------
@@ -129,14 +130,15 @@ __device__ __forceinline__ bool wait_count(const int* ctr, int target, int* stat
     return ok;
 }
 
-// Two-stage bulk-copy pipeline over a contiguous j-range [j0, j1) of one float4 stream, kEnsTile records
+// Two-stage bulk-copy pipeline over a contiguous j-range [j0, j1) of one float4 stream, `tile` records
 // per stage (the last one ragged). The stage counter runs on across items so the mbarrier phases stay
 // in step.
 struct RangePipe {
-    float4* buf;    // shared [2][kEnsTile]
+    float4* buf;    // shared [2][tile]
     uint64_t* bar;  // shared [2]
     const float4* src;
     int* status;
+    int tile;       // j-particles per stage
     uint32_t kst = 0;
 
     __device__ __forceinline__ void init() {
@@ -149,16 +151,16 @@ struct RangePipe {
     }
     __device__ __forceinline__ void issue(int b, int64_t j, int nj) {
         mbar_expect_tx(&bar[b], static_cast<uint32_t>(nj * sizeof(float4)));
-        bulk_g2s(buf + static_cast<int64_t>(b) * kEnsTile, src + j, static_cast<uint32_t>(nj * sizeof(float4)), &bar[b]);
+        bulk_g2s(buf + static_cast<int64_t>(b) * tile, src + j, static_cast<uint32_t>(nj * sizeof(float4)), &bar[b]);
     }
     // body(stage, nj, first j of the stage); false if a wait gave up
     template <typename Body>
     __device__ __forceinline__ bool run(int64_t j0, int64_t j1, Body&& body) {
         const int64_t len = j1 - j0;
-        const int nst = static_cast<int>((len + kEnsTile - 1) / kEnsTile);
-        auto cnt = [&](int st) { return static_cast<int>(lmin(kEnsTile, len - static_cast<int64_t>(st) * kEnsTile)); };
+        const int nst = static_cast<int>((len + tile - 1) / tile);
+        auto cnt = [&](int st) { return static_cast<int>(lmin(tile, len - static_cast<int64_t>(st) * tile)); };
         if (threadIdx.x == 0)
-            for (int st = 0; st < 2 && st < nst; ++st) issue((kst + st) & 1, j0 + static_cast<int64_t>(st) * kEnsTile, cnt(st));
+            for (int st = 0; st < 2 && st < nst; ++st) issue((kst + st) & 1, j0 + static_cast<int64_t>(st) * tile, cnt(st));
         for (int st = 0; st < nst; ++st) {
             const int b = kst & 1;
             const bool ok = mbar_wait_bounded(&bar[b], (kst >> 1) & 1, status);
@@ -168,9 +170,9 @@ struct RangePipe {
                 __syncthreads();
                 return false;
             }
-            body(buf + static_cast<int64_t>(b) * kEnsTile, cnt(st), j0 + static_cast<int64_t>(st) * kEnsTile);
+            body(buf + static_cast<int64_t>(b) * tile, cnt(st), j0 + static_cast<int64_t>(st) * tile);
             __syncthreads();
-            if (threadIdx.x == 0 && st + 2 < nst) issue(b, j0 + static_cast<int64_t>(st + 2) * kEnsTile, cnt(st + 2));
+            if (threadIdx.x == 0 && st + 2 < nst) issue(b, j0 + static_cast<int64_t>(st + 2) * tile, cnt(st + 2));
             ++kst;
         }
         return true;
@@ -370,7 +372,8 @@ __global__ void __launch_bounds__(kEnsThreads) k_ensemble(DevArrays a, DevParams
     __shared__ int s_item, s_flag;
     RangePipe pipe;
     pipe.buf = reinterpret_cast<float4*>(smem_raw);
-    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * kEnsTile * sizeof(float4));
+    pipe.tile = v.tile;
+    pipe.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * static_cast<size_t>(v.tile) * sizeof(float4));
     pipe.src = a.posm;
     pipe.status = a.status;
     pipe.init();
@@ -556,47 +559,54 @@ __global__ void k_ens_iota(int* v, int64_t n) {
     if (i < n) v[i] = static_cast<int>(i);
 }
 
-size_t ens_smem() { return pipe_smem_bytes(1, kEnsTile); }
+size_t ens_smem(int tile) { return pipe_smem_bytes(1, tile); }
 
 template <int GRAV, bool SPH, int PASS, bool SOLIDS, bool COMP>
-cudaError_t launch_t(const DevArrays& a, const DevParams& p, const EnsView& v, int sm_count, cudaStream_t s) {
+cudaError_t launch_t(const DevArrays& a, const DevParams& p, const EnsView& v, int sm_count, int per_sm_cap,
+                     cudaStream_t s) {
     auto kern = k_ensemble<GRAV, SPH, PASS, SOLIDS, COMP>;
-    const size_t smem = ens_smem();
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEnsThreads, smem);
+    const size_t smem = ens_smem(v.tile);
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEnsThreads, smem);
+    if (e != cudaSuccess) return e;
+    per_sm = std::max(per_sm, 1);
+    if (per_sm_cap > 0) per_sm = std::min(per_sm, per_sm_cap);
     const int total = v.ngroups * v.nstages;
-    const int grid = std::max(1, std::min(total, sm_count * std::max(per_sm, 1)));
+    const int grid = std::max(1, std::min(total, sm_count * per_sm));
     kern<<<grid, kEnsThreads, smem, s>>>(a, p, v);
     return cudaGetLastError();
 }
 
 template <int GRAV, bool SPH>
-cudaError_t launch_g(const DevArrays& a, const DevParams& p, const EnsView& v, bool comp, int sm_count, cudaStream_t s) {
+cudaError_t launch_g(const DevArrays& a, const DevParams& p, const EnsView& v, bool comp, int sm_count, int cap,
+                     cudaStream_t s) {
     if (!SPH) {
-        return comp ? launch_t<GRAV, false, PASS_ACC, false, true>(a, p, v, sm_count, s)
-                    : launch_t<GRAV, false, PASS_ACC, false, false>(a, p, v, sm_count, s);
+        return comp ? launch_t<GRAV, false, PASS_ACC, false, true>(a, p, v, sm_count, cap, s)
+                    : launch_t<GRAV, false, PASS_ACC, false, false>(a, p, v, sm_count, cap, s);
     }
     const bool solids = has(p, GSPH_SOLIDS);
     const bool vgrad = solids || has(p, GSPH_INTEGRATE_DENSITY);
     if (solids)
-        return comp ? launch_t<GRAV, true, PASS_FUSED, true, true>(a, p, v, sm_count, s)
-                    : launch_t<GRAV, true, PASS_FUSED, true, false>(a, p, v, sm_count, s);
+        return comp ? launch_t<GRAV, true, PASS_FUSED, true, true>(a, p, v, sm_count, cap, s)
+                    : launch_t<GRAV, true, PASS_FUSED, true, false>(a, p, v, sm_count, cap, s);
     if (vgrad)
-        return comp ? launch_t<GRAV, true, PASS_FUSED, false, true>(a, p, v, sm_count, s)
-                    : launch_t<GRAV, true, PASS_FUSED, false, false>(a, p, v, sm_count, s);
-    return comp ? launch_t<GRAV, true, PASS_ACC, false, true>(a, p, v, sm_count, s)
-                : launch_t<GRAV, true, PASS_ACC, false, false>(a, p, v, sm_count, s);
+        return comp ? launch_t<GRAV, true, PASS_FUSED, false, true>(a, p, v, sm_count, cap, s)
+                    : launch_t<GRAV, true, PASS_FUSED, false, false>(a, p, v, sm_count, cap, s);
+    return comp ? launch_t<GRAV, true, PASS_ACC, false, true>(a, p, v, sm_count, cap, s)
+                : launch_t<GRAV, true, PASS_ACC, false, false>(a, p, v, sm_count, cap, s);
 }
 
 cudaError_t launch_ensemble(const DevArrays& a, const DevParams& p, const EnsView& v, bool comp, int sm_count,
-                            cudaStream_t s) {
+                            int cap, cudaStream_t s) {
     const bool sph = has(p, GSPH_SPH);
     if (!has(p, GSPH_SELF_GRAVITY))
-        return sph ? launch_g<0, true>(a, p, v, comp, sm_count, s) : launch_g<0, false>(a, p, v, comp, sm_count, s);
+        return sph ? launch_g<0, true>(a, p, v, comp, sm_count, cap, s) : launch_g<0, false>(a, p, v, comp, sm_count, cap, s);
     if (p.eps2 > 0.0f)
-        return sph ? launch_g<1, true>(a, p, v, comp, sm_count, s) : launch_g<1, false>(a, p, v, comp, sm_count, s);
-    return sph ? launch_g<2, true>(a, p, v, comp, sm_count, s) : launch_g<2, false>(a, p, v, comp, sm_count, s);
+        return sph ? launch_g<1, true>(a, p, v, comp, sm_count, cap, s) : launch_g<1, false>(a, p, v, comp, sm_count, cap, s);
+    return sph ? launch_g<2, true>(a, p, v, comp, sm_count, cap, s) : launch_g<2, false>(a, p, v, comp, sm_count, cap, s);
 }
 
 }  // namespace
@@ -632,6 +642,8 @@ struct gsph_ensemble {
     double* tmp8 = nullptr;
     float* bbox = nullptr;               // [S][8]
     int steps_since_sort = 0;
+    int tile = kEnsTile;   // DENS j-tile (autotuned)
+    int per_sm_cap = 0;    // CTAs per SM of the persistent grid (0: as many as fit; autotuned)
     std::vector<void*> allocations;
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -696,6 +708,7 @@ EnsView view_of(const gsph_ensemble* e, const int* stages, int nstages) {
     v.nbcnt = e->nbcnt;
     v.n = e->a.n;
     v.kick_dt = e->dp.fixed_dt;
+    v.tile = e->tile;
     return v;
 }
 
@@ -704,7 +717,8 @@ int run_stages(gsph_ensemble* e, const int* stages, int nstages, float kick_dt, 
     EnsView v = view_of(e, stages, nstages);
     v.kick_dt = kick_dt;
     ENS_CK(e, cudaMemsetAsync(e->counters, 0, (1 + 2 * static_cast<size_t>(e->nsims)) * sizeof(int), s), "counter reset");
-    ENS_CK(e, launch_ensemble(e->a, e->dp, v, e->opt.accum == GSPH_ACCUM_COMPENSATED, e->sm_count, s), "ensemble launch");
+    ENS_CK(e, launch_ensemble(e->a, e->dp, v, e->opt.accum == GSPH_ACCUM_COMPENSATED, e->sm_count, e->per_sm_cap, s),
+           "ensemble launch");
     e->launches += 1;
     return GSPH_OK;
 }
@@ -1021,6 +1035,56 @@ int gsph_ensemble_diagnostics(gsph_ensemble* e, double half_kick, gsph_diag* out
         o.mass = d[10];
     }
     return GSPH_OK;
+}
+
+int gsph_ensemble_autotune(gsph_ensemble* e, int32_t reps, int32_t* tile, int32_t* per_sm, void* stream) {
+    if (!e) return GSPH_E_INVALID;
+    if (reps < 1) reps = 2;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int st[3];
+    const int ns = derivative_stages(e, st);  // derivatives only: the state is left as it was
+    cudaEvent_t e0, e1;
+    ENS_CK(e, cudaEventCreate(&e0), "event");
+    ENS_CK(e, cudaEventCreate(&e1), "event");
+    float best = 1e30f;
+    int bt = e->tile, bp = e->per_sm_cap;
+    int rc = GSPH_OK;
+    for (int t : {256, 512, 1024}) {
+        for (int cap : {0, 2, 3, 4}) {
+            e->tile = t;
+            e->per_sm_cap = cap;
+            std::vector<float> ms;
+            for (int r = 0; r <= reps && rc == GSPH_OK; ++r) {
+                cudaEventRecord(e0, s);
+                rc = run_stages(e, st, ns, e->dp.fixed_dt, s);
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float x = 0.0f;
+                cudaEventElapsedTime(&x, e0, e1);
+                if (r > 0) ms.push_back(x);
+            }
+            if (rc != GSPH_OK) break;
+            std::sort(ms.begin(), ms.end());
+            if (ms[ms.size() / 2] < best) {
+                best = ms[ms.size() / 2];
+                bt = t;
+                bp = cap;
+            }
+        }
+        if (rc != GSPH_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    e->tile = bt;
+    e->per_sm_cap = bp;
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->graph_exec = nullptr;
+    e->graph = nullptr;
+    if (rc != GSPH_OK) return rc;
+    if (tile) *tile = bt;
+    if (per_sm) *per_sm = bp;
+    return ens_status(e, s);
 }
 
 int gsph_ensemble_launch_count(const gsph_ensemble* e, int64_t* count) {

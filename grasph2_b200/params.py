@@ -130,6 +130,16 @@ def config1_params():
 CONFIG4_N_BIG, CONFIG4_N_SMALL = 233017, 29127  # N = 262,144 split 8:1 like the 65,536 impact (equal number density)
 
 
+def impact_params(n_big, n_small, **over):
+    """The elastic-plastic impact physics (as the N=65,536 impact) for another particle count: h = 2.5 x
+    the mean spacing of n_big + n_small particles in spheres of radius 1 and 0.5."""
+    kw = dict(switches=("SELF_GRAVITY", "SPH", "SOLIDS", "ARTIFICIAL_VISCOSITY", "PLASTICITY_MIESE"),
+              H=impact_smoothing_length(n_big, 1.0, n_small, 0.5), grav_eps=0.01, rho0=1.0, bulk=10.0, dbulk_dp=1.0,
+              soundspeed=math.sqrt(10.0), shear=5.0, Y=0.5, av_alpha=1.0, av_beta=2.0, fixed_dt=1e-4)
+    kw.update(over)
+    return make_params(**kw)
+
+
 def config4_params():
     """The elastic-plastic impact physics at N=262,144 (h = 2.5 x mean spacing = 0.0655), for the learned
     surrogate: rho0=1, Murnaghan K=10 dK0=1, shear=5, von Mises Y=0.5, AV alpha=1 beta=2, G=1 eps=0.01,

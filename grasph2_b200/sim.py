@@ -163,6 +163,16 @@ class DeviceParticleBuffer:
         self._check(f(self._ctx, float(half_kick), ctypes.byref(d), _stream_handle(stream)))
         return d.as_dict()
 
+    def autotune(self, reps=3, stream=None):
+        """Time candidate launch shapes on the current state and keep the fastest; returns the shape."""
+        self._check(self.lib.gsph_autotune(self._ctx, int(reps), _stream_handle(stream)))
+        return self.launch_shape()
+
+    def launch_shape(self):
+        sh = _abi.GsphLaunchShape()
+        self._check(self.lib.gsph_launch_shape_get(self._ctx, ctypes.byref(sh)))
+        return sh.as_dict()
+
     def launch_count(self):
         c = ctypes.c_int64()
         self._check(self.lib.gsph_launch_count(self._ctx, ctypes.byref(c)))
@@ -274,6 +284,13 @@ class Ensemble:
         arr = (GsphDiag * self.nsims)()
         self._check(self.lib.gsph_ensemble_diagnostics(self._h, float(half_kick), arr, _stream_handle(stream)))
         return [d.as_dict() for d in arr]
+
+    def autotune(self, reps=2, stream=None):
+        """Time the DENS j-tile and the persistent grid's CTAs per SM; keep the fastest."""
+        t, c = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self.lib.gsph_ensemble_autotune(self._h, int(reps), ctypes.byref(t), ctypes.byref(c),
+                                                    _stream_handle(stream)))
+        return {"tile": t.value, "ctas_per_sm": c.value}
 
     def launch_count(self):
         c = ctypes.c_int64()

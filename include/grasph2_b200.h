@@ -259,6 +259,17 @@ int gsph_diagnostics(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stre
  * relative error of e_grav ~1e-7): one FP32 N^2 sweep instead of an FP64 one, for frequent checks. */
 int gsph_diagnostics_fast(gsph_ctx* ctx, double half_kick, gsph_diag* out, void* stream);
 
+/* Autotuner (no counterpart in the reference): times candidate launch shapes on the context's current
+ * state and keeps the fastest, `reps` timed launches each (median): the gravity kernel's i-blocking,
+ * j-tile and j-split; the culled SPH passes' work-item count, or the all-pairs SPH tile shape. Results
+ * change only by summation order. The next gsph_step re-captures its graph. */
+int gsph_autotune(gsph_ctx* ctx, int32_t reps, void* stream);
+typedef struct gsph_launch_shape {
+    int32_t cull, grav_ipt, grav_jt, grav_nseg, grav_x2, sph_threads, sph_jt, sph_nseg, items;
+    int32_t reserved[7];
+} gsph_launch_shape;
+int gsph_launch_shape_get(gsph_ctx* ctx, gsph_launch_shape* out);
+
 /* Number of particles of the context. */
 int gsph_size(gsph_ctx* ctx, int64_t* n);
 /* Re-sort the device-side particle order along a Hilbert curve of the current positions (a no-op
@@ -353,6 +364,10 @@ int gsph_ensemble_integrate(gsph_ensemble* e, int32_t not_first_step, void* stre
 int gsph_ensemble_step(gsph_ensemble* e, int32_t nsteps, void* stream);
 /* FP64 diagnostics of every simulation into out[nsims] (as gsph_diagnostics); synchronises `stream` */
 int gsph_ensemble_diagnostics(gsph_ensemble* e, double half_kick, gsph_diag* out, void* stream);
+/* Autotuner: times the DENS j-tile (256, 512, 1024) and the CTAs per SM of the persistent grid on the
+ * current state (derivative launches only) and keeps the fastest; tile / per_sm (nullable) receive the
+ * choice (per_sm 0: as many as fit). */
+int gsph_ensemble_autotune(gsph_ensemble* e, int32_t reps, int32_t* tile, int32_t* per_sm, void* stream);
 int gsph_ensemble_launch_count(const gsph_ensemble* e, int64_t* count);
 /* text of the last failure on `e` (or of the last failed gsph_ensemble_create when e is NULL) */
 const char* gsph_ensemble_last_error(const gsph_ensemble* e);

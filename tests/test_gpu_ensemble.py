@@ -220,3 +220,20 @@ def test_ensemble_rejects_unsupported():
     with pytest.raises(GsphError) as e:
         Ensemble(config0_params(), [100], make_options(precision="double"))
     assert e.value.code == -7
+
+
+def test_ensemble_autotune_keeps_results(oracle):
+    p = VARIANTS["solid"]()
+    sizes = [3000, 700]
+    states = [sim_state(n, seed=800 + k) for k, n in enumerate(sizes)]
+    with Ensemble(p, sizes) as ens:
+        ens.upload(pack_states(states))
+        shape = ens.autotune(1)
+        assert shape["tile"] in (256, 512, 1024)
+        ens.compute_derivatives()
+        got = ens.split(ens.download())
+        ens.step(2)
+    for k, st in enumerate(states):
+        ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st, trials=1)
+        for f, tol in fields(p).items():
+            check_within(got[k][f], ref[f], sens[f], tol, "autotuned sim %d %s" % (k, f))
