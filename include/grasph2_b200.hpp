@@ -110,10 +110,62 @@ public:
         check(gsph_diagnostics(ctx_, half_kick, &d, stream), ctx_);
         return d;
     }
+    // time candidate launch shapes on the current state and keep the fastest
+    gsph_launch_shape autotune(int reps = 3, void* stream = nullptr) {
+        check(gsph_autotune(ctx_, reps, stream), ctx_);
+        gsph_launch_shape s{};
+        check(gsph_launch_shape_get(ctx_, &s), ctx_);
+        return s;
+    }
     gsph_ctx* get() const { return ctx_; }
 
 private:
     gsph_ctx* ctx_ = nullptr;
+};
+
+// Many simulations of one physics setup, advanced together (RAII over gsph_ensemble_*). Host buffers
+// hold the simulations back to back in the order of offsets().
+class Ensemble {
+public:
+    Ensemble(const gsph_params& p, const std::vector<int64_t>& counts, const gsph_options* opt = nullptr) {
+        int rc = gsph_ensemble_create(&p, opt, static_cast<int32_t>(counts.size()), counts.data(), &e_);
+        if (rc != GSPH_OK) throw Error(rc, gsph_ensemble_last_error(nullptr));
+        off_.resize(counts.size() + 1);
+        chk(gsph_ensemble_offsets(e_, off_.data()));
+    }
+    ~Ensemble() {
+        if (e_) gsph_ensemble_destroy(e_);
+    }
+    Ensemble(const Ensemble&) = delete;
+    Ensemble& operator=(const Ensemble&) = delete;
+    const std::vector<int64_t>& offsets() const { return off_; }
+    int64_t size() const { return off_.back(); }
+    void upload(HostParticleBuffer& h, uint32_t mask, void* stream = nullptr) {
+        gsph_host_particles v = h.view();
+        chk(gsph_ensemble_upload(e_, mask, &v, stream));
+    }
+    void download(HostParticleBuffer& h, uint32_t mask = GSPH_ALL_ATTRIBS, void* stream = nullptr) {
+        if (h.size() != static_cast<size_t>(size())) h.resize(static_cast<size_t>(size()));
+        gsph_host_particles v = h.view();
+        chk(gsph_ensemble_download(e_, mask, &v, stream));
+    }
+    void step(int nsteps, void* stream = nullptr) { chk(gsph_ensemble_step(e_, nsteps, stream)); }
+    std::vector<gsph_diag> diagnostics(double half_kick = 0.0, void* stream = nullptr) {
+        std::vector<gsph_diag> d(off_.size() - 1);
+        chk(gsph_ensemble_diagnostics(e_, half_kick, d.data(), stream));
+        return d;
+    }
+    void autotune(int reps = 2, void* stream = nullptr) {
+        chk(gsph_ensemble_autotune(e_, reps, nullptr, nullptr, stream));
+    }
+    gsph_ensemble* get() const { return e_; }
+
+private:
+    void chk(int rc) {
+        if (rc != GSPH_OK) throw Error(rc, gsph_ensemble_last_error(e_));
+    }
+    gsph_ensemble* e_ = nullptr;
+    std::vector<int64_t> off_;
 };
 
 // hostBuffer = deviceBuffer

@@ -66,6 +66,31 @@ int main(int argc, char** argv) {
     } catch (const gsph::Error& e) {
         if (e.code() != GSPH_E_INVALID) return 1;
     }
+    {  // the same physics as an ensemble of three simulations of uneven sizes
+        gsph_params q = p;
+        q.flags &= ~(GSPH_VARIABLE_TIMESTEP | GSPH_BALSARA_SWITCH);
+        std::vector<int64_t> counts = {300, 77, 512};
+        gsph::Ensemble ens(q, counts);
+        gsph::HostParticleBuffer h(static_cast<size_t>(ens.size()));
+        for (size_t i = 0; i < h.size(); ++i) {
+            const double u = std::fmod(0.6180339887 * (i + 1), 1.0), w = std::fmod(0.7548776662 * (i + 1), 1.0),
+                         z = std::fmod(0.5698402910 * (i + 1), 1.0);
+            h.pos[3 * i] = static_cast<float>(u - 0.5);
+            h.pos[3 * i + 1] = static_cast<float>(w - 0.5);
+            h.pos[3 * i + 2] = static_cast<float>(z - 0.5);
+            h.mass[i] = 1.0f / 300.0f;
+            h.density[i] = static_cast<float>(q.rho0);
+        }
+        ens.upload(h, GSPH_POS | GSPH_MASS | GSPH_VEL | GSPH_DENSITY | GSPH_DSTRESS);
+        ens.autotune(1);
+        ens.step(3);
+        ens.download(h);
+        const std::vector<gsph_diag> d = ens.diagnostics();
+        if (d.size() != counts.size() || !(d[2].mass > 0)) {
+            std::printf("ensemble check failed\n");
+            return 1;
+        }
+    }
     std::printf("ADAPTER OK t=%.6f file=%s\n", t, fn.c_str());
     return 0;
 }
