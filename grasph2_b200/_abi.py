@@ -137,6 +137,16 @@ _SIGNATURES = {
                                    ctypes.c_void_p]),
     "gsph_download": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
                                      ctypes.c_void_p]),
+    "gsph_upload_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
+                                          ctypes.c_void_p]),
+    "gsph_ic_uniform_sphere": (ctypes.c_int, [ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              ctypes.POINTER(ctypes.c_double), ctypes.c_uint64, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_ic_plummer": (ctypes.c_int, [ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]),
+    "gsph_ic_com_correct": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
     "gsph_upload_f64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles64),
                                        ctypes.c_void_p]),
     "gsph_download_f64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles64),

@@ -563,7 +563,22 @@ int gsph_destroy(gsph_ctx* c) {
     return GSPH_OK;
 }
 
+namespace {
+int upload_any(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void* stream, cudaMemcpyKind kind);
+}  // namespace
+
 int gsph_upload(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void* stream) {
+    return upload_any(c, mask, src, stream, cudaMemcpyHostToDevice);
+}
+
+int gsph_upload_device(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void* stream) {
+    return upload_any(c, mask, src, stream, cudaMemcpyDeviceToDevice);
+}
+
+}  // extern "C"
+
+namespace {
+int upload_any(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void* stream, cudaMemcpyKind kind) {
     if (!c) return GSPH_E_INVALID;
     if (!src) return fail(c, GSPH_E_INVALID, "src is NULL");
     if (mask & ~GSPH_ALL_ATTRIBS) return fail(c, GSPH_E_INVALID, "unknown attribute bits in mask");
@@ -575,8 +590,7 @@ int gsph_upload(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void
     cudaStream_t s = as_stream(stream);
     for (int k = 0; k < 11; ++k) {
         if (!(mask >> k & 1u)) continue;
-        GSPH_CK(c, cudaMemcpyAsync(c->staging, ptrs[k], comps[k] * c->a.n * sizeof(float), cudaMemcpyHostToDevice, s),
-                "upload copy");
+        GSPH_CK(c, cudaMemcpyAsync(c->staging, ptrs[k], comps[k] * c->a.n * sizeof(float), kind, s), "upload copy");
         if (c->fp64) GSPH_CK(c, launch64_pack(c->a64, k, c->staging, s), "upload pack");
         else GSPH_CK(c, launch_pack(c->a, k, c->staging, ext_map(c), s), "upload pack");
         c->launches += 1;
@@ -592,6 +606,9 @@ int gsph_upload(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void
     }
     return GSPH_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int gsph_download(gsph_ctx* c, uint32_t mask, gsph_host_particles* dst, void* stream) {
     if (!c) return GSPH_E_INVALID;

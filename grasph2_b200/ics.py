@@ -102,3 +102,50 @@ def ensemble_sizes(count=512, lo=1024, hi=32768, seed=0):
     """Seeded log-uniform integer sizes in [lo, hi]."""
     rng = np.random.Generator(np.random.PCG64(seed))
     return np.floor(np.exp(rng.uniform(math.log(lo), math.log(hi + 1), count))).astype(np.int64).clip(lo, hi)
+
+
+# ---- generators on the device (gsph_ic_*): torch CUDA tensors in the host layout ------------------
+def _dev(n, k=None):
+    import torch
+    return torch.empty((n, k) if k else (n,), dtype=torch.float32, device="cuda")
+
+
+def _com(lib, n, st):
+    import ctypes
+    import torch
+    scratch = torch.empty(7 * 256, dtype=torch.float64, device="cuda")
+    rc = lib.gsph_ic_com_correct(n, ctypes.c_void_p(st["pos"].data_ptr()), ctypes.c_void_p(st["vel"].data_ptr()),
+                                 ctypes.c_void_p(st["mass"].data_ptr()), ctypes.c_void_p(scratch.data_ptr()), None)
+    if rc != 0:
+        raise RuntimeError(lib.gsph_last_error(None).decode())
+
+
+def uniform_sphere_device(n, radius=1.0, total_mass=1.0, rho0=1.0, omega=(0.0, 0.0, 0.0), seed=0, com_correct=True):
+    """Uniform sphere generated on the GPU (counter-based draws; see include/grasph2_b200.h)."""
+    import ctypes
+    from ._abi import load_library
+    lib = load_library()
+    st = {"pos": _dev(n, 3), "vel": _dev(n, 3), "mass": _dev(n), "density": _dev(n)}
+    w = (ctypes.c_double * 3)(*omega)
+    rc = lib.gsph_ic_uniform_sphere(n, radius, total_mass, rho0, w, seed, *(ctypes.c_void_p(st[k].data_ptr())
+                                    for k in ("pos", "vel", "mass", "density")), None)
+    if rc != 0:
+        raise RuntimeError(lib.gsph_last_error(None).decode())
+    if com_correct:
+        _com(lib, n, st)
+    return st
+
+
+def plummer_sphere_device(n, a=1.0, total_mass=1.0, G=1.0, seed=0, com_correct=True):
+    """Plummer sphere generated on the GPU."""
+    import ctypes
+    from ._abi import load_library
+    lib = load_library()
+    st = {"pos": _dev(n, 3), "vel": _dev(n, 3), "mass": _dev(n)}
+    rc = lib.gsph_ic_plummer(n, a, total_mass, G, seed, *(ctypes.c_void_p(st[k].data_ptr())
+                             for k in ("pos", "vel", "mass")), None)
+    if rc != 0:
+        raise RuntimeError(lib.gsph_last_error(None).decode())
+    if com_correct:
+        _com(lib, n, st)
+    return st

@@ -111,6 +111,18 @@ class DeviceParticleBuffer:
         self._check(self.lib.gsph_download(self._ctx, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
         return {k: st[k] for k in names} if attributes is not None else st
 
+    def upload_device(self, state, attributes=None, stream=None):
+        """Upload from device arrays in the host layout (torch CUDA float32 tensors)."""
+        names = [k for k in ATTR_BITS if k in state] if attributes is None else list(attributes)
+        hp = GsphHostParticles()
+        for k in names:
+            v = state[k]
+            if v.shape[0] != self.n or not v.is_cuda or not v.is_contiguous():
+                raise ValueError("attribute %s must be a contiguous CUDA tensor with %d rows" % (k, self.n))
+            setattr(hp, k, ctypes.cast(ctypes.c_void_p(v.data_ptr()), ctypes.POINTER(ctypes.c_float)))
+        self._check(self.lib.gsph_upload_device(self._ctx, mask_of(names), ctypes.byref(hp), _stream_handle(stream)))
+        return self
+
     def upload_f64(self, state, attributes=None, stream=None):
         """Double-precision host buffers (the reference's DOUBLE_PRECISION layout)."""
         names = [k for k in ATTR_BITS if k in state] if attributes is None else list(attributes)

@@ -338,6 +338,22 @@ int gsph_surrogate_apply(gsph_ctx* ctx, const float* delta, const float* out_mu,
 int gsph_snapshot(gsph_ctx* ctx, int32_t slot, int32_t restore, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * initial conditions on the device (the reference's particle sources, src/initialConditions/
+ * particleSources/UniformSphere.cu, PlummerSphere.cu, and the centre-of-mass correction of
+ * InitGenerator.h:113-152). Outputs are device arrays in the host layout of gsph_host_particles
+ * (pos/vel 3n floats), ready for gsph_upload_device. Draws are counter-based (splitmix64 of seed,
+ * draw and particle index): independent of the launch shape and reproducible on the host.
+ * ------------------------------------------------------------------------------------------- */
+int gsph_ic_uniform_sphere(int64_t n, double radius, double total_mass, double rho0, const double* omega,
+                           uint64_t seed, float* pos, float* vel, float* mass, float* density, void* stream);
+int gsph_ic_plummer(int64_t n, double a, double total_mass, double G, uint64_t seed, float* pos, float* vel,
+                    float* mass, void* stream);
+/* subtract the mass-weighted mean position and velocity (vel may be NULL); scratch: 7 * 256 device doubles */
+int gsph_ic_com_correct(int64_t n, float* pos, float* vel, const float* mass, double* scratch, void* stream);
+/* gsph_upload from device arrays in the host layout (e.g. the generators above) */
+int gsph_upload_device(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * batched ensemble: S independent simulations of uneven particle counts with one parameter set,
  * advanced by one persistent launch per substep. No counterpart in the reference, which runs one
  * simulation per process (src/main.cu:228-273); each simulation follows computeDerivatives /
