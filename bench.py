@@ -377,6 +377,49 @@ def ensemble_workload(nsims, seed=20261206):
     return config0_params(), sizes, states, desc
 
 
+def ensemble_drift(params, states, steps, every, stream):
+    """Energy of each simulation along `steps` steps run as an ensemble (FP32, the batched form) and one by
+    one in the double-precision form, from the same float32-representable states. Returns per simulation
+    max_t |E_ens(t) - E_fp64(t)| / |E_fp64(0)|, with the energy at the synchronous velocity after a
+    derivative refresh every `every` steps (as energy_drift)."""
+    from grasph2_b200.params import make_options
+    from grasph2_b200.sim import DeviceParticleBuffer, Ensemble, pack_states
+    from grasph2_b200.state import as_dtype
+    states = [as_dtype(as_dtype(s, np.float32), np.float64) for s in states]
+    sizes = [s["mass"].shape[0] for s in states]
+    dt = params.fixed_dt
+    e_ens = []
+    with Ensemble(params, sizes) as ens:
+        ens.upload(pack_states([as_dtype(s, np.float32) for s in states]), stream=stream)
+        done = 0
+        while True:
+            ens.compute_derivatives(stream)
+            e_ens.append([total_energy(d) for d in ens.diagnostics(0.5 * dt, stream)])
+            if done >= steps:
+                break
+            k = min(every, steps - done)
+            ens.step(k, stream)
+            done += k
+    e_ens = np.array(e_ens)
+    out = []
+    for j, st in enumerate(states):
+        e64 = []
+        with DeviceParticleBuffer(params, sizes[j], make_options(precision="double")) as pb:
+            pb.upload_f64(st, stream=stream)
+            done = 0
+            while True:
+                pb.compute_derivatives(stream)
+                e64.append(total_energy(pb.diagnostics(0.5 * dt, stream)))
+                if done >= steps:
+                    break
+                k = min(every, steps - done)
+                pb.step(k, stream)
+                done += k
+        e64 = np.array(e64)
+        out.append(float(np.abs(e_ens[:, j] - e64).max() / abs(e64[0])))
+    return out
+
+
 def run_ensemble(args, rank, world, local):
     """One step = every simulation of the ensemble advanced once (one persistent launch)."""
     import torch
@@ -493,10 +536,20 @@ def run_ensemble(args, rank, world, local):
         cpu = {"value": rate / scale, "unit": "steps/s", "cores": cores, "kind": kind,
                "sample": "the largest simulation (N=%d): %s; the ensemble step scaled by sum N_k^2 / N^2 = %.1f"
                          % (int(sizes[big]), sdesc, scale)}
+    drift = None
+    if args.drift_steps != 0:
+        nd = args.drift_steps if args.drift_steps > 0 else 1000
+        order = np.argsort(sizes)
+        pick = order[np.linspace(0, len(order) - 1, 8).astype(int)]
+        d = ensemble_drift(params, [states[k] for k in pick], nd, args.drift_every, stream)
+        drift = {"steps": nd, "simulations": [int(sizes[k]) for k in pick], "rel_drift_vs_fp64": d,
+                 "max_rel_drift_vs_fp64": max(d),
+                 "sample": "8 simulations spanning the size range, run as an ensemble (FP32) and one by one in FP64"}
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded initial conditions)",
+        "energy_drift": drift,
         "config": {"workload": desc, "nsims": int(len(sizes)), "n_total": n_total, "form": args.accum,
                    "l2": "flushed between timed steps (256 MiB write)",
                    "step": "every simulation: computeDerivatives + integrate, one persistent launch in a CUDA graph",
@@ -563,11 +616,11 @@ def run_surrogate(args, rank, world, local):
                 r = S.advance(pb, sur, args.windows, M=M, use_net=(form == "surrogate"))
             d = pb.diagnostics(0.0, fast=True)
             energies[form] = d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
-            errs = np.array(r.get("errors", [(np.nan, np.nan)]))
+            errs = np.array(r["errors"]) if r.get("errors") else None
             out[form] = {"sim_time_per_wall_s": substeps * dt / r["wall_s"], "substeps_per_s": substeps / r["wall_s"],
                          "accepted_windows": r["accepted"], "windows": r["windows"],
-                         "mean_position_error": float(np.nanmean(errs[:, 0])),
-                         "mean_energy_error": float(np.nanmean(errs[:, 1]))}
+                         "position_errors": None if errs is None else [float(x) for x in errs[:, 0]],
+                         "energy_errors": None if errs is None else [float(x) for x in errs[:, 1]]}
     clocks = sampler.stop()
     for form in out:
         out[form]["energy_vs_plain_at_end"] = abs(energies[form] - energies["plain"]) / abs(energies["plain"])

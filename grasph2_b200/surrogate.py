@@ -152,9 +152,9 @@ class Surrogate:
             apply(pb, self.K, None, None, None, stream)
 
 
-def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, stream=None):
+def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, stream=None):
     """Train a Surrogate on (X, Y) with the device kernels (forward + backward on the tensor cores, Adam);
-    returns (surrogate, loss history)."""
+    wout weights the 13 standardised outputs in the loss (default 1). Returns (surrogate, loss history)."""
     torch = _torch()
     from .mlp import init_params
     in_mu, in_sig = X.mean(0), X.std(0) + 1e-6
@@ -164,7 +164,7 @@ def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, stream=N
                     out_mu.astype(np.float32), out_sig.astype(np.float32))
     Xd = ((torch.from_numpy(X).cuda() - sur.dev["in_mu"]) / sur.dev["in_sig"]).contiguous()
     Yd = ((torch.from_numpy(Y).cuda() - sur.dev["out_mu"]) / sur.dev["out_sig"]).contiguous()
-    w = torch.ones(NO, dtype=torch.float32, device="cuda")
+    w = torch.from_numpy(np.asarray(wout if wout is not None else np.ones(NO), dtype=np.float32)).cuda()
     g = torch.Generator(device="cuda").manual_seed(seed)
     m = X.shape[0]
     hist = []

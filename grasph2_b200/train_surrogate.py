@@ -1,6 +1,6 @@
 """Train the learned surrogate of the impact workload on trajectories of the plain solver.
 
-    python -m grasph2_b200.train_surrogate [--n 262144] [--trajectories 200] [--windows 16] [--every 2]
+    python -m grasph2_b200.train_surrogate [--n 262144] [--trajectories 200] [--windows 32] [--every 4]
                                            [--rows 8192] [--steps 6000] [--out grasph2_b200/data/...npz]
 
 Each trajectory is a two-sphere impact (radii 1 and 0.5, equal number density, N split 8:1) with a
@@ -27,8 +27,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--trajectories", type=int, default=200)
-    ap.add_argument("--windows", type=int, default=16)
-    ap.add_argument("--every", type=int, default=2)
+    ap.add_argument("--windows", type=int, default=32)
+    ap.add_argument("--every", type=int, default=4)
     ap.add_argument("--rows", type=int, default=8192)
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=65536)
