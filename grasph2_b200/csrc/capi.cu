@@ -506,6 +506,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     a.dt_state = static_cast<float*>(dalloc(c, 4 * sizeof(float), ae));
     a.diag = static_cast<double*>(dalloc(c, diag_scratch_doubles(n) * sizeof(double), ae));
     a.status = static_cast<int*>(dalloc(c, sizeof(int) * 4, ae));
+    a.grav = static_cast<float4*>(dalloc(c, n_pad * sizeof(float4), ae));
     if (c->fp64) {
         DevArrays64& b = c->a64;
         b.n = n;
@@ -1099,6 +1100,34 @@ int gsph_launch_shape_get(gsph_ctx* c, gsph_launch_shape* out) {
     out->sph_jt = c->L.jt;
     out->sph_nseg = c->L.nseg;
     out->items = c->L.cull ? c->sp.item_target : 0;
+    return GSPH_OK;
+}
+
+int gsph_state_compare(gsph_ctx* c, int32_t slot_p, int32_t slot_0, double* out, void* stream) {
+    if (!c || !out) return c ? fail(c, GSPH_E_INVALID, "out is NULL") : GSPH_E_INVALID;
+    if (c->fp64) return fail(c, GSPH_E_UNSUPPORTED, "single precision only");
+    if (slot_p < 0 || slot_p >= kSnapSlots || slot_0 < 0 || slot_0 >= kSnapSlots || c->snap[slot_p].empty() ||
+        c->snap[slot_0].empty())
+        return fail(c, GSPH_E_STATE, "both snapshot slots must hold a saved state");
+    auto view = [&](int slot) {  // the saved arrays, in gsph_snapshot's order
+        DevArrays v = c->a;
+        const std::vector<void*>& sn = c->snap[slot];
+        v.posm = static_cast<float4*>(sn[0]);
+        v.velrho = static_cast<float4*>(sn[1]);
+        v.acc = static_cast<float4*>(sn[2]);
+        v.sA = static_cast<float4*>(sn[4]);
+        v.sB = static_cast<float4*>(sn[5]);
+        v.pos64 = static_cast<double*>(sn[10]);
+        return v;
+    };
+    cudaStream_t s = as_stream(stream);
+    GSPH_CK(c, launch_state_compare(c->a, view(slot_p), view(slot_0), c->dp, c->a.diag, c->diag_out, s), "compare");
+    c->launches += 2;
+    double h[4];
+    GSPH_CK(c, cudaMemcpyAsync(h, c->diag_out, sizeof h, cudaMemcpyDeviceToHost, s), "compare read");
+    const int rc = check_status(c, s);
+    if (rc != GSPH_OK) return rc;
+    for (int k = 0; k < 4; ++k) out[k] = h[k];
     return GSPH_OK;
 }
 

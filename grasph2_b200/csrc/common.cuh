@@ -60,6 +60,7 @@ struct DevArrays {
     float* part;      // j-split partial sums [segment][component][n_pad]
     float* gpart;     // gravity partial sums of the culled path [segment][component][n_pad]
     float* dt_state;  // variable step: [0] current, [1] next (float bit patterns, positive)
+    float4* grav;     // gravitational acceleration of the last derivative evaluation (nullable)
     double* diag;     // diagnostics scratch
     int* status;      // device status word (0 = ok)
 };

@@ -180,6 +180,44 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_fast(DevArrays a, DevPara
     }
 }
 
+// Comparison of the current state Q with a saved state P (and a saved start state X0), O(N):
+//   0: E_local(P) - E_local(Q) - sum_i m_i g_i . (x_P,i - x_Q,i)    (kinetic + internal + shear energy
+//      exactly, the gravitational energy change to first order in the position difference, g = the
+//      gravitational acceleration of Q's last derivative evaluation)
+//   1: sum_i |x_P,i - x_Q,i|^2      2: sum_i |x_Q,i - x_0,i|^2      3: E_local(Q)
+__global__ void __launch_bounds__(kDiagThreads) k_state_compare(DevArrays q, DevArrays pv, DevArrays x0, DevParams p) {
+    __shared__ double red[32];
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double f[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i < q.n) {
+        double fq[kDiagFields], fp[kDiagFields];
+#pragma unroll
+        for (int k = 0; k < kDiagFields; ++k) fq[k] = fp[k] = 0.0;
+        diag_terms(q, p, i, 0.0, fq);
+        diag_terms(pv, p, i, 0.0, fp);
+        const double eq = fq[0] + fq[2] + fq[3], ep = fp[0] + fp[2] + fp[3];
+        const int64_t np = q.n_pad;
+        double dg = 0.0, dx2 = 0.0, d02 = 0.0;
+        const float4 g = q.grav ? q.grav[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float gc[3] = {g.x, g.y, g.z};
+        for (int c = 0; c < 3; ++c) {
+            const double xq = q.pos64[c * np + i], xp = pv.pos64[c * np + i], xs = x0.pos64[c * np + i];
+            dg += static_cast<double>(gc[c]) * (xp - xq);
+            dx2 += (xp - xq) * (xp - xq);
+            d02 += (xq - xs) * (xq - xs);
+        }
+        f[0] = ep - eq - static_cast<double>(q.posm[i].w) * dg;
+        f[1] = dx2;
+        f[2] = d02;
+        f[3] = eq;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double sum = block_sum(f[k], red);
+        if (threadIdx.x == 0) q.diag[static_cast<int64_t>(blockIdx.x) * kDiagFields + k] = sum;
+    }
+}
+
 __global__ void k_diag_reduce(DevArrays a, int nblocks, double* out) {
     const int k = threadIdx.x;
     if (k >= kDiagFields) return;
@@ -344,6 +382,18 @@ cudaError_t launch_diagnostics_fast(const DevArrays& a, const DevParams& p, doub
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_diag_reduce<<<1, 32, 0, s>>>(a, static_cast<int>(nb), out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_state_compare(const DevArrays& q, const DevArrays& p_state, const DevArrays& x0, const DevParams& p,
+                                 double* scratch, double* out_dev, cudaStream_t s) {
+    const unsigned nb = blocks_for(q.n, kDiagThreads);
+    DevArrays qq = q;
+    qq.diag = scratch;
+    k_state_compare<<<nb, kDiagThreads, 0, s>>>(qq, p_state, x0, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_diag_reduce<<<1, 32, 0, s>>>(qq, static_cast<int>(nb), out_dev);
     return cudaGetLastError();
 }
 

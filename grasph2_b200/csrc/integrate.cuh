@@ -13,6 +13,9 @@ cudaError_t launch_diagnostics(const DevArrays& a, const DevParams& p, double ha
 // the same with the pair potential summed in FP32 (compensated across tiles, FP64 across particles)
 cudaError_t launch_diagnostics_fast(const DevArrays& a, const DevParams& p, double half_kick, double* out_dev,
                                     cudaStream_t s);
+// O(N) comparison of the current state with two saved states (gsph_state_compare); out_dev: 4 doubles
+cudaError_t launch_state_compare(const DevArrays& q, const DevArrays& p_state, const DevArrays& x0, const DevParams& p,
+                                 double* scratch, double* out_dev, cudaStream_t s);
 // `ext` (nullable) maps each device slot to the caller's particle index
 cudaError_t launch_pack(const DevArrays& a, int attr, const float* src_dev, const int* ext, cudaStream_t s);
 cudaError_t launch_unpack(const DevArrays& a, int attr, float* dst_dev, const int* ext, cudaStream_t s);

@@ -626,6 +626,7 @@ __global__ void k_gravity_finish(DevArrays a, DevParams p, int nseg) {
             acc[c] = p.G * s;
         }
     }
+    if (a.grav) a.grav[i] = make_float4(acc[0], acc[1], acc[2], 0.0f);
     environment(p, a.posm[i], a.velrho[i], acc[0], acc[1], acc[2]);
     a.acc[i] = make_float4(acc[0], acc[1], acc[2], 0.0f);
     a.xvel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);

@@ -241,6 +241,7 @@ __device__ __forceinline__ void sph_finish(const DevArrays& a, const DevParams& 
             ax = fmaf(p.G, g[0], ax);
             ay = fmaf(p.G, g[1], ay);
             az = fmaf(p.G, g[2], az);
+            if (a.grav) a.grav[i] = make_float4(p.G * g[0], p.G * g[1], p.G * g[2], 0.0f);
         }
         const float4 x = a.posm[i];
         environment(p, x, vi, ax, ay, az);

@@ -180,20 +180,28 @@ def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=Non
     return sur, hist
 
 
-def window_errors(pb, sur, use_net=True, stream=None):
+def compare(pb, slot_p, slot_0, stream=None):
+    """gsph_state_compare: (E(P) - E(Q), sum |x_P - x_Q|^2, sum |x_Q - x_0|^2, local energy of Q)."""
+    out = (ctypes.c_double * 4)()
+    pb._check(pb.lib.gsph_state_compare(pb.handle, int(slot_p), int(slot_0), out, _stream_handle(stream)))
+    return tuple(out)
+
+
+def window_errors(pb, sur, use_net=True, e_ref=None, stream=None):
     """One proposal and the plain K steps from the same state; returns (position error, relative energy
     error). The position error is norm-wise over all particles, relative to the plain displacement:
-    ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2. The context ends on the plain result."""
+    ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2; the energy error is |E_proposal - E_plain| / |E|
+    (gsph_state_compare, O(N) on the device; E from the fast diagnostics unless e_ref is given). The
+    context ends on the plain result."""
+    if e_ref is None:
+        e_ref = _energy(pb.diagnostics(0.0, stream, fast=True))
     snapshot(pb, 1, False, stream)
-    x0 = pb.download_pos64()
     sur.propose(pb, use_net, stream)
-    xp = pb.download_pos64()
-    ep = _energy(pb.diagnostics(0.0, stream, fast=True))
+    snapshot(pb, 2, False, stream)
     snapshot(pb, 1, True, stream)
     pb.step(sur.K, stream)
-    xq = pb.download_pos64()
-    eq = _energy(pb.diagnostics(0.0, stream, fast=True))
-    return float(np.linalg.norm(xp - xq) / np.linalg.norm(xq - x0)), float(abs(ep - eq) / abs(eq))
+    de, dx2, d02, _ = compare(pb, 2, 1, stream)
+    return float(math.sqrt(dx2 / d02)) if d02 > 0 else float("inf"), float(abs(de) / abs(e_ref))
 
 
 def _energy(d):
@@ -206,12 +214,13 @@ def advance(pb, sur, nwin, M=4, pos_tol=1e-3, e_tol=1e-4, use_net=True, stream=N
     torch = _torch()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    e_ref = _energy(pb.diagnostics(0.0, stream, fast=True))  # the scale of the energy criterion
     acc, errs = 0, []
     for _ in range(nwin):
         snapshot(pb, 0, False, stream)
         for _ in range(M - 1):
             sur.propose(pb, use_net, stream)
-        ex, ee = window_errors(pb, sur, use_net, stream)
+        ex, ee = window_errors(pb, sur, use_net, e_ref, stream)
         errs.append((ex, ee))
         if ex <= pos_tol and ee <= e_tol:
             acc += 1

@@ -336,6 +336,12 @@ int gsph_surrogate_features(gsph_ctx* ctx, const float* mu, const float* sigma, 
 int gsph_surrogate_apply(gsph_ctx* ctx, const float* delta, const float* out_mu, const float* out_sigma, int32_t K,
                          void* stream);
 int gsph_snapshot(gsph_ctx* ctx, int32_t slot, int32_t restore, void* stream);
+/* O(N) comparison of the current state Q with the states saved in slot_p (P) and slot_0 (X0), for the
+ * surrogate's judge (synchronises `stream`): out[0] = E(P) - E(Q), with the kinetic, internal and shear
+ * energies exact and the gravitational energy to first order in x_P - x_Q (-sum m g . dx, g the
+ * gravitational acceleration of Q's last derivative evaluation); out[1] = sum |x_P - x_Q|^2;
+ * out[2] = sum |x_Q - x_0|^2; out[3] = E_kin + E_int + E_shear of Q. */
+int gsph_state_compare(gsph_ctx* ctx, int32_t slot_p, int32_t slot_0, double* out, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
  * initial conditions on the device (the reference's particle sources, src/initialConditions/

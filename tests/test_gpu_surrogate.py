@@ -187,3 +187,29 @@ def test_advance_rejects_back_to_the_plain_path():
     assert r["accepted"] == 0 and r["substeps"] == 48
     for k in x:
         np.testing.assert_array_equal(x[k], y[k], err_msg=k)
+
+
+def test_state_compare_matches_full_energies():
+    """The judge's O(N) comparison against full diagnostics of both states and host position norms."""
+    nb, ns = 7282, 910
+    p = impact_params(nb, ns)
+    st = ics.two_sphere_impact(nb, ns, v_rel=0.6, y_offset=0.4, seed=31)
+    sur = S.Surrogate(8)
+    with DeviceParticleBuffer(p, nb + ns) as pb:
+        pb.upload(st)
+        pb.step(5)
+        S.snapshot(pb, 1, False)
+        x0 = pb.download_pos64()
+        sur.propose(pb, use_net=False)
+        S.snapshot(pb, 2, False)
+        xp = pb.download_pos64()
+        ep = S._energy(pb.diagnostics(0.0))
+        S.snapshot(pb, 1, True)
+        pb.step(8)
+        xq = pb.download_pos64()
+        eq = S._energy(pb.diagnostics(0.0))
+        de, dx2, d02, _ = S.compare(pb, 2, 1)
+    np.testing.assert_allclose(dx2, ((xp - xq) ** 2).sum(), rtol=1e-9)
+    np.testing.assert_allclose(d02, ((xq - x0) ** 2).sum(), rtol=1e-9)
+    # first-order gravitational energy change: agrees to a small fraction of the difference itself
+    assert abs(de - (ep - eq)) <= 0.05 * abs(ep - eq) + 1e-9 * abs(eq), (de, ep - eq)
