@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["impact", "fluid", "plummer", "ensemble", "surrogate"], default="impact")
+    ap.add_argument("--workload", choices=["impact", "fluid", "plummer", "ensemble", "surrogate", "mlp"],
+                    default="impact")
     ap.add_argument("--windows", type=int, default=8, help="surrogate: windows of M proposals")
     ap.add_argument("--model", default=os.path.join(ROOT, "grasph2_b200", "data", "surrogate_impact_n262144.npz"),
                     help="surrogate: trained model (grasph2_b200/train_surrogate.py)")
@@ -640,6 +641,57 @@ def run_surrogate(args, rank, world, local):
     print(json.dumps(line))
 
 
+MLP_FWD_FLOPS = 2 * (32 * 128 + 2 * 128 * 128 + 128 * 13)                  # per row
+MLP_TRAIN_FLOPS = MLP_FWD_FLOPS + 2 * (32 * 128 + 2 * 128 * 128 + 128 * 13) + 2 * (2 * 128 * 128 + 13 * 128)
+
+
+def run_mlp(args, rank, world, local):
+    """The surrogate's MLP on the tensor cores: forward over 1,048,576 rows and the gradient over 262,144
+    rows per step (random inputs), TFLOP/s against the measured bf16 GEMM peak."""
+    import torch
+    torch.cuda.set_device(local)
+    from grasph2_b200.mlp import MLP, init_params
+    if rank != 0:
+        return
+    nf, nt = 1 << 20, 1 << 18
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(nf, 32, device="cuda", generator=g)
+    y = torch.empty(nf, 13, device="cuda")
+    t = torch.randn(nt, 13, device="cuda", generator=g)
+    w = torch.ones(13, device="cuda")
+    stream = torch.cuda.current_stream()
+    net = MLP(init_params(0))
+    res = {}
+    for name, f, rows, flops in (("forward", lambda: net.forward(x, y, nf, stream), nf, MLP_FWD_FLOPS),
+                                 ("gradient", lambda: net.gradient(x, t, w, nt, stream, want=False), nt,
+                                  MLP_TRAIN_FLOPS)):
+        for _ in range(max(args.warmup, 1)):
+            f()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for a, b in ev:
+            a.record(stream)
+            f()
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = sorted(a.elapsed_time(b) for a, b in ev)[len(ev) // 2]
+        res[name] = {"rows": rows, "ms": ms, "rows_per_s": rows / (ms * 1e-3), "tflops": rows * flops / (ms * 1e-3) / 1e12}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
+    peak = peaks["bf16_tflops"]
+    line = {"metric": "MLP rows/s (forward) on the tensor cores", "value": res["forward"]["rows_per_s"], "unit": "rows/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["forward"]["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (random inputs)",
+            "config": {"workload": "surrogate MLP 32-128-128-128-13 SiLU, BF16 operands, FP32 accumulation in TMEM",
+                       "forward_rows": nf, "gradient_rows": nt},
+            "kernels": res,
+            "roofline": {"bound": "tensor", "kernel": "k_mlp_forward", "achieved": res["forward"]["tflops"], "peak": peak,
+                         "unit": "TFLOP/s", "frac": res["forward"]["tflops"] / peak, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"},
+            "gpu_launches": args.steps * 3}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -654,6 +706,9 @@ def main():
         return
     if args.workload == "surrogate":
         run_surrogate(args, rank, world, local)
+        return
+    if args.workload == "mlp":
+        run_mlp(args, rank, world, local)
         return
     import torch
     torch.cuda.set_device(local)
