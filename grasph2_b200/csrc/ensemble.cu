@@ -179,11 +179,32 @@ struct RangePipe {
     }
 };
 
+// Bounding box of the block's points (each thread passes its own min and max): box[0..2] = lo,
+// box[3..5] = hi, in shared memory and visible to every thread on return. scratch: 6 x warps floats.
+__device__ __forceinline__ void block_box(float lx, float ly, float lz, float hx, float hy, float hz, float* scratch,
+                                          float* box) {
+    float v[6] = {lx, ly, lz, -hx, -hy, -hz};  // all minima
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[d] = fminf(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
+        if (lane == 0) scratch[warp * 6 + d] = v[d];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        float m = INFINITY;
+        for (int w = 0; w < kEnsThreads / 32; ++w) m = fminf(m, scratch[w * 6 + threadIdx.x]);
+        box[threadIdx.x] = threadIdx.x < 3 ? m : -m;
+    }
+    __syncthreads();
+}
+
 // ---- DENS: gravity + density + neighbour lists over the group's simulation -------------------------
 // GRAV: 0 off, 1 softened, 2 unsoftened (the self pair gives 0 through the clamp of 1/r).
 template <int GRAV, bool SPH, bool COMP>
 __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p, const EnsView& v, RangePipe& pipe,
-                                          int4 grp, int4 sm) {
+                                          int4 grp, int4 sm, float* sbox) {
     constexpr int P = kEnsIpt / 2;
     const int64_t g0 = grp.y;
     int64_t idx[kEnsIpt];
@@ -209,8 +230,41 @@ __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p
     const uint32_t span = __float_as_uint(p.H2);
     const float H2 = p.H2;
     const float inv_h = p.inv_h;
+    float* scratch = sbox;
+    float* gbox = sbox + 6 * (kEnsThreads / 32);
+    float* tbox = gbox + 6;
+    const float H2m = H2 * (1.0f + 1e-3f);  // conservative: a tile farther than this has no neighbour in any rounding
+    if (SPH) {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            lo[0] = fminf(lo[0], fminf(X[k].x, X[k].y)); hi[0] = fmaxf(hi[0], fmaxf(X[k].x, X[k].y));
+            lo[1] = fminf(lo[1], fminf(Y[k].x, Y[k].y)); hi[1] = fmaxf(hi[1], fmaxf(Y[k].x, Y[k].y));
+            lo[2] = fminf(lo[2], fminf(Z[k].x, Z[k].y)); hi[2] = fmaxf(hi[2], fmaxf(Z[k].x, Z[k].y));
+        }
+        block_box(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], scratch, gbox);
+    }
 
     const bool ok = pipe.run(sm.x, static_cast<int64_t>(sm.x) + sm.y, [&](const float4* J, int nj, int64_t jb) {
+        // is any j of this tile within h of the group's box? (else the neighbour tests are skipped)
+        bool near_tile = false;
+        if (SPH) {
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (int t = threadIdx.x; t < nj; t += kEnsThreads) {
+                const float4 q = J[t];
+                lo[0] = fminf(lo[0], q.x); hi[0] = fmaxf(hi[0], q.x);
+                lo[1] = fminf(lo[1], q.y); hi[1] = fmaxf(hi[1], q.y);
+                lo[2] = fminf(lo[2], q.z); hi[2] = fmaxf(hi[2], q.z);
+            }
+            block_box(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], scratch, tbox);
+            float d2 = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float d = fmaxf(0.0f, fmaxf(gbox[c] - tbox[3 + c], tbox[c] - gbox[3 + c]));
+                d2 = fmaf(d, d, d2);
+            }
+            near_tile = d2 <= H2m;
+        }
         float2 TX[P], TY[P], TZ[P];
         float tr[kEnsIpt];
 #pragma unroll
@@ -240,7 +294,7 @@ __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p
                     }
                 }
             }
-            if (SPH) {
+            if (SPH && near_tile) {
                 // one warp vote per j: particles of a group are close along the curve, so for most j no
                 // lane has a neighbour and the per-particle window tests are skipped
                 bool near = false;
@@ -370,6 +424,7 @@ template <int GRAV, bool SPH, int PASS, bool SOLIDS, bool COMP>
 __global__ void __launch_bounds__(kEnsThreads) k_ensemble(DevArrays a, DevParams p, EnsView v) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item, s_flag;
+    __shared__ float s_box[6 * (kEnsThreads / 32) + 12];  // reduction scratch, group box, tile box
     RangePipe pipe;
     pipe.buf = reinterpret_cast<float4*>(smem_raw);
     pipe.tile = v.tile;
@@ -390,7 +445,7 @@ __global__ void __launch_bounds__(kEnsThreads) k_ensemble(DevArrays a, DevParams
         const int sim = grp.x;
         const int4 sm = v.sims[sim];
         if (stage == ST_DENS) {
-            if (!dens_item<GRAV, SPH, COMP>(a, p, v, pipe, grp, sm)) return;
+            if (!dens_item<GRAV, SPH, COMP>(a, p, v, pipe, grp, sm, s_box)) return;
             signal_done(v.done + sim);
         } else if (stage == ST_SPH) {
             if (!wait_count(v.done + sim, sm.w, a.status, &s_flag)) return;
