@@ -43,6 +43,7 @@ FLOP_FUSED_NB = 160        # strain/rotation rates, div v, stress acceleration, 
 FLOP_ACC_NB = 60           # pressure acceleration + AV per neighbour (fluid, acceleration pass only)
 
 FLUSH_BYTES = 256 << 20
+FLAG_DEAL_WITH_NO_PARTNERS = 1 << 3  # GSPH_DEAL_WITH_NO_PARTNERS
 
 
 def parse():
@@ -371,11 +372,17 @@ def ensemble_workload(nsims, seed=20261206):
     from grasph2_b200.params import config0_params
     sizes = ics.ensemble_sizes(nsims, seed=seed)
     rng = np.random.default_rng(seed + 1)
+    params = config0_params()
+    # h = 0.15 is fixed while N_k goes down to 1024: the smallest spheres have a mean spacing (0.16)
+    # above h, so a particle can have no neighbour and a zero summed density. The reference's own
+    # DEAL_WITH_NO_PARTNERS floor (rho < 0.001 -> 0.01 rho0, computeDerivatives.h:85-88) keeps them finite.
+    params.flags |= FLAG_DEAL_WITH_NO_PARTNERS
     states = [ics.uniform_sphere(int(n), radius=1.0, rho0=0.239, omega=(0.0, 0.0, rng.uniform(0.0, 0.5)),
                                  seed=seed + 2 + k) for k, n in enumerate(sizes)]
     desc = ("batched ensemble of %d self-gravitating SPH spheres, N_k log-uniform in [1024, 32768] (total %d), "
-            "radius 1, omega ~ U[0,0.5], h=0.15, eps=0.02, c_s=1, rho0=0.239, dt=1e-3" % (nsims, int(sizes.sum())))
-    return config0_params(), sizes, states, desc
+            "radius 1, omega ~ U[0,0.5], h=0.15, eps=0.02, c_s=1, rho0=0.239, dt=1e-3, density floor "
+            "DEAL_WITH_NO_PARTNERS" % (nsims, int(sizes.sum())))
+    return params, sizes, states, desc
 
 
 def ensemble_drift(params, states, steps, every, stream):
@@ -608,6 +615,7 @@ def run_surrogate(args, rank, world, local):
             pb.upload(st)
             pb.step(max(args.warmup, 1))
             torch.cuda.synchronize()
+            l0 = pb.launch_count()
             t0 = time.perf_counter()
             if form == "plain":
                 pb.step(substeps)
@@ -615,11 +623,13 @@ def run_surrogate(args, rank, world, local):
                 r = {"wall_s": time.perf_counter() - t0, "accepted": None, "windows": args.windows}
             else:
                 r = S.advance(pb, sur, args.windows, M=M, use_net=(form == "surrogate"))
+            launches = pb.launch_count() - l0
             d = pb.diagnostics(0.0, fast=True)
             energies[form] = d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
             errs = np.array(r["errors"]) if r.get("errors") else None
             out[form] = {"sim_time_per_wall_s": substeps * dt / r["wall_s"], "substeps_per_s": substeps / r["wall_s"],
                          "accepted_windows": r["accepted"], "windows": r["windows"],
+                         "library_launches": launches,
                          "position_errors": None if errs is None else [float(x) for x in errs[:, 0]],
                          "energy_errors": None if errs is None else [float(x) for x in errs[:, 1]]}
     clocks = sampler.stop()
@@ -636,7 +646,7 @@ def run_surrogate(args, rank, world, local):
         "forms": out,
         "speedup_vs_plain": value / out["plain"]["substeps_per_s"],
         "clocks": clocks,
-        "gpu_launches": None,
+        "gpu_launches": out["surrogate"]["library_launches"],
     }
     print(json.dumps(line))
 
