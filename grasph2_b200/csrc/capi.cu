@@ -40,6 +40,7 @@ struct gsph_ctx {
     double* staging64 = nullptr;  // 9 * n doubles
     double* diag_out = nullptr;   // device, 12 doubles
     size_t part_cap = 0, gpart_cap = 0, item_cap = 0;  // floats allocated for a.part, a.gpart, sp.item_part
+    size_t item_nb_items = 0;                          // work items the neighbour-list buffers hold
     std::vector<void*> snap[4];    // gsph_snapshot slots: saved copies of the state arrays (allocated on first save)
     cudaStream_t capture_stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -264,15 +265,16 @@ int derivatives(gsph_ctx* c, cudaStream_t s) {
         }
         const bool vgrad = has(p, GSPH_SOLIDS) || has(p, GSPH_INTEGRATE_DENSITY) || has(p, GSPH_BALSARA_SWITCH);
         const int gnseg = grav_kernel ? c->L.grav_nseg : 0;
+        const bool lists = sp && !has(p, GSPH_INTEGRATE_DENSITY);  // the density pass stored neighbour lists
         if (vgrad && has(p, GSPH_BALSARA_SWITCH)) {
-            e = launch_pairs(PASS_VGRAD, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_VGRAD), sp);
+            e = launch_pairs(PASS_VGRAD, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_VGRAD), sp, 0, nullptr, lists);
             if (e != cudaSuccess) return cuda_fail(c, e, "velocity-gradient pass");
-            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, gnseg, join);
+            e = launch_pairs(PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, gnseg, join, lists);
             if (e != cudaSuccess) return cuda_fail(c, e, "acceleration pass");
             c->launches += 4;
         } else {
             e = launch_pairs(vgrad ? PASS_FUSED : PASS_ACC, c->a, p, c->L, s, slot_timer(c, GSPH_KSLOT_PAIRS), sp, gnseg,
-                             join);
+                             join, lists);
             if (e != cudaSuccess) return cuda_fail(c, e, "pair pass");
             c->launches += 2;
         }
@@ -489,6 +491,9 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         const size_t cap = static_cast<size_t>(sp.item_target) + static_cast<size_t>(ngroups);
         c->item_cap = cap * kk * kGroup;
         sp.item_part = static_cast<float*>(dalloc(c, c->item_cap * sizeof(float), ae));
+        c->item_nb_items = cap;
+        sp.item_nb = static_cast<int*>(dalloc(c, cap * kItemNb * kGroup * sizeof(int), ae));
+        sp.item_nbcnt = static_cast<int*>(dalloc(c, cap * kGroup * sizeof(int), ae));
         sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));
@@ -982,7 +987,7 @@ int gsph_autotune(gsph_ctx* c, int32_t reps, void* stream) {
         Launch best = L;
         float best_ms = 1e30f;
         const int ipts[3] = {2, 4, 8};
-        const int jts[2] = {128, 256};
+        const int jts[3] = {128, 256, 512};
         for (int ip : ipts)
             for (int jt : jts) {
                 if (np % (int64_t(L.grav_threads) * ip) || np % jt) continue;
@@ -1053,8 +1058,15 @@ int gsph_autotune(gsph_ctx* c, int32_t reps, void* stream) {
             const int target_mult = t.nseg < 0 ? -t.nseg : 0;
             if (target_mult) {
                 t.nseg = L.nseg;
-                rc = grow(c, &c->sp.item_part, c->item_cap,
-                          (static_cast<size_t>(target_mult) * L.item_grid + ngroups) * kk * kGroup);
+                const size_t items = static_cast<size_t>(target_mult) * L.item_grid + ngroups;
+                rc = grow(c, &c->sp.item_part, c->item_cap, items * kk * kGroup);
+                if (rc == GSPH_OK && items > c->item_nb_items) {
+                    size_t cap_nb = c->item_nb_items * kItemNb * kGroup, cap_cnt = c->item_nb_items * kGroup;
+                    rc = grow(c, reinterpret_cast<float**>(&c->sp.item_nb), cap_nb, items * kItemNb * kGroup);
+                    if (rc == GSPH_OK)
+                        rc = grow(c, reinterpret_cast<float**>(&c->sp.item_nbcnt), cap_cnt, items * kGroup);
+                    if (rc == GSPH_OK) c->item_nb_items = items;
+                }
                 if (rc != GSPH_OK) break;
                 c->sp.item_target = target_mult * L.item_grid;
             } else {

@@ -94,8 +94,9 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm
     if (COMP) part[(seg * 2 + 1) * n_pad + i] = rho_c;
 }
 
-// culled density sum over the near-chunk work items (persistent grid)
-template <bool COMP>
+// culled density sum over the near-chunk work items (persistent grid); with LISTS every lane also
+// records the indices of its neighbours in this item (for the SPH passes of the same step)
+template <bool COMP, bool LISTS>
 __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restrict__ posm, DevParams p, CullView cv,
                                                           int* status) {
     constexpr int SJ = kStageChunks * kChunk;
@@ -113,8 +114,33 @@ __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restri
         cv.item(w, g, c0, c1);
         const float4 pi = posm[static_cast<int64_t>(g) * kGroup + threadIdx.x];
         float rho_s = 0.0f, rho_c = 0.0f;
-        if (!pipe.run(cv.list + static_cast<int64_t>(g) * cv.nchunks + c0, c1 - c0, [&](const float4* J, int nj) {
-                const float t = density_tile(J, nj, pi, span, p.inv_h);
+        int cnt = 0;
+        int* lst = LISTS ? cv.nb + static_cast<int64_t>(w) * kItemNb * kGroup + threadIdx.x : nullptr;
+        const int* chunks = cv.list + static_cast<int64_t>(g) * cv.nchunks + c0;
+        int chunk_base = 0;
+        if (!pipe.run(chunks, c1 - c0, [&](const float4* J, int nj) {
+                float t;
+                if (LISTS) {  // the density_tile loop, recording the neighbours as well (same order)
+                    t = 0.0f;
+                    for (int s0 = 0; s0 < nj; s0 += kChunk) {
+                        const int jb = chunks[chunk_base + s0 / kChunk] * kChunk;
+#pragma unroll 8
+                        for (int j = 0; j < kChunk; ++j) {
+                            const float4 q = J[s0 + j];
+                            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+                            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            if (in_open_closed(r2, 0u, span)) {
+                                const float r = r2 * rsqrtf(r2);
+                                t = fmaf(q.w, w_poly(r * p.inv_h), t);
+                                if (cnt < kItemNb) lst[cnt * kGroup] = jb + j;
+                                ++cnt;
+                            }
+                        }
+                    }
+                    chunk_base += nj / kChunk;
+                } else {
+                    t = density_tile(J, nj, pi, span, p.inv_h);
+                }
                 if (COMP) fold(rho_s, rho_c, t);
                 else rho_s += t;
             }))
@@ -122,6 +148,7 @@ __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restri
         float* out = cv.part + static_cast<int64_t>(w) * (COMP ? 2 : 1) * kGroup + threadIdx.x;
         out[0] = rho_s;
         if (COMP) out[kGroup] = rho_c;
+        if (LISTS) cv.nbcnt[static_cast<int64_t>(w) * kGroup + threadIdx.x] = min(cnt, kItemNb + 1);
     }
 }
 
@@ -291,6 +318,34 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
 #pragma unroll
         for (int f = 0; f < F_COUNT; ++f) S.f[f] = C.f[f] = T.f[f] = 0.0f;
         float maxv = 0.0f;
+        // the density pass's neighbour lists of this item, when every lane's list is complete
+        int lcnt = cv.nb ? cv.nbcnt[static_cast<int64_t>(w) * kGroup + threadIdx.x] : kItemNb + 1;
+        if (!__syncthreads_or(lcnt > kItemNb)) {
+            const int* lst = cv.nb + static_cast<int64_t>(w) * kItemNb * kGroup + threadIdx.x;
+            const float4 zero = make_float4(0, 0, 0, 0);
+            int jn = lcnt > 0 ? lst[0] : 0;
+            float4 qn = a.posm[jn], vn = a.velrho[jn];
+            float4 an = DO_A ? a.jA[jn] : zero, bn = DO_A ? a.jB[jn] : zero;
+            for (int k = 0; k < lcnt; ++k) {  // software pipeline: neighbour k+1's records in flight
+                const float4 q = qn, vj = vn, ja = an, jb = bn;
+                if (k + 1 < lcnt) {
+                    jn = lst[(k + 1) * kGroup];
+                    qn = a.posm[jn];
+                    vn = a.velrho[jn];
+                    if (DO_A) {
+                        an = a.jA[jn];
+                        bn = a.jB[jn];
+                    }
+                }
+                const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, vj, ja, jb, p);
+            }
+            fold_tile<MASK, COMP>(S, C, T);
+            store_partials<MASK, COMP>(cv.part + static_cast<int64_t>(w) * (COMP ? 2 * K : K) * kGroup + threadIdx.x,
+                                       kGroup, S, C, maxv);
+            continue;
+        }
         int cnt = 0;
         // phase 2 over the lane lists collected so far
         auto drain = [&]() {
@@ -663,6 +718,8 @@ CullView cull_view(const DevArrays& a, const SpatialArrays& sp) {
     cv.ngroups = static_cast<int>(a.n_pad / kGroup);
     cv.nchunks = a.n_pad / kChunk;
     cv.part = sp.item_part;
+    cv.nb = nullptr;
+    cv.nbcnt = nullptr;
     return cv;
 }
 PartView seg_view(const DevArrays& a, int nseg, int KK) { return PartView{a.part, a.n_pad, nseg, nullptr, KK}; }
@@ -741,8 +798,11 @@ cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch&
     if (sp) {
         const size_t smem = pipe_smem_bytes(1, kStageChunks * kChunk);
         const CullView cv = cull_view(a, *sp);
-        if (comp) k_density_items<true><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
-        else k_density_items<false><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cv, a.status);
+        CullView cvl = cv;
+        cvl.nb = sp->item_nb;
+        cvl.nbcnt = sp->item_nbcnt;
+        if (comp) k_density_items<true, true><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cvl, a.status);
+        else k_density_items<false, true><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cvl, a.status);
     } else {
         const int T = 256;
         const dim3 grid(static_cast<unsigned>(a.n_pad / T), static_cast<unsigned>(L.nseg));
@@ -768,7 +828,7 @@ cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t 
 namespace {
 template <int PASS, int GRAV, bool SOLIDS, bool COMP>
 cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
-                    const SpatialArrays* sp, int gnseg, cudaEvent_t join) {
+                    const SpatialArrays* sp, int gnseg, cudaEvent_t join, bool lists) {
     constexpr int NS = (PASS == PASS_VGRAD) ? 2 : 4;
     if (sp) {  // SPH terms over the near-chunk work items; gravity partials come from elsewhere
         constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
@@ -781,7 +841,12 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
             if (e != cudaSuccess) return e;
         }
         GSPH_TIMER_MARK(t, start);
-        k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cull_view(a, *sp));
+        CullView cv = cull_view(a, *sp);
+        if (lists) {
+            cv.nb = sp->item_nb;
+            cv.nbcnt = sp->item_nbcnt;
+        }
+        k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cv);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         GSPH_TIMER_MARK(t, stop);
@@ -814,24 +879,24 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
 
 template <int PASS, int GRAV>
 cudaError_t pairs_g(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t,
-                    const SpatialArrays* sp, int gnseg, cudaEvent_t join) {
+                    const SpatialArrays* sp, int gnseg, cudaEvent_t join, bool lists = false) {
     const bool solids = has(p, GSPH_SOLIDS);
     const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
     if (solids)
-        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t, sp, gnseg, join)
-                    : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t, sp, gnseg, join);
-    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t, sp, gnseg, join)
-                : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t, sp, gnseg, join);
+        return comp ? pairs_t<PASS, GRAV, true, true>(a, p, L, s, t, sp, gnseg, join, lists)
+                    : pairs_t<PASS, GRAV, true, false>(a, p, L, s, t, sp, gnseg, join, lists);
+    return comp ? pairs_t<PASS, GRAV, false, true>(a, p, L, s, t, sp, gnseg, join, lists)
+                : pairs_t<PASS, GRAV, false, false>(a, p, L, s, t, sp, gnseg, join, lists);
 }
 }  // namespace
 
 cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
-                         const KTimer* t, const SpatialArrays* sp, int gnseg, cudaEvent_t join) {
+                         const KTimer* t, const SpatialArrays* sp, int gnseg, cudaEvent_t join, bool lists) {
     if (sp) {  // the culled kernels carry no gravity
         switch (pass) {
-            case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, sp, 0, join);
-            case PASS_ACC: return pairs_g<PASS_ACC, 0>(a, p, L, s, t, sp, gnseg, join);
-            default: return pairs_g<PASS_FUSED, 0>(a, p, L, s, t, sp, gnseg, join);
+            case PASS_VGRAD: return pairs_g<PASS_VGRAD, 0>(a, p, L, s, t, sp, 0, join, lists);
+            case PASS_ACC: return pairs_g<PASS_ACC, 0>(a, p, L, s, t, sp, gnseg, join, lists);
+            default: return pairs_g<PASS_FUSED, 0>(a, p, L, s, t, sp, gnseg, join, lists);
         }
     }
     const int grav = !has(p, GSPH_SELF_GRAVITY) ? 0 : (p.eps2 > 0.0f ? 1 : 2);

@@ -86,6 +86,7 @@ struct JTilePipe {
 
 // ---- culled passes: work items over the near-chunk lists ------------------------------------------
 constexpr int kStageChunks = 4;  // chunks staged per pipeline stage (256 j-particles)
+constexpr int kItemNb = 96;      // neighbour-list slots per lane and work item (density pass -> SPH passes)
 
 // Work item w of the culled passes: i-group g, positions [c0, c1) of g's near-chunk list. Items are
 // numbered group by group (item_start[g] .. item_start[g+1]-1), at most item_chunks chunks each.
@@ -97,6 +98,8 @@ struct CullView {
     int ngroups;
     int64_t nchunks;        // row stride of `list`
     float* part;            // [item][field][kGroup]
+    int* nb;                // nullable: per item, each lane's neighbour indices [item][kItemNb][kGroup] ...
+    int* nbcnt;             // ... and their count [item][kGroup] (kItemNb + 1: the list overflowed)
     __device__ __forceinline__ int items() const { return item_start[ngroups]; }
     __device__ __forceinline__ void item(int w, int& g, int& c0, int& c1) const {
         int lo = 0, hi = ngroups;  // item_start[lo] <= w < item_start[hi]
@@ -242,6 +245,8 @@ struct Launch {
     int density_grid;  // persistent grid of the culled density kernel
 };
 
+// With `sp`, the culled density pass also stores every lane's neighbour indices per work item
+// (sp->item_nb), which the SPH passes of the same step then use instead of scanning the chunks again.
 cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                            const KTimer* t = nullptr, const SpatialArrays* sp = nullptr);
 // near-chunk work items of the culled passes (item_start scan); needs launch_chunk_lists first.
@@ -253,7 +258,7 @@ cudaError_t launch_prepare(const DevArrays& a, const DevParams& p, cudaStream_t 
 // when it is given (the gravity kernel may run on another stream).
 cudaError_t launch_pairs(int pass, const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                          const KTimer* t = nullptr, const SpatialArrays* sp = nullptr, int gnseg = 0,
-                         cudaEvent_t join = nullptr);
+                         cudaEvent_t join = nullptr, bool lists = false);
 cudaError_t launch_gravity_partials(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,
                                     const KTimer* t = nullptr);
 cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s,

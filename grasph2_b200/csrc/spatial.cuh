@@ -25,6 +25,8 @@ struct SpatialArrays {
     int* item_start;   // [n_pad / kGroup + 2] first work item of each group, number of items, chunks per item
     int item_target;   // items aimed at per pass (the item buffer holds item_target + groups items)
     float* item_part;  // [items][fields][kGroup] partial sums of the culled passes
+    int* item_nb;      // [items][kItemNb][kGroup] neighbour indices found by the culled density pass
+    int* item_nbcnt;   // [items][kGroup]
     int* ext_of_int;   // [n_pad] caller's index of the particle stored at each internal slot
     int* order;        // [n_pad] scratch: sort values / gather map
     unsigned* keys;    // [2 n_pad] sort keys (in, out)
