@@ -300,6 +300,33 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def integrator_bytes(params):
+    """Algorithmic bytes per particle of the leapfrog: read x64 24 + v 16 + a 16 (+ rho 4 + drho/dt 4 with
+    SPH, + S 24 + dS/dt 24 with solids), write x64 24 + posm 16 + v 16 (+ rho 4, + S 24): 196 for the
+    impact, 112 for gravity alone."""
+    from grasph2_b200._abi import FLAG_BITS as F
+    b = 56 + 56
+    if params.flags & F["SPH"]:
+        b += 12
+        if params.flags & F["SOLIDS"]:
+            b += 72
+    return b
+
+
+def integrator_roofline(prof, n, params):
+    """HBM roofline of the leapfrog kernels: algorithmic bytes per launch / the launch's event time."""
+    ms, cnt = prof.get("integrate", (0.0, 0))
+    if not cnt:
+        return None
+    INTEGRATOR_BYTES = integrator_bytes(params)
+    peaks = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks))["hbm_gbs"] if os.path.exists(peaks) else 6650.0
+    gbs = INTEGRATOR_BYTES * n / (ms / cnt * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_leapfrog_*", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "bytes_per_launch": INTEGRATOR_BYTES * n, "us_per_launch": ms / cnt * 1e3, "traffic": None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if os.path.exists(peaks) else "fallback"}
+
+
 def total_energy(d):
     return d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
 
@@ -854,6 +881,7 @@ def main():
                      "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if (achieved and peak_tflops) else None,
                      "traffic": None, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
                      "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
+        "integrator_roofline": integrator_roofline(prof, n, params),
         "cpu_baseline": cpu,
         "clocks": clocks,
         "e2e": ({"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,

@@ -108,8 +108,8 @@ class GsphDiag(ctypes.Structure):
                     e_total=self.e_kin + self.e_grav + self.e_int + self.e_shear)
 
 
-KSLOTS = 5
-KSLOT_NAMES = ("density", "vgrad", "pairs", "gravity", "step")
+KSLOTS = 6
+KSLOT_NAMES = ("density", "vgrad", "pairs", "gravity", "step", "integrate")
 
 
 class GsphProfile(ctypes.Structure):

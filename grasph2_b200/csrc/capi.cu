@@ -307,7 +307,10 @@ int integrate(gsph_ctx* c, int not_first_step, cudaStream_t s) {
         if (e != cudaSuccess) return cuda_fail(c, e, "FP64 leapfrog");
         return GSPH_OK;
     }
-    cudaError_t e = launch_leapfrog(c->a, c->dp, not_first_step, s);
+    const KTimer* t = slot_timer(c, GSPH_KSLOT_INTEGRATE);
+    cudaError_t e = t ? timer_record(t->start, s) : cudaSuccess;
+    if (e == cudaSuccess) e = launch_leapfrog(c->a, c->dp, not_first_step, s);
+    if (e == cudaSuccess && t) e = timer_record(t->stop, s);
     if (e != cudaSuccess) return cuda_fail(c, e, "leapfrog");
     c->launches += has(c->dp, GSPH_VARIABLE_TIMESTEP) ? 3 : 1;
     return GSPH_OK;

@@ -403,7 +403,8 @@ const char* gsph_ensemble_last_error(const gsph_ensemble* e);
 #define GSPH_KSLOT_PAIRS    2   /* acceleration / fused pair kernel               */
 #define GSPH_KSLOT_GRAVITY  3   /* gravity-only pair kernel                       */
 #define GSPH_KSLOT_STEP     4   /* one whole step (derivatives + integrate)       */
-#define GSPH_KSLOTS         5
+#define GSPH_KSLOT_INTEGRATE 5  /* the leapfrog kernels of integrate              */
+#define GSPH_KSLOTS         6
 typedef struct gsph_profile {
     double  ms[GSPH_KSLOTS];        /* accumulated device time per slot (CUDA events) */
     int64_t launches[GSPH_KSLOTS];  /* launches timed per slot                         */
