@@ -201,6 +201,12 @@ _SIGNATURES = {
                                             ctypes.c_int32, ctypes.c_void_p]),
     "gsph_snapshot": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     "gsph_state_compare": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _dp, ctypes.c_void_p]),
+    "gsph_writer_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "gsph_writer_write": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]),
+    "gsph_writer_flush": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_writer_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gsph_writer_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "gsph_mlp_param_count": (ctypes.c_int64, []),
     "gsph_mlp_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_void_p)]),
     "gsph_mlp_destroy": (ctypes.c_int, [ctypes.c_void_p]),

@@ -321,6 +321,14 @@ int integrate(gsph_ctx* c, int not_first_step, cudaStream_t s) {
 // the parameter block of the kernels, for the other translation units (ensemble.cu)
 DevParams gsph_dev_params(const gsph_params& p) { return make_dev_params(p); }
 
+// the device arrays and the slot -> caller order map of a single-precision context (writer.cu)
+bool gsph_ctx_state(gsph_ctx* c, DevArrays* a, const int** ext) {
+    if (!c || c->fp64) return false;
+    *a = c->a;
+    *ext = ext_map(c);
+    return true;
+}
+
 extern "C" {
 
 int gsph_params_reference_defaults(gsph_params* p) {

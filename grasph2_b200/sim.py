@@ -212,6 +212,43 @@ class DeviceParticleBuffer:
 
 
 # reference-named free functions --------------------------------------------------------------
+class SnapshotWriter:
+    """Asynchronous tsv snapshots of a context (gsph_writer_*): write() returns once the state is copied
+    on the device; a worker thread writes the files."""
+
+    def __init__(self, pb, attributes=("pos", "mass", "vel", "density"), depth=2):
+        self.lib = pb.lib
+        self._h = ctypes.c_void_p()
+        rc = self.lib.gsph_writer_create(pb.handle, mask_of(attributes), int(depth), ctypes.byref(self._h))
+        if rc != 0:
+            raise GsphError(rc, self.lib.gsph_last_error(None).decode())
+
+    def _check(self, rc):
+        if rc != 0:
+            raise GsphError(rc, self.lib.gsph_writer_last_error(self._h).decode())
+
+    def write(self, filename, stream=None):
+        self._check(self.lib.gsph_writer_write(self._h, str(filename).encode(), _stream_handle(stream)))
+
+    def flush(self):
+        n = ctypes.c_int64()
+        self._check(self.lib.gsph_writer_flush(self._h, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if self._h:
+            rc = self.lib.gsph_writer_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            if rc != 0:
+                raise GsphError(rc, "snapshot writer failed")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Ensemble:
     """S independent simulations of uneven sizes with one parameter set (gsph_ensemble_*). Host states
     hold the simulations back to back, simulation k in rows offsets[k]:offsets[k+1]."""

@@ -360,6 +360,23 @@ int gsph_ic_com_correct(int64_t n, float* pos, float* vel, const float* mass, do
 int gsph_upload_device(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * asynchronous snapshot output (the reference's ResultStorageManager, src/ResultStorageManager.h:
+ * 140-148, .cu:102-186): gsph_writer_write copies the context's state on the device into one of
+ * `depth` slots (ordered on `stream`), converts and copies it to pinned host memory on the writer's own
+ * stream, and returns; a worker thread writes the tsv file (GraSPH2's format and attribute order).
+ * When every slot is busy, write waits for the oldest. Calls on a writer come from the thread that
+ * drives its context; the context must outlive the writer.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct gsph_writer gsph_writer;
+int gsph_writer_create(gsph_ctx* ctx, uint32_t attr_mask, int32_t depth, gsph_writer** out);
+int gsph_writer_write(gsph_writer* w, const char* filename, void* stream);
+/* wait until every queued snapshot is on disk; the first failure's status (message in
+ * gsph_writer_last_error), `written` (nullable) = files written so far */
+int gsph_writer_flush(gsph_writer* w, int64_t* written);
+const char* gsph_writer_last_error(gsph_writer* w);
+int gsph_writer_destroy(gsph_writer* w);
+
+/* ---------------------------------------------------------------------------------------------
  * batched ensemble: S independent simulations of uneven particle counts with one parameter set,
  * advanced by one persistent launch per substep. No counterpart in the reference, which runs one
  * simulation per process (src/main.cu:228-273); each simulation follows computeDerivatives /

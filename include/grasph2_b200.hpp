@@ -215,22 +215,57 @@ inline std::string snapshotFileName(const std::string& directory, const std::str
     return fn.str();
 }
 
-inline void printTextFile(const HostParticleBuffer& h, const std::string& filename,
+// the same from raw host arrays (a gsph_host_particles view of n particles)
+inline void printTextFile(const gsph_host_particles& v, size_t n, const std::string& filename,
                           uint32_t mask = kDefaultStoredAttributes) {
+    const float* a[11] = {v.pos, v.mass, v.vel, v.acc, v.balsara, v.xvel, v.density, v.density_dt, v.dstress,
+                          v.dstress_dt, v.maxvsig};
     std::ofstream file(filename);
     if (!file.is_open()) throw Error(GSPH_E_INVALID, "Could not open output file: " + filename);
     file << std::fixed << std::setprecision(std::numeric_limits<float>::digits10 + 1);
-    for (size_t i = 0; i < h.size(); ++i) {
+    for (size_t i = 0; i < n; ++i) {
         for (int b = 0; b < 11; ++b) {
             if (!(mask >> b & 1u)) continue;
             const int k = attribute_components(b);
-            const std::vector<float>& a = attribute_data(h, b);
-            for (int c = 0; c < k; ++c) file << a[k * i + c] << "\t";
+            for (int c = 0; c < k; ++c) file << a[b][k * i + c] << "\t";
         }
         file << "\n";
     }
     if (file.fail()) throw Error(GSPH_E_INVALID, "Error writing output file: " + filename);
 }
+
+inline void printTextFile(const HostParticleBuffer& h, const std::string& filename,
+                          uint32_t mask = kDefaultStoredAttributes) {
+    gsph_host_particles v = const_cast<HostParticleBuffer&>(h).view();
+    printTextFile(v, h.size(), filename, mask);
+}
+
+// Asynchronous snapshots (ResultStorageManager::printToFile, src/ResultStorageManager.cu:102-186): write()
+// returns once the state is copied on the device; a worker thread writes the tsv file.
+class SnapshotWriter {
+public:
+    SnapshotWriter(DeviceParticleBuffer& pb, uint32_t mask = kDefaultStoredAttributes, int depth = 2) {
+        const int rc = gsph_writer_create(pb.get(), mask, depth, &w_);
+        if (rc != GSPH_OK) throw Error(rc, gsph_last_error(nullptr));
+    }
+    ~SnapshotWriter() {
+        if (w_) gsph_writer_destroy(w_);
+    }
+    SnapshotWriter(const SnapshotWriter&) = delete;
+    SnapshotWriter& operator=(const SnapshotWriter&) = delete;
+    void write(const std::string& filename, void* stream = nullptr) { chk(gsph_writer_write(w_, filename.c_str(), stream)); }
+    int64_t flush() {
+        int64_t n = 0;
+        chk(gsph_writer_flush(w_, &n));
+        return n;
+    }
+
+private:
+    void chk(int rc) {
+        if (rc != GSPH_OK) throw Error(rc, gsph_writer_last_error(w_));
+    }
+    gsph_writer* w_ = nullptr;
+};
 
 // TextFile reader (src/initialConditions/particleSources/TextFile.h:76-120): non-blank lines are
 // particles, values separated by `sep`, the attributes in `mask` in particle_bases order.

@@ -91,6 +91,23 @@ int main(int argc, char** argv) {
             return 1;
         }
     }
+    {  // asynchronous snapshots while stepping
+        gsph::SnapshotWriter w(pb, gsph::kDefaultStoredAttributes, 2);
+        for (int k = 0; k < 3; ++k) {
+            gsph::integrate(pb, true);
+            gsph::computeDerivatives(pb);
+            w.write(gsph::snapshotFileName(tmp + "/", "async_", "test", static_cast<float>(k)));
+        }
+        if (w.flush() != 3) {
+            std::printf("writer count mismatch\n");
+            return 1;
+        }
+        gsph::HostParticleBuffer last = gsph::readTextFile(gsph::snapshotFileName(tmp + "/", "async_", "test", 2.0f));
+        if (last.size() != out.size()) {
+            std::printf("async snapshot size mismatch\n");
+            return 1;
+        }
+    }
     std::printf("ADAPTER OK t=%.6f file=%s\n", t, fn.c_str());
     return 0;
 }

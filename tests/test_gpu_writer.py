@@ -1,0 +1,34 @@
+"""Asynchronous snapshot writer: files equal synchronous downloads of the same states."""
+
+import numpy as np
+import pytest
+
+from grasph2_b200 import ics
+from grasph2_b200.params import config0_params
+from grasph2_b200.sim import DeviceParticleBuffer, SnapshotWriter
+
+pytestmark = pytest.mark.gpu
+
+
+def read_tsv(path):
+    return np.loadtxt(path, delimiter="\t", usecols=range(8), dtype=np.float64)
+
+
+def test_async_snapshots_match_downloads(tmp_path):
+    p = config0_params()
+    n = 3000
+    st = ics.uniform_sphere(n, rho0=0.239, omega=(0, 0, 0.1), seed=5)
+    want = []
+    with DeviceParticleBuffer(p, n) as pb:
+        pb.upload(st)
+        with SnapshotWriter(pb, depth=2) as w:
+            for k in range(4):
+                pb.step(3)
+                w.write(tmp_path / ("snap_%d.tsv" % k))
+                d = pb.download(["pos", "mass", "vel", "density"])
+                want.append(np.concatenate([d["pos"], d["mass"][:, None], d["vel"], d["density"][:, None]], 1))
+            assert w.flush() == 4
+    for k in range(4):
+        got = read_tsv(tmp_path / ("snap_%d.tsv" % k))
+        # the tsv holds digits10 + 1 = 7 significant decimal digits of each float
+        np.testing.assert_allclose(got, want[k], rtol=2e-6, atol=1e-7)
