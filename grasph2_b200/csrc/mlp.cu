@@ -183,10 +183,15 @@ __device__ __forceinline__ void hidden_out(uint32_t tD, const float* bias, unsig
     }
 }
 
-// forward over tiles of 128 rows (persistent grid): y[n][13] = MLP(x[n][32])
-__global__ void __launch_bounds__(kTileM, 1) k_mlp_forward(const float* __restrict__ x, float* __restrict__ y, int64_t n,
-                                                          const __nv_bfloat16* __restrict__ wq,
-                                                          const float* __restrict__ bq, int* status) {
+// Forward over tiles of 128 rows (persistent grid): y[n][13] = MLP(x[n][32]). Four warpgroups per CTA:
+// warpgroup q loads columns 8q..8q+7 of the inputs and drains columns 32q..32q+31 of every hidden
+// accumulator (each warp reads its 32 tensor-memory lanes), so the epilogues run four times wider than
+// the one-warpgroup training kernel; warpgroup 0 writes the outputs.
+constexpr int kFwdThreads = 4 * kTileM;
+
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __restrict__ x, float* __restrict__ y,
+                                                               int64_t n, const __nv_bfloat16* __restrict__ wq,
+                                                               const float* __restrict__ bq, int* status) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint64_t bar;
     __shared__ uint32_t tslot;
@@ -202,43 +207,66 @@ __global__ void __launch_bounds__(kTileM, 1) k_mlp_forward(const float* __restri
     umma::fence_after();
     const uint32_t T0 = tslot, T1 = tslot + 128;
     const uint32_t base = smem_u32(sm);
+    const int row = threadIdx.x & (kTileM - 1), q = threadIdx.x >> 7;
     uint32_t phase = 0;
+    // hidden epilogue of this thread's row and column quarter: h = SiLU(D + b)
+    auto hidden = [&](uint32_t tD, const float* bias) {
+        float v[32];
+        umma::ld32(umma::lane_addr(tD, 32 * q), v);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) v[k] = silu(v[k] + bias[32 * q + k]);
+#pragma unroll
+        for (int k = 0; k < 32; k += 8) umma::st8(sm + sH1, row, 32 * q + k, kTileM, v + k);
+    };
     const int64_t tiles = (n + kTileM - 1) / kTileM;
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int64_t p = tile * kTileM + threadIdx.x;
-        load_x(sm, x, p, n);
+        const int64_t p = tile * kTileM + row;
+        {  // inputs: 8 columns of one row per thread
+            float v[8];
+            if (p < n) {
+                const float4* src = reinterpret_cast<const float4*>(x + p * kIn + 8 * q);
+                const float4 a = src[0], b = src[1];
+                v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] = 0.0f;
+            }
+            umma::st8(sm + sX, row, 8 * q, kTileM, v);
+        }
         before_issue();
         if (threadIdx.x == 0) {
             issue(T0, base + sX, kTileM, false, base + sW1, kHid, false, kHid, kIn);
             umma::commit(&bar);
         }
         if (!after_commit(&bar, phase, status)) break;
-        hidden_out(T0, sbias, sm + sH1);
+        hidden(T0, sbias);
         before_issue();
         if (threadIdx.x == 0) {
             issue(T1, base + sH1, kTileM, false, base + sW2, kHid, false, kHid, kHid);
             umma::commit(&bar);
         }
         if (!after_commit(&bar, phase, status)) break;
-        hidden_out(T1, sbias + kHid, sm + sH1);
+        hidden(T1, sbias + kHid);
         before_issue();
         if (threadIdx.x == 0) {
             issue(T0, base + sH1, kTileM, false, base + sW3, kHid, false, kHid, kHid);
             umma::commit(&bar);
         }
         if (!after_commit(&bar, phase, status)) break;
-        hidden_out(T0, sbias + 2 * kHid, sm + sH1);
+        hidden(T0, sbias + 2 * kHid);
         before_issue();
         if (threadIdx.x == 0) {
             issue(T1, base + sH1, kTileM, false, base + sW4, kOutP, false, kOutP, kHid);
             umma::commit(&bar);
         }
         if (!after_commit(&bar, phase, status)) break;
-        float v[16];
-        umma::ld16(umma::lane_addr(T1, 0), v);
-        if (p < n) {
+        if (q == 0) {
+            float v[16];
+            umma::ld16(umma::lane_addr(T1, 0), v);
+            if (p < n) {
 #pragma unroll
-            for (int o = 0; o < kOut; ++o) y[p * kOut + o] = v[o] + sbias[3 * kHid + o];
+                for (int o = 0; o < kOut; ++o) y[p * kOut + o] = v[o] + sbias[3 * kHid + o];
+            }
         }
     }
     umma::fence_before();
@@ -620,7 +648,7 @@ int gsph_mlp_forward(gsph_mlp* m, const float* x, float* y, int64_t n, void* str
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int64_t tiles = (n + kTileM - 1) / kTileM;
     const int grid = static_cast<int>(tiles < m->grid ? tiles : m->grid);
-    k_mlp_forward<<<grid, kTileM, kFwdSmem, s>>>(x, y, n, m->wq, m->bq, m->status);
+    k_mlp_forward<<<grid, kFwdThreads, kFwdSmem, s>>>(x, y, n, m->wq, m->bq, m->status);
     MLP_CK(m, cudaGetLastError(), "forward launch");
     return GSPH_OK;
 }

@@ -78,7 +78,7 @@ __device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-// 32 consecutive FP32 columns of this thread's tensor-memory lane (warp w reads lanes 32w .. 32w+31)
+// 32 consecutive FP32 columns of this thread's tensor-memory lane (see lane_addr)
 __device__ __forceinline__ void ld32(uint32_t taddr, float* v) {
     uint32_t r[32];
     asm volatile(
@@ -105,9 +105,9 @@ __device__ __forceinline__ void ld16(uint32_t taddr, float* v) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
-// lane of this thread in a 128-lane accumulator: warp w owns lanes 32w .. 32w + 31
+// lane of this thread in a 128-lane accumulator: warp w of each warpgroup owns lanes 32 (w % 4) .. + 31
 __device__ __forceinline__ uint32_t lane_addr(uint32_t tbase, int col) {
-    return tbase + (static_cast<uint32_t>((threadIdx.x >> 5) * 32) << 16) + static_cast<uint32_t>(col);
+    return tbase + (static_cast<uint32_t>(((threadIdx.x >> 5) & 3) * 32) << 16) + static_cast<uint32_t>(col);
 }
 
 // store 8 consecutive bf16 columns c0..c0+7 (c0 % 8 == 0) of row r: one 16-byte write
