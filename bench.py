@@ -300,6 +300,21 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """The largest of a local value over all ranks (a job's time is its slowest rank's)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(steps, world, total_ms):
+    """Units all ranks processed / the slowest rank's time (replicas: every rank does `steps`)."""
+    return steps * world / (total_ms * 1e-3)
+
+
 def integrator_bytes(params):
     """Algorithmic bytes per particle of the leapfrog: read x64 24 + v 16 + a 16 (+ rho 4 + drho/dt 4 with
     SPH, + S 24 + dS/dt 24 with solids), write x64 24 + posm 16 + v 16 (+ rho 4, + S 24): 196 for the
@@ -501,11 +516,7 @@ def run_ensemble(args, rank, world, local):
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
     gpu_launches = ens.launch_count() - launches0
-    total_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(ev0, ev1)), dist, dev)
     ms_per_step = total_ms / args.steps
 
     # e2e through the public API with pinned host buffers: upload, one step, download
@@ -559,7 +570,7 @@ def run_ensemble(args, rank, world, local):
         if dist is not None:
             dist.destroy_process_group()
         return
-    value = world / (ms_per_step * 1e-3)
+    value = whole_job_rate(args.steps, world, total_ms)
     nb = sum(neighbour_pairs(s["pos"], params.H, dev) for s in states[::8]) * 8
     flops = FLOP_GRAV_PAIR * pairs + FLOP_DENS_PAIR * pairs + (FLOP_DENS_NB + FLOP_ACC_NB) * nb
     achieved = flops / (ms_per_step * 1e-3) / 1e12
@@ -807,11 +818,7 @@ def main():
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
     gpu_launches = pb.launch_count() - launches0
-    total_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(ev0, ev1)), dist, dev)
     prof = pb.profile_read()
 
     # e2e: the public API with host buffers (pinned): upload inputs, one step, download the result
@@ -851,8 +858,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    steps_total = args.steps * world
-    value = steps_total / (total_ms * 1e-3)
+    value = whole_job_rate(args.steps, world, total_ms)
     ms_per_step = total_ms / args.steps
     nb = neighbour_pairs(st["pos"], params.H, dev) if (params.flags & 2) else 0
     fl = flops_per_step(params, st, nb, culled=not args.no_cull)
