@@ -43,6 +43,14 @@ FLOP_FUSED_NB = 160        # strain/rotation rates, div v, stress acceleration, 
 FLOP_ACC_NB = 60           # pressure acceleration + AV per neighbour (fluid, acceleration pass only)
 
 FLUSH_BYTES = 256 << 20
+
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture of the same workload:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none \
+#       -k regex:"k_gravity_x2|k_pairs_items|k_density_items" -s 9 -c 6 --csv \
+#       python bench.py --steps 5 --warmup 3 --no-cpu-baseline --no-e2e --no-peak --drift-steps 0 --no-autotune
+# k_gravity_x2 on the impact: 1.06-1.08 MB read, 0 written (its j-segment partials stay in L2) = the
+# 1.05 MB of j-records: no re-reads.
+MEASURED_TRAFFIC = {("impact", 65536, "gravity"): 1.08e6}
 FLAG_DEAL_WITH_NO_PARTNERS = 1 << 3  # GSPH_DEAL_WITH_NO_PARTNERS
 
 
@@ -893,7 +901,8 @@ def main():
         "kernel_ms_per_step": {k: (v[0] / v[1] if v[1] else None) for k, v in prof.items()},
         "roofline": {"bound": "fp32", "kernel": dominant, "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if (achieved and peak_tflops) else None,
-                     "traffic": None, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
+                     "traffic": MEASURED_TRAFFIC.get((args.workload, n, dominant)),
+                     "algorithmic_bytes": 16 * n, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
                      "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
         "integrator_roofline": integrator_roofline(prof, n, params),
         "cpu_baseline": cpu,
