@@ -18,9 +18,7 @@ oracle/_ref) on this machine's cores, on bounded row samples of the same workloa
 """
 
 import argparse
-import ctypes
 import json
-import math
 import os
 import statistics
 import subprocess

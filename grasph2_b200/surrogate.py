@@ -25,9 +25,8 @@ import time
 
 import numpy as np
 
-from ._abi import load_library
 from .mlp import MLP
-from .sim import GsphError, _stream_handle
+from .sim import _stream_handle
 
 NF, NO = 32, 13
 OUT_NAMES = ["dx", "dy", "dz", "dvx", "dvy", "dvz", "drho", "dSxx", "dSyy", "dSzz", "dSxy", "dSxz", "dSyz"]
@@ -119,7 +118,6 @@ class Surrogate:
     def __init__(self, K=8, params=None, in_mu=None, in_sig=None, out_mu=None, out_sig=None):
         torch = _torch()
         self.K = int(K)
-        from . import mlp as _m  # noqa: F401
         self.net = MLP(params)
         z = lambda k: np.zeros(k, np.float32)  # noqa: E731
         o = lambda k: np.ones(k, np.float32)  # noqa: E731

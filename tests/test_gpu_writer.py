@@ -32,3 +32,18 @@ def test_async_snapshots_match_downloads(tmp_path):
         got = read_tsv(tmp_path / ("snap_%d.tsv" % k))
         # the tsv holds digits10 + 1 = 7 significant decimal digits of each float
         np.testing.assert_allclose(got, want[k], rtol=2e-6, atol=1e-7)
+
+
+def test_writer_reports_a_failed_file(tmp_path):
+    p = config0_params()
+    st = ics.uniform_sphere(500, rho0=0.239, seed=6)
+    with DeviceParticleBuffer(p, 500) as pb:
+        pb.upload(st)
+        w = SnapshotWriter(pb, depth=1)
+        w.write(tmp_path / "missing_dir" / "x.tsv")
+        w.write(tmp_path / "ok.tsv")  # the single slot frees once the first job has failed
+        with pytest.raises(Exception):
+            w.flush()
+        with pytest.raises(Exception):
+            w.close()
+    assert (tmp_path / "ok.tsv").exists()
