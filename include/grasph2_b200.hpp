@@ -44,6 +44,41 @@ inline void check(int rc, gsph_ctx* ctx) {
     if (rc != GSPH_OK) throw Error(rc, gsph_last_error(ctx));
 }
 
+// ---- precision types (settings/precisionSettings.h, src/types.h:32-56; the single-precision build) ----
+using f1_t = float;
+struct f3_t {
+    f1_t x = 0, y = 0, z = 0;
+};
+struct f4_t {
+    f1_t x = 0, y = 0, z = 0, w = 0;
+};
+inline f3_t operator+(f3_t a, f3_t b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline f3_t operator-(f3_t a, f3_t b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline f3_t operator*(f3_t a, f1_t s) { return {a.x * s, a.y * s, a.z * s}; }
+inline f3_t operator*(f1_t s, f3_t a) { return a * s; }
+inline f1_t dot(f3_t a, f3_t b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// 3x3 matrix, row-major; m(r, c) and m[r][c] as mpu::Mat's accessors
+struct m3_t {
+    f1_t v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    f1_t& operator()(int r, int c) { return v[3 * r + c]; }
+    f1_t operator()(int r, int c) const { return v[3 * r + c]; }
+    f1_t* operator[](int r) { return v + 3 * r; }
+    const f1_t* operator[](int r) const { return v + 3 * r; }
+};
+
+// One particle with every attribute of the reference's DeviceParticlesType (settings/settings.h:184),
+// the counterpart of Particle<...> (src/particles/Particle.h) for host-side access.
+struct Particle {
+    f3_t pos;
+    f1_t mass = 0;
+    f3_t vel, acc;
+    f1_t balsara = 0;
+    f3_t xvel;
+    f1_t density = 0, density_dt = 0;
+    m3_t dstress, dstress_dt;
+    f1_t maxvsig = 0;
+};
+
 // Host particle attributes in the reference layout, one std::vector<float> per attribute.
 class HostParticleBuffer {
 public:
@@ -61,6 +96,46 @@ public:
                                    density.data(), density_dt.data(), dstress.data(), dstress_dt.data(), maxvsig.data()};
     }
     std::vector<float> pos, mass, vel, acc, balsara, xvel, density, density_dt, dstress, dstress_dt, maxvsig;
+
+    // HostParticleBuffer::loadParticle / storeParticle (src/particles/HostParticleBuffer.h:79-83); the
+    // attributes written are chosen by a GSPH_* mask instead of the reference's template arguments
+    Particle loadParticle(size_t i) const {
+        Particle p;
+        p.pos = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+        p.mass = mass[i];
+        p.vel = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+        p.acc = {acc[3 * i], acc[3 * i + 1], acc[3 * i + 2]};
+        p.balsara = balsara[i];
+        p.xvel = {xvel[3 * i], xvel[3 * i + 1], xvel[3 * i + 2]};
+        p.density = density[i];
+        p.density_dt = density_dt[i];
+        for (int k = 0; k < 9; ++k) {
+            p.dstress.v[k] = dstress[9 * i + k];
+            p.dstress_dt.v[k] = dstress_dt[9 * i + k];
+        }
+        p.maxvsig = maxvsig[i];
+        return p;
+    }
+    void storeParticle(size_t i, const Particle& p, uint32_t mask = GSPH_ALL_ATTRIBS) {
+        auto put3 = [&](std::vector<float>& a, const f3_t& v) {
+            a[3 * i] = v.x;
+            a[3 * i + 1] = v.y;
+            a[3 * i + 2] = v.z;
+        };
+        if (mask & GSPH_POS) put3(pos, p.pos);
+        if (mask & GSPH_MASS) mass[i] = p.mass;
+        if (mask & GSPH_VEL) put3(vel, p.vel);
+        if (mask & GSPH_ACC) put3(acc, p.acc);
+        if (mask & GSPH_BALSARA) balsara[i] = p.balsara;
+        if (mask & GSPH_XVEL) put3(xvel, p.xvel);
+        if (mask & GSPH_DENSITY) density[i] = p.density;
+        if (mask & GSPH_DENSITY_DT) density_dt[i] = p.density_dt;
+        for (int k = 0; k < 9; ++k) {
+            if (mask & GSPH_DSTRESS) dstress[9 * i + k] = p.dstress.v[k];
+            if (mask & GSPH_DSTRESS_DT) dstress_dt[9 * i + k] = p.dstress_dt.v[k];
+        }
+        if (mask & GSPH_MAXVSIG) maxvsig[i] = p.maxvsig;
+    }
 
 private:
     size_t n_ = 0;

@@ -108,6 +108,16 @@ int main(int argc, char** argv) {
             return 1;
         }
     }
+    {  // per-particle host access with the reference's names
+        gsph::Particle q = out.loadParticle(5);
+        q.pos = q.pos + gsph::f3_t{1.0f, 0.0f, 0.0f};
+        q.dstress(0, 1) = 0.25f;
+        out.storeParticle(5, q, GSPH_POS | GSPH_DSTRESS);
+        if (out.pos[15] != q.pos.x || out.dstress[9 * 5 + 1] != 0.25f) {
+            std::printf("particle access mismatch\n");
+            return 1;
+        }
+    }
     std::printf("ADAPTER OK t=%.6f file=%s\n", t, fn.c_str());
     return 0;
 }
