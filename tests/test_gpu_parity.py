@@ -342,14 +342,15 @@ def test_periodic_resort_matches(oracle):
     check_within(out[1]["vel"], out[0]["vel"], sens["vel"], TOL_STEP, "resorted vel")
 
 
+@pytest.mark.parametrize("accum", ["plain", "compensated"])
 @pytest.mark.parametrize("name,cull", [("solid", True), ("solid", False), ("nbody", True), ("fluid", True)])
-def test_autotune_keeps_results(oracle, name, cull):
+def test_autotune_keeps_results(oracle, name, cull, accum):
     """The autotuner only changes launch shapes: results stay within the parity bound, and stepping
     re-captures the step graph with the tuned shapes."""
     p = variant_params(name)
     st = _edge_state(name, 3000, seed=31)
     ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st)
-    with DeviceParticleBuffer(p, 3000, make_options(cull=cull)) as pb:
+    with DeviceParticleBuffer(p, 3000, make_options(cull=cull, accum=accum)) as pb:
         pb.upload(st)
         shape = pb.autotune(2)
         assert shape["grav_ipt"] in (1, 2, 4, 8) and shape["cull"] == int(cull and bool(p.flags & F["SPH"]))
@@ -357,4 +358,4 @@ def test_autotune_keeps_results(oracle, name, cull):
         got = pb.download()
         pb.step(2)
         pb.download()
-    check_derivatives(got, ref, sens, p, "%s autotuned cull=%s" % (name, cull))
+    check_derivatives(got, ref, sens, p, "%s autotuned cull=%s %s" % (name, cull, accum))

@@ -213,3 +213,28 @@ def test_state_compare_matches_full_energies():
     np.testing.assert_allclose(d02, ((xq - x0) ** 2).sum(), rtol=1e-9)
     # first-order gravitational energy change: agrees to a small fraction of the difference itself
     assert abs(de - (ep - eq)) <= 0.05 * abs(ep - eq) + 1e-9 * abs(eq), (de, ep - eq)
+
+
+def test_surrogate_entry_points_reject_unsupported_contexts():
+    from grasph2_b200.params import make_options
+    from grasph2_b200.sim import GsphError
+    p = impact_params(900, 100)
+    st = solid_state(1000, 9)
+    with DeviceParticleBuffer(p, 1000, make_options(cull=False)) as pb:
+        pb.upload(st)
+        with pytest.raises(GsphError) as e:
+            S.features(pb)
+        assert e.value.code == -7
+    with DeviceParticleBuffer(p, 1000, make_options(precision="double")) as pb:
+        with pytest.raises(GsphError) as e:
+            S.apply(pb, 8)
+        assert e.value.code == -7
+        with pytest.raises(GsphError):
+            S.snapshot(pb, 0, False)
+    with DeviceParticleBuffer(p, 1000) as pb:
+        pb.upload(st)
+        with pytest.raises(GsphError) as e:
+            S.snapshot(pb, 0, True)  # nothing saved yet
+        assert e.value.code == -4
+        with pytest.raises(GsphError):
+            S.snapshot(pb, 9, False)  # no such slot
