@@ -150,9 +150,11 @@ class Surrogate:
             apply(pb, self.K, None, None, None, stream)
 
 
-def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, stream=None):
+def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, clip=0.0, stream=None):
     """Train a Surrogate on (X, Y) with the device kernels (forward + backward on the tensor cores, Adam);
-    wout weights the 13 standardised outputs in the loss (default 1). Returns (surrogate, loss history)."""
+    wout weights the 13 standardised outputs in the loss (default 1); clip > 0 limits the standardised
+    targets to +-clip (the heavy tails of the impact zone otherwise dominate single batches). Returns
+    (surrogate, loss history)."""
     torch = _torch()
     from .mlp import init_params
     in_mu, in_sig = X.mean(0), X.std(0) + 1e-6
@@ -162,6 +164,8 @@ def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=Non
                     out_mu.astype(np.float32), out_sig.astype(np.float32))
     Xd = ((torch.from_numpy(X).cuda() - sur.dev["in_mu"]) / sur.dev["in_sig"]).contiguous()
     Yd = ((torch.from_numpy(Y).cuda() - sur.dev["out_mu"]) / sur.dev["out_sig"]).contiguous()
+    if clip > 0:
+        Yd.clamp_(-clip, clip)
     w = torch.from_numpy(np.asarray(wout if wout is not None else np.ones(NO), dtype=np.float32)).cuda()
     g = torch.Generator(device="cuda").manual_seed(seed)
     m = X.shape[0]

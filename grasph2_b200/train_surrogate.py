@@ -33,6 +33,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--clip", type=float, default=0.0, help="limit the standardised targets to +-clip (0: off)")
     ap.add_argument("--K", type=int, default=8)
     ap.add_argument("--seed", type=int, default=20261207)
     ap.add_argument("--out", default=DEFAULT_OUT)
@@ -62,12 +63,13 @@ def main(argv=None):
     X, Y = np.concatenate(X), np.concatenate(Y)
     t_collect = time.time() - t0
     t0 = time.time()
-    sur, hist = S.fit(X, Y, a.K, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=max(1, a.steps // 20))
+    sur, hist = S.fit(X, Y, a.K, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=max(1, a.steps // 20),
+                      clip=a.clip)
     torch.cuda.synchronize()
     t_fit = time.time() - t0
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     meta = dict(n=a.n, trajectories=a.trajectories, windows=a.windows, every=a.every, rows=a.rows, steps=a.steps,
-                batch=a.batch, lr=a.lr, seed=a.seed, samples=int(X.shape[0]), collect_s=t_collect, fit_s=t_fit,
+                batch=a.batch, lr=a.lr, clip=a.clip, seed=a.seed, samples=int(X.shape[0]), collect_s=t_collect, fit_s=t_fit,
                 loss=[(int(s), float(l)) for s, l in hist])
     sur.save(a.out, meta=json.dumps(meta))
     with open(os.path.splitext(a.out)[0] + ".json", "w") as f:
