@@ -670,7 +670,7 @@ def run_surrogate(args, rank, world, local):
             pb.upload(st)
             pb.step(max(args.warmup, 1))
             torch.cuda.synchronize()
-            l0 = pb.launch_count()
+            l0 = pb.launch_count() + sur.launch_count()
             t0 = time.perf_counter()
             if form == "plain":
                 pb.step(substeps)
@@ -678,7 +678,7 @@ def run_surrogate(args, rank, world, local):
                 r = {"wall_s": time.perf_counter() - t0, "accepted": None, "windows": args.windows}
             else:
                 r = S.advance(pb, sur, args.windows, M=M, use_net=(form == "surrogate"))
-            launches = pb.launch_count() - l0
+            launches = pb.launch_count() + sur.launch_count() - l0
             d = pb.diagnostics(0.0, fast=True)
             energies[form] = d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
             errs = np.array(r["errors"]) if r.get("errors") else None

@@ -222,7 +222,29 @@ _SIGNATURES = {
     "gsph_mlp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_surrogate_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)] * 5 +
+                              [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "gsph_surrogate_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "gsph_surrogate_save": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "gsph_surrogate_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_surrogate_mlp": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "gsph_surrogate_substeps": (ctypes.c_int32, [ctypes.c_void_p]),
+    "gsph_surrogate_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "gsph_surrogate_propose": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    "gsph_surrogate_judge": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_double,
+                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_surrogate_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
+    "gsph_surrogate_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "gsph_surrogate_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
 }
+
+
+class SurrogateWindow(ctypes.Structure):
+    """gsph_surrogate_window"""
+    _fields_ = [("pos_error", ctypes.c_double), ("energy_error", ctypes.c_double), ("accepted", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 def load_library(path=None):

@@ -92,18 +92,44 @@ constexpr int kBias = 3 * kHid + kOutP;
 // shared-memory map (bytes)
 constexpr uint32_t sW1 = 0, sW2 = sW1 + kHid * kIn * 2, sW3 = sW2 + kHid * kHid * 2, sW4 = sW3 + kHid * kHid * 2,
                    sX = sW4 + kOutP * kHid * 2, sH1 = sX + kTileM * kIn * 2;
-// inference: one activation buffer
-constexpr uint32_t sBiasF = sH1 + kTileM * kHid * 2, kFwdSmem = sBiasF + kBias * 4;
+// inference: per tile slot one input and one activation buffer
+constexpr int kSlots = 2;
+constexpr uint32_t kSlotBytes = kTileM * kIn * 2 + kTileM * kHid * 2;
+constexpr uint32_t sBiasF = sX + kSlots * kSlotBytes, kFwdSmem = sBiasF + kBias * 4;
+static_assert(kFwdSmem <= 227 * 1024, "forward kernel shared memory");
 // training: three activation buffers, the output gradient, the layer gradient, a block of ones
 constexpr uint32_t sH2 = sH1 + kTileM * kHid * 2, sH3 = sH2 + kTileM * kHid * 2, sG4 = sH3 + kTileM * kHid * 2,
                    sG = sG4 + kTileM * kOutP * 2, sOnes = sG + kTileM * kHid * 2, sBiasT = sOnes + kTileM * 16 * 2,
                    kTrainSmem = sBiasT + kBias * 4;
 static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU through one hardware tanh (tanh.approx.f32, PTX ISA 7.0; relative error about 2^-11, below the
+// bf16 rounding of the activations): z sigmoid(z) = u + u tanh(u) with u = z / 2, and
+// d/dz [z sigmoid(z)] = s (1 + z (1 - s)) with s = sigmoid(z) = 1/2 + tanh(u) / 2
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float silu(float z) {
+    const float u = 0.5f * z;
+    return fmaf(u, tanh_hw(u), u);
+}
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
+    const float s = fmaf(0.5f, tanh_hw(0.5f * z), 0.5f);
+    return s * fmaf(z, 1.0f - s, 1.0f);
+}
+
+// named CTA barrier `id` over `n` threads (a multiple of 32), and the same with an AND over a predicate
+__device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ bool named_and(int id, int n, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, %2, %3, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(r)
+        : "r"(v ? 1u : 0u), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
 }
 
 // stage the packed weights (row-major bf16) into the core-matrix layout, biases as FP32
@@ -183,86 +209,103 @@ __device__ __forceinline__ void hidden_out(uint32_t tD, const float* bias, unsig
     }
 }
 
-// Forward over tiles of 128 rows (persistent grid): y[n][13] = MLP(x[n][32]). Four warpgroups per CTA:
-// warpgroup q loads columns 8q..8q+7 of the inputs and drains columns 32q..32q+31 of every hidden
-// accumulator (each warp reads its 32 tensor-memory lanes), so the epilogues run four times wider than
-// the one-warpgroup training kernel; warpgroup 0 writes the outputs.
-constexpr int kFwdThreads = 4 * kTileM;
+// Forward over tiles of 128 rows (persistent grid): y[n][13] = MLP(x[n][32]). A CTA runs two
+// independent tile pipelines (slots) of two warpgroups each; a slot has its own input and activation
+// buffers, 128 tensor-memory columns, MMA barrier and named CTA barrier, so while one slot drains an
+// accumulator (bias, SiLU, bf16 pack) the tensor cores run the other slot's layer and its input loads
+// are in flight. Slot s takes tiles 2 b + s, 2 (b + grid) + s, ... of CTA b. In a slot, warp w drains
+// tensor-memory lanes 32 (w % 4) .. + 31 (its rows) and columns 64 (w / 4) .. + 63 of each hidden
+// accumulator; the first warpgroup writes the outputs.
+constexpr int kSlotThreads = 2 * kTileM, kFwdThreads = kSlots * kSlotThreads;
 
 __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __restrict__ x, float* __restrict__ y,
                                                                int64_t n, const __nv_bfloat16* __restrict__ wq,
                                                                const float* __restrict__ bq, int* status) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[kSlots];
     __shared__ uint32_t tslot;
     float* sbias = reinterpret_cast<float*>(sm + sBiasF);
     stage_weights(sm, wq, bq, sbias);
     if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
+        for (int k = 0; k < kSlots; ++k) mbar_init(&bar[k], 1);
         fence_barrier_init();
     }
     if (threadIdx.x < 32) umma::tmem_alloc(&tslot, 256);
     umma::fence_before();
     __syncthreads();
     umma::fence_after();
-    const uint32_t T0 = tslot, T1 = tslot + 128;
+    const int slot = threadIdx.x / kSlotThreads, t = threadIdx.x % kSlotThreads;
+    const int row = t & (kTileM - 1), half = t / kTileM;
+    const int bid = 1 + slot;  // named barrier of the slot (0 is __syncthreads)
+    const uint32_t T = tslot + 128 * slot;
     const uint32_t base = smem_u32(sm);
-    const int row = threadIdx.x & (kTileM - 1), q = threadIdx.x >> 7;
+    const uint32_t xo = sX + slot * kSlotBytes, ho = xo + kTileM * kIn * 2;
+    uint64_t* mbar = &bar[slot];
     uint32_t phase = 0;
-    // hidden epilogue of this thread's row and column quarter: h = SiLU(D + b)
-    auto hidden = [&](uint32_t tD, const float* bias) {
-        float v[32];
-        umma::ld32(umma::lane_addr(tD, 32 * q), v);
+    // shared-memory writes and tensor-memory reads of the slot before the MMAs its first thread issues
+    auto slot_sync = [&] {
+        umma::fence_smem_to_async();
+        umma::fence_before();
+        named_sync(bid, kSlotThreads);
+        umma::fence_after();
+    };
+    // every thread of the slot waits for the last commit; uniform result
+    auto slot_wait = [&]() -> bool {
+        const bool ok = named_and(bid, kSlotThreads, umma::wait_mma(mbar, phase, status));
+        phase ^= 1u;
+        umma::fence_after();
+        return ok;
+    };
+    auto layer = [&](uint32_t a, uint32_t b, int N, int K) {
+        slot_sync();
+        if (t == 0) {
+            issue(T, base + a, kTileM, false, base + b, N, false, N, K);
+            umma::commit(mbar);
+        }
+        return slot_wait();
+    };
+    // hidden epilogue of this thread's row and column half: h = SiLU(D + b)
+    auto hidden = [&](const float* bias) {
+#pragma unroll 1
+        for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 32) {
+            float v[32];
+            umma::ld32(umma::lane_addr(T, c0), v);
 #pragma unroll
-        for (int k = 0; k < 32; ++k) v[k] = silu(v[k] + bias[32 * q + k]);
+            for (int k = 0; k < 32; ++k) v[k] = silu(v[k] + bias[c0 + k]);
 #pragma unroll
-        for (int k = 0; k < 32; k += 8) umma::st8(sm + sH1, row, 32 * q + k, kTileM, v + k);
+            for (int k = 0; k < 32; k += 8) umma::st8(sm + ho, row, c0 + k, kTileM, v + k);
+        }
     };
     const int64_t tiles = (n + kTileM - 1) / kTileM;
-    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (int64_t tile = static_cast<int64_t>(blockIdx.x) * kSlots + slot; tile < tiles;
+         tile += static_cast<int64_t>(gridDim.x) * kSlots) {
         const int64_t p = tile * kTileM + row;
-        {  // inputs: 8 columns of one row per thread
-            float v[8];
+        {  // inputs: 16 columns of one row per thread
+            float v[16];
             if (p < n) {
-                const float4* src = reinterpret_cast<const float4*>(x + p * kIn + 8 * q);
-                const float4 a = src[0], b = src[1];
-                v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+                const float4* src = reinterpret_cast<const float4*>(x + p * kIn + 16 * half);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float4 q = src[k];
+                    v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
+                }
             } else {
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = 0.0f;
+                for (int k = 0; k < 16; ++k) v[k] = 0.0f;
             }
-            umma::st8(sm + sX, row, 8 * q, kTileM, v);
+            umma::st8(sm + xo, row, 16 * half, kTileM, v);
+            umma::st8(sm + xo, row, 16 * half + 8, kTileM, v + 8);
         }
-        before_issue();
-        if (threadIdx.x == 0) {
-            issue(T0, base + sX, kTileM, false, base + sW1, kHid, false, kHid, kIn);
-            umma::commit(&bar);
-        }
-        if (!after_commit(&bar, phase, status)) break;
-        hidden(T0, sbias);
-        before_issue();
-        if (threadIdx.x == 0) {
-            issue(T1, base + sH1, kTileM, false, base + sW2, kHid, false, kHid, kHid);
-            umma::commit(&bar);
-        }
-        if (!after_commit(&bar, phase, status)) break;
-        hidden(T1, sbias + kHid);
-        before_issue();
-        if (threadIdx.x == 0) {
-            issue(T0, base + sH1, kTileM, false, base + sW3, kHid, false, kHid, kHid);
-            umma::commit(&bar);
-        }
-        if (!after_commit(&bar, phase, status)) break;
-        hidden(T0, sbias + 2 * kHid);
-        before_issue();
-        if (threadIdx.x == 0) {
-            issue(T1, base + sH1, kTileM, false, base + sW4, kOutP, false, kOutP, kHid);
-            umma::commit(&bar);
-        }
-        if (!after_commit(&bar, phase, status)) break;
-        if (q == 0) {
+        if (!layer(xo, sW1, kHid, kIn)) break;
+        hidden(sbias);
+        if (!layer(ho, sW2, kHid, kHid)) break;
+        hidden(sbias + kHid);
+        if (!layer(ho, sW3, kHid, kHid)) break;
+        hidden(sbias + 2 * kHid);
+        if (!layer(ho, sW4, kOutP, kHid)) break;
+        if (half == 0) {
             float v[16];
-            umma::ld16(umma::lane_addr(T1, 0), v);
+            umma::ld16(umma::lane_addr(T, 0), v);
             if (p < n) {
 #pragma unroll
                 for (int o = 0; o < kOut; ++o) y[p * kOut + o] = v[o] + sbias[3 * kHid + o];
@@ -647,7 +690,8 @@ int gsph_mlp_forward(gsph_mlp* m, const float* x, float* y, int64_t n, void* str
     if (n == 0) return GSPH_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int64_t tiles = (n + kTileM - 1) / kTileM;
-    const int grid = static_cast<int>(tiles < m->grid ? tiles : m->grid);
+    const int64_t pairs = (tiles + kSlots - 1) / kSlots;  // a CTA takes kSlots tiles at a time
+    const int grid = static_cast<int>(pairs < m->grid ? pairs : m->grid);
     k_mlp_forward<<<grid, kFwdThreads, kFwdSmem, s>>>(x, y, n, m->wq, m->bq, m->status);
     MLP_CK(m, cudaGetLastError(), "forward launch");
     return GSPH_OK;

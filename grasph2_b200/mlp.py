@@ -53,7 +53,19 @@ class MLP:
         if rc != 0:
             raise GsphError(rc, self.lib.gsph_last_error(None).decode())
 
+    @classmethod
+    def borrow(cls, handle, owner):
+        """A view of an MLP owned by another native object (`owner` is kept alive; close() is a no-op)."""
+        self = cls.__new__(cls)
+        self.lib = load_library()
+        self.count = int(self.lib.gsph_mlp_param_count())
+        self._h = ctypes.c_void_p(handle)
+        self._owner = owner
+        return self
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            return
         if self._h:
             self.lib.gsph_mlp_destroy(self._h)
             self._h = ctypes.c_void_p()

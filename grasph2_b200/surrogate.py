@@ -25,10 +25,12 @@ import time
 
 import numpy as np
 
+from ._abi import SurrogateWindow, load_library
 from .mlp import MLP
-from .sim import _stream_handle
+from .sim import GsphError, _stream_handle
 
 NF, NO = 32, 13
+NSTATS = 2 * NF + 2 * NO
 OUT_NAMES = ["dx", "dy", "dz", "dvx", "dvy", "dvz", "drho", "dSxx", "dSyy", "dSzz", "dSxy", "dSxz", "dSyz"]
 
 
@@ -39,6 +41,10 @@ def _torch():
 
 def _p(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
 def features(pb, mu=None, sig=None, out=None, stream=None):
@@ -113,41 +119,74 @@ def collect(pb, nwin, K, rows, rng, every=1, stream=None):
 
 
 class Surrogate:
-    """MLP + standardisation of its inputs and outputs + the substep count K."""
+    """The native surrogate (gsph_surrogate_*): its MLP, the standardisation of the MLP's inputs and
+    outputs, and the substep count K. `net` is a view of the surrogate's own MLP (train it in place)."""
 
-    def __init__(self, K=8, params=None, in_mu=None, in_sig=None, out_mu=None, out_sig=None):
+    def __init__(self, K=8, params=None, in_mu=None, in_sig=None, out_mu=None, out_sig=None, _handle=None):
         torch = _torch()
-        self.K = int(K)
-        self.net = MLP(params)
-        z = lambda k: np.zeros(k, np.float32)  # noqa: E731
-        o = lambda k: np.ones(k, np.float32)  # noqa: E731
-        self.stats = {"in_mu": in_mu if in_mu is not None else z(NF), "in_sig": in_sig if in_sig is not None else o(NF),
-                      "out_mu": out_mu if out_mu is not None else z(NO),
-                      "out_sig": out_sig if out_sig is not None else o(NO)}
-        self.dev = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).cuda() for k, v in self.stats.items()}
-        self._feat = self._out = None
+        self.lib = load_library()
+        if _handle is None:
+            count = int(self.lib.gsph_mlp_param_count())
+            arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32).ravel()
+                    for a in (params, in_mu, in_sig, out_mu, out_sig)]
+            for a, k in zip(arrs, (count, NF, NF, NO, NO)):
+                if a is not None and a.shape != (k,):
+                    raise ValueError("surrogate arrays must have %d, %d, %d, %d and %d values" % (count, NF, NF, NO, NO))
+            _handle = ctypes.c_void_p()
+            rc = self.lib.gsph_surrogate_create(*[_fp(a) for a in arrs], int(K), ctypes.byref(_handle))
+            if rc != 0:
+                raise GsphError(rc, self.lib.gsph_last_error(None).decode())
+        self._h = _handle
+        self.K = int(self.lib.gsph_surrogate_substeps(self._h))
+        self.net = MLP.borrow(self.lib.gsph_surrogate_mlp(self._h), self)
+        st = np.empty(NSTATS, dtype=np.float32)
+        self._check(self.lib.gsph_surrogate_stats(self._h, _fp(st)))
+        self.stats = {"in_mu": st[:NF], "in_sig": st[NF:2 * NF], "out_mu": st[2 * NF:2 * NF + NO],
+                      "out_sig": st[2 * NF + NO:]}
+        self.dev = {k: torch.from_numpy(v.copy()).cuda() for k, v in self.stats.items()}
+
+    def _check(self, rc):
+        if rc != 0:
+            raise GsphError(rc, self.lib.gsph_surrogate_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            self.lib.gsph_surrogate_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def save(self, path, **meta):
-        np.savez(path, params=self.net.params(), K=self.K, **self.stats, **meta)
+        """`.gsur`: the native model file (gsph_surrogate_save); otherwise an npz with `meta` beside."""
+        if str(path).endswith(".gsur"):
+            self._check(self.lib.gsph_surrogate_save(self._h, str(path).encode()))
+        else:
+            np.savez(path, params=self.net.params(), K=self.K, **self.stats, **meta)
 
     @classmethod
     def load(cls, path):
+        if str(path).endswith(".gsur"):
+            lib = load_library()
+            h = ctypes.c_void_p()
+            rc = lib.gsph_surrogate_load(str(path).encode(), ctypes.byref(h))
+            if rc != 0:
+                raise GsphError(rc, lib.gsph_last_error(None).decode())
+            return cls(_handle=h)
         z = np.load(path)
         return cls(int(z["K"]), z["params"], z["in_mu"], z["in_sig"], z["out_mu"], z["out_sig"])
 
     def propose(self, pb, use_net=True, stream=None):
-        """Advance pb by K substeps in one proposal."""
-        torch = _torch()
-        if self._feat is None or self._feat.shape[0] != pb.n:
-            self._feat = torch.empty(pb.n, NF, dtype=torch.float32, device="cuda")
-            self._out = torch.empty(pb.n, NO, dtype=torch.float32, device="cuda")
-        pb.compute_derivatives(stream)
-        if use_net:
-            features(pb, self.dev["in_mu"], self.dev["in_sig"], self._feat, stream)
-            self.net.forward(self._feat, self._out, pb.n, stream)
-            apply(pb, self.K, self._out, self.dev["out_mu"], self.dev["out_sig"], stream)
-        else:
-            apply(pb, self.K, None, None, None, stream)
+        """Advance pb by K substeps in one proposal (gsph_surrogate_propose)."""
+        self._check(self.lib.gsph_surrogate_propose(self._h, pb.handle, int(bool(use_net)), _stream_handle(stream)))
+
+    def launch_count(self):
+        c = ctypes.c_int64(0)
+        self._check(self.lib.gsph_surrogate_launch_count(self._h, ctypes.byref(c)))
+        return c.value
 
 
 def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, clip=0.0, stream=None):
@@ -190,20 +229,15 @@ def compare(pb, slot_p, slot_0, stream=None):
 
 
 def window_errors(pb, sur, use_net=True, e_ref=None, stream=None):
-    """One proposal and the plain K steps from the same state; returns (position error, relative energy
-    error). The position error is norm-wise over all particles, relative to the plain displacement:
-    ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2; the energy error is |E_proposal - E_plain| / |E|
-    (gsph_state_compare, O(N) on the device; E from the fast diagnostics unless e_ref is given). The
-    context ends on the plain result."""
-    if e_ref is None:
-        e_ref = _energy(pb.diagnostics(0.0, stream, fast=True))
-    snapshot(pb, 1, False, stream)
-    sur.propose(pb, use_net, stream)
-    snapshot(pb, 2, False, stream)
-    snapshot(pb, 1, True, stream)
-    pb.step(sur.K, stream)
-    de, dx2, d02, _ = compare(pb, 2, 1, stream)
-    return float(math.sqrt(dx2 / d02)) if d02 > 0 else float("inf"), float(abs(de) / abs(e_ref))
+    """One proposal and the plain K steps from the same state (gsph_surrogate_judge); returns (position
+    error, relative energy error). The position error is norm-wise over all particles, relative to the
+    plain displacement: ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2; the energy error is
+    |E_proposal - E_plain| / |E| (gsph_state_compare, O(N) on the device; E from the fast diagnostics
+    unless e_ref is given). The context ends on the plain result."""
+    w = SurrogateWindow()
+    sur._check(sur.lib.gsph_surrogate_judge(sur._h, pb.handle, int(bool(use_net)), float(e_ref or 0.0),
+                                            ctypes.byref(w), _stream_handle(stream)))
+    return w.pos_error, w.energy_error
 
 
 def _energy(d):
@@ -211,24 +245,17 @@ def _energy(d):
 
 
 def advance(pb, sur, nwin, M=4, pos_tol=1e-3, e_tol=1e-4, use_net=True, stream=None):
-    """nwin windows of M proposals (K substeps each), the last one judged against the plain integrator.
-    Returns a dict: substeps advanced, wall seconds, accepted windows, per-window errors."""
+    """nwin windows of M proposals (K substeps each), the last one judged against the plain integrator
+    (gsph_surrogate_advance). Returns a dict: substeps advanced, wall seconds, accepted windows,
+    per-window errors."""
     torch = _torch()
+    wins = (SurrogateWindow * max(1, nwin))()
+    acc = ctypes.c_int32(0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e_ref = _energy(pb.diagnostics(0.0, stream, fast=True))  # the scale of the energy criterion
-    acc, errs = 0, []
-    for _ in range(nwin):
-        snapshot(pb, 0, False, stream)
-        for _ in range(M - 1):
-            sur.propose(pb, use_net, stream)
-        ex, ee = window_errors(pb, sur, use_net, e_ref, stream)
-        errs.append((ex, ee))
-        if ex <= pos_tol and ee <= e_tol:
-            acc += 1
-        else:  # discard the window's proposals: plain integrator from the window's start
-            snapshot(pb, 0, True, stream)
-            pb.step(M * sur.K, stream)
+    sur._check(sur.lib.gsph_surrogate_advance(sur._h, pb.handle, int(nwin), int(M), float(pos_tol), float(e_tol),
+                                              int(bool(use_net)), wins, ctypes.byref(acc), _stream_handle(stream)))
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
-    return {"substeps": nwin * M * sur.K, "wall_s": wall, "accepted": acc, "windows": nwin, "errors": errs}
+    errs = [(wins[k].pos_error, wins[k].energy_error) for k in range(nwin)]
+    return {"substeps": nwin * M * sur.K, "wall_s": wall, "accepted": acc.value, "windows": nwin, "errors": errs}

@@ -7,8 +7,9 @@ Each trajectory is a two-sphere impact (radii 1 and 0.5, equal number density, N
 seeded relative velocity in [0.2, 1.0] and y-offset in [0, 0.8], advanced by the plain solver for
 windows x K substeps (K = 8); every `every`-th window contributes the features at its start and the
 K-step targets of `rows` random particles. The MLP is then fitted on the device by the project's own
-tensor-core forward/backward kernels and Adam. Writes the model (parameters, standardisation, K) and a
-summary of the run (collection and training times, loss history) next to it.
+tensor-core forward/backward kernels and Adam. Writes the model (parameters, standardisation, K) as an
+npz and as the native model file (.gsur, gsph_surrogate_load), and a summary of the run (collection and
+training times, loss history) next to them.
 """
 
 import argparse
@@ -72,6 +73,7 @@ def main(argv=None):
                 batch=a.batch, lr=a.lr, clip=a.clip, seed=a.seed, samples=int(X.shape[0]), collect_s=t_collect, fit_s=t_fit,
                 loss=[(int(s), float(l)) for s, l in hist])
     sur.save(a.out, meta=json.dumps(meta))
+    sur.save(os.path.splitext(a.out)[0] + ".gsur")  # the native model file (gsph_surrogate_load)
     with open(os.path.splitext(a.out)[0] + ".json", "w") as f:
         json.dump(meta, f, indent=1)
     print(json.dumps(meta))

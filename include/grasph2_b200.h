@@ -343,6 +343,49 @@ int gsph_snapshot(gsph_ctx* ctx, int32_t slot, int32_t restore, void* stream);
  * out[2] = sum |x_Q - x_0|^2; out[3] = E_kin + E_int + E_shear of Q. */
 int gsph_state_compare(gsph_ctx* ctx, int32_t slot_p, int32_t slot_0, double* out, void* stream);
 
+/* The learned surrogate as a native object (no counterpart in the reference): its MLP, the
+ * standardisation of the 32 inputs and 13 outputs, and K. A proposal advances a context by K substeps
+ * at once: gsph_compute_derivatives, gsph_surrogate_features (standardised), gsph_mlp_forward and
+ * gsph_surrogate_apply (use_net = 0: the extrapolation alone). A window is M proposals whose last one
+ * the plain integrator re-advances from the same state as judge; it is accepted when the proposal is
+ * within pos_tol of the plain result in position (norm over all particles, relative to the plain
+ * displacement) and within e_tol in total energy (relative to the energy at the start of the
+ * gsph_surrogate_advance call), and the state continues from the plain result; otherwise the window is
+ * re-run by the plain integrator from its start. Uses snapshot slots 0-2 of the context and
+ * synchronises `stream` once per window. Statistics (create's scale arrays; NULL means 0 for a mean and
+ * 1 for a sigma) and the model file hold, in order, in_mu[32], in_sigma[32], out_mu[13], out_sigma[13].
+ * Model file (little-endian): "GSPHSUR1", int32 K, int32 parameter count, the FP32 parameters, the 90
+ * FP32 statistics. */
+typedef struct gsph_surrogate gsph_surrogate;
+typedef struct gsph_surrogate_window {
+    double pos_error;     /* ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2 of the judged proposal */
+    double energy_error;  /* |E_proposal - E_plain| / |E_ref|                                        */
+    int32_t accepted;
+    int32_t reserved;
+} gsph_surrogate_window;
+#define GSPH_SURROGATE_STATS 90
+int gsph_surrogate_create(const float* params, const float* in_mu, const float* in_sigma, const float* out_mu,
+                          const float* out_sigma, int32_t K, gsph_surrogate** out);
+int gsph_surrogate_load(const char* path, gsph_surrogate** out);
+int gsph_surrogate_save(gsph_surrogate* s, const char* path);
+int gsph_surrogate_destroy(gsph_surrogate* s);
+/* the surrogate's own MLP (owned by it), e.g. to train it with gsph_mlp_gradient / gsph_mlp_adam */
+gsph_mlp* gsph_surrogate_mlp(gsph_surrogate* s);
+int32_t gsph_surrogate_substeps(const gsph_surrogate* s);
+/* the GSPH_SURROGATE_STATS statistics into stats (host) */
+int gsph_surrogate_stats(const gsph_surrogate* s, float* stats);
+int gsph_surrogate_propose(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, void* stream);
+/* one judged proposal from the current state; the context ends on the plain result. e_ref: the energy
+ * scale of out->energy_error, or 0 for the current total energy (gsph_diagnostics_fast) */
+int gsph_surrogate_judge(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, double e_ref, gsph_surrogate_window* out,
+                         void* stream);
+/* nwin windows; windows (nwin entries) and accepted may be NULL */
+int gsph_surrogate_advance(gsph_surrogate* s, gsph_ctx* ctx, int32_t nwin, int32_t M, double pos_tol, double e_tol,
+                           int32_t use_net, gsph_surrogate_window* windows, int32_t* accepted, void* stream);
+/* MLP forward launches made by the surrogate (the context counts its own kernels) */
+int gsph_surrogate_launch_count(const gsph_surrogate* s, int64_t* count);
+const char* gsph_surrogate_last_error(const gsph_surrogate* s);
+
 /* ---------------------------------------------------------------------------------------------
  * initial conditions on the device (the reference's particle sources, src/initialConditions/
  * particleSources/UniformSphere.cu, PlummerSphere.cu, and the centre-of-mass correction of

@@ -342,6 +342,41 @@ private:
     gsph_writer* w_ = nullptr;
 };
 
+// The learned K-substep surrogate (gsph_surrogate_*): load a trained model file and advance a buffer
+// by judged windows of proposals.
+class Surrogate {
+public:
+    explicit Surrogate(const std::string& modelFile) {
+        const int rc = gsph_surrogate_load(modelFile.c_str(), &s_);
+        if (rc != GSPH_OK) throw Error(rc, gsph_last_error(nullptr));
+    }
+    ~Surrogate() {
+        if (s_) gsph_surrogate_destroy(s_);
+    }
+    Surrogate(const Surrogate&) = delete;
+    Surrogate& operator=(const Surrogate&) = delete;
+    int substeps() const { return gsph_surrogate_substeps(s_); }
+    void propose(DeviceParticleBuffer& pb, bool useNet = true, void* stream = nullptr) {
+        chk(gsph_surrogate_propose(s_, pb.get(), useNet ? 1 : 0, stream));
+    }
+    // nwin windows of M proposals; returns the per-window errors and acceptance
+    std::vector<gsph_surrogate_window> advance(DeviceParticleBuffer& pb, int nwin, int M = 4, double posTol = 1e-3,
+                                               double energyTol = 1e-4, bool useNet = true, void* stream = nullptr) {
+        std::vector<gsph_surrogate_window> w(static_cast<size_t>(nwin));
+        chk(gsph_surrogate_advance(s_, pb.get(), nwin, M, posTol, energyTol, useNet ? 1 : 0, w.data(), nullptr,
+                                   stream));
+        return w;
+    }
+    void save(const std::string& modelFile) { chk(gsph_surrogate_save(s_, modelFile.c_str())); }
+    gsph_surrogate* get() { return s_; }
+
+private:
+    void chk(int rc) {
+        if (rc != GSPH_OK) throw Error(rc, gsph_surrogate_last_error(s_));
+    }
+    gsph_surrogate* s_ = nullptr;
+};
+
 // TextFile reader (src/initialConditions/particleSources/TextFile.h:76-120): non-blank lines are
 // particles, values separated by `sep`, the attributes in `mask` in particle_bases order.
 inline HostParticleBuffer readTextFile(const std::string& filename, uint32_t mask = kDefaultStoredAttributes,

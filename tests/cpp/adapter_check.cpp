@@ -108,6 +108,24 @@ int main(int argc, char** argv) {
             return 1;
         }
     }
+    if (argc > 2) {  // the learned surrogate from a model file: one judged window, then a save/load round trip
+        gsph_params q = p;
+        q.flags &= ~(GSPH_VARIABLE_TIMESTEP | GSPH_BALSARA_SWITCH);
+        gsph::DeviceParticleBuffer sb(q, n);
+        sb = hpb;
+        gsph::Surrogate sur(argv[2]);
+        const std::vector<gsph_surrogate_window> w = sur.advance(sb, 1, 2);
+        if (w.size() != 1 || !(w[0].pos_error >= 0) || !(w[0].energy_error >= 0)) {
+            std::printf("surrogate window failed\n");
+            return 1;
+        }
+        sur.save(tmp + "/model.gsur");
+        gsph::Surrogate back2(tmp + "/model.gsur");
+        if (back2.substeps() != sur.substeps()) {
+            std::printf("surrogate file round trip failed\n");
+            return 1;
+        }
+    }
     {  // per-particle host access with the reference's names
         gsph::Particle q = out.loadParticle(5);
         q.pos = q.pos + gsph::f3_t{1.0f, 0.0f, 0.0f};

@@ -20,6 +20,8 @@ def test_cpp_adapter_main_loop():
         subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
                         os.path.join(ROOT, "tests", "cpp", "adapter_check.cpp"), "-L", os.path.dirname(_abi.LIB_PATH),
                         "-lgrasph2_b200", "-Wl,-rpath," + os.path.dirname(_abi.LIB_PATH), "-o", exe], check=True)
-        r = subprocess.run([exe, d], capture_output=True, text=True, timeout=300)
+        model = os.path.join(ROOT, "grasph2_b200", "data", "surrogate_impact_n262144.gsur")
+        assert os.path.exists(model), model
+        r = subprocess.run([exe, d, model], capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stdout + r.stderr
         assert "ADAPTER OK" in r.stdout

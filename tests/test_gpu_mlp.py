@@ -54,7 +54,7 @@ def _blocks(g):
     return out
 
 
-@pytest.mark.parametrize("n", [1, 127, 128, 1000, 40000])
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 40000, 300001])
 def test_mlp_forward_vs_oracle(n):
     import torch
     from grasph2_b200.mlp import MLP

@@ -238,3 +238,70 @@ def test_surrogate_entry_points_reject_unsupported_contexts():
         assert e.value.code == -4
         with pytest.raises(GsphError):
             S.snapshot(pb, 9, False)  # no such slot
+
+
+def _quiet_surrogate(K=8, seed=3):
+    """A random network whose outputs are scaled to ~1e-7: proposals stay close to the extrapolation."""
+    from grasph2_b200.mlp import init_params
+    rng = np.random.default_rng(seed)
+    return S.Surrogate(K, init_params(seed), rng.normal(size=32) * 0.1, rng.uniform(0.5, 2.0, 32),
+                       np.zeros(13), np.full(13, 1e-7))
+
+
+def test_native_window_loop_matches_the_primitives():
+    """gsph_surrogate_advance with every window accepted equals the same window rule written out with
+    the public primitives (snapshots, proposals, plain steps, state comparison), bit for bit."""
+    nb, ns = 1800, 225
+    p = impact_params(nb, ns)
+    st = ics.two_sphere_impact(nb, ns, v_rel=0.5, y_offset=0.3, seed=11)
+    sur = _quiet_surrogate()
+    M, K, nwin = 3, sur.K, 2
+    with DeviceParticleBuffer(p, nb + ns) as a, DeviceParticleBuffer(p, nb + ns) as b:
+        a.upload(st)
+        b.upload(st)
+        r = S.advance(a, sur, nwin, M=M, pos_tol=1e30, e_tol=1e30)
+        e_ref = S._energy(b.diagnostics(0.0, fast=True))
+        want = []
+        for _ in range(nwin):
+            S.snapshot(b, 0, False)
+            for _ in range(M - 1):
+                sur.propose(b)
+            S.snapshot(b, 1, False)
+            sur.propose(b)
+            S.snapshot(b, 2, False)
+            S.snapshot(b, 1, True)
+            b.step(K)
+            de, dx2, d02, _ = S.compare(b, 2, 1)
+            want.append((np.sqrt(dx2 / d02), abs(de) / abs(e_ref)))
+        x, y = a.download(), b.download()
+        assert np.array_equal(a.download_pos64(), b.download_pos64())
+    assert r["accepted"] == nwin and r["substeps"] == nwin * M * K
+    for k in x:
+        np.testing.assert_array_equal(x[k], y[k], err_msg=k)
+    np.testing.assert_allclose(np.array(r["errors"]), np.array(want), rtol=1e-12)
+
+
+def test_surrogate_model_file_round_trip(tmp_path):
+    sur = _quiet_surrogate(K=6, seed=5)
+    f = str(tmp_path / "m.gsur")
+    sur.save(f)
+    back = S.Surrogate.load(f)
+    assert back.K == 6
+    np.testing.assert_array_equal(back.net.params(), sur.net.params())
+    for k in sur.stats:
+        np.testing.assert_array_equal(back.stats[k], sur.stats[k], err_msg=k)
+    g = str(tmp_path / "m.npz")
+    sur.save(g)
+    again = S.Surrogate.load(g)
+    np.testing.assert_array_equal(again.net.params(), sur.net.params())
+
+
+def test_committed_model_files_agree():
+    """The trained model ships as an npz (with its training summary) and as the native model file."""
+    import os
+    base = os.path.join(os.path.dirname(S.__file__), "data", "surrogate_impact_n262144")
+    a, b = S.Surrogate.load(base + ".npz"), S.Surrogate.load(base + ".gsur")
+    assert a.K == b.K == 8
+    np.testing.assert_array_equal(a.net.params(), b.net.params())
+    for k in a.stats:
+        np.testing.assert_array_equal(a.stats[k], b.stats[k], err_msg=k)
