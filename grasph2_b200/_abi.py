@@ -238,13 +238,18 @@ _SIGNATURES = {
                                               ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
     "gsph_surrogate_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_surrogate_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gsph_surrogate_set_energy_correction": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double]),
+    "gsph_surrogate_energy_bias": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "gsph_state_compare_parts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _dp,
+                                                ctypes.c_void_p]),
+    "gsph_energy_adjust": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
 }
 
 
 class SurrogateWindow(ctypes.Structure):
     """gsph_surrogate_window"""
-    _fields_ = [("pos_error", ctypes.c_double), ("energy_error", ctypes.c_double), ("accepted", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+    _fields_ = [("pos_error", ctypes.c_double), ("energy_error", ctypes.c_double),
+                ("energy_parts", ctypes.c_double * 4), ("accepted", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 def load_library(path=None):

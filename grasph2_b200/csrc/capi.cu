@@ -1126,7 +1126,11 @@ int gsph_launch_shape_get(gsph_ctx* c, gsph_launch_shape* out) {
     return GSPH_OK;
 }
 
-int gsph_state_compare(gsph_ctx* c, int32_t slot_p, int32_t slot_0, double* out, void* stream) {
+}  // extern "C"
+
+namespace {
+// gsph_state_compare and gsph_state_compare_parts: the first `nout` (<= 8) fields of k_state_compare
+int state_compare(gsph_ctx* c, int32_t slot_p, int32_t slot_0, double* out, int nout, void* stream) {
     if (!c || !out) return c ? fail(c, GSPH_E_INVALID, "out is NULL") : GSPH_E_INVALID;
     if (c->fp64) return fail(c, GSPH_E_UNSUPPORTED, "single precision only");
     if (slot_p < 0 || slot_p >= kSnapSlots || slot_0 < 0 || slot_0 >= kSnapSlots || c->snap[slot_p].empty() ||
@@ -1146,11 +1150,31 @@ int gsph_state_compare(gsph_ctx* c, int32_t slot_p, int32_t slot_0, double* out,
     cudaStream_t s = as_stream(stream);
     GSPH_CK(c, launch_state_compare(c->a, view(slot_p), view(slot_0), c->dp, c->a.diag, c->diag_out, s), "compare");
     c->launches += 2;
-    double h[4];
+    double h[8];
     GSPH_CK(c, cudaMemcpyAsync(h, c->diag_out, sizeof h, cudaMemcpyDeviceToHost, s), "compare read");
     const int rc = check_status(c, s);
     if (rc != GSPH_OK) return rc;
-    for (int k = 0; k < 4; ++k) out[k] = h[k];
+    for (int k = 0; k < nout; ++k) out[k] = h[k];
+    return GSPH_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int gsph_state_compare(gsph_ctx* c, int32_t slot_p, int32_t slot_0, double* out, void* stream) {
+    return state_compare(c, slot_p, slot_0, out, 4, stream);
+}
+
+int gsph_state_compare_parts(gsph_ctx* c, int32_t slot_p, int32_t slot_0, double* out, void* stream) {
+    return state_compare(c, slot_p, slot_0, out, 8, stream);
+}
+
+int gsph_energy_adjust(gsph_ctx* c, double d_kin, double d_shear, void* stream) {
+    if (!c) return GSPH_E_INVALID;
+    if (c->fp64) return fail(c, GSPH_E_UNSUPPORTED, "single precision only");
+    if (!std::isfinite(d_kin) || !std::isfinite(d_shear)) return fail(c, GSPH_E_INVALID, "energy changes must be finite");
+    GSPH_CK(c, launch_energy_adjust(c->a, c->dp, d_kin, d_shear, c->diag_out, as_stream(stream)), "energy adjust");
+    c->launches += 3;
     return GSPH_OK;
 }
 

@@ -185,10 +185,11 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_fast(DevArrays a, DevPara
 //      exactly, the gravitational energy change to first order in the position difference, g = the
 //      gravitational acceleration of Q's last derivative evaluation)
 //   1: sum_i |x_P,i - x_Q,i|^2      2: sum_i |x_Q,i - x_0,i|^2      3: E_local(Q)
+//   4-7: the parts of field 0: kinetic, internal, shear, first-order gravitational
 __global__ void __launch_bounds__(kDiagThreads) k_state_compare(DevArrays q, DevArrays pv, DevArrays x0, DevParams p) {
     __shared__ double red[32];
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    double f[4] = {0.0, 0.0, 0.0, 0.0};
+    double f[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i < q.n) {
         double fq[kDiagFields], fp[kDiagFields];
 #pragma unroll
@@ -210,11 +211,67 @@ __global__ void __launch_bounds__(kDiagThreads) k_state_compare(DevArrays q, Dev
         f[1] = dx2;
         f[2] = d02;
         f[3] = eq;
+        f[4] = fp[0] - fq[0];
+        f[5] = fp[2] - fq[2];
+        f[6] = fp[3] - fq[3];
+        f[7] = -static_cast<double>(q.posm[i].w) * dg;
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 8; ++k) {
         const double sum = block_sum(f[k], red);
         if (threadIdx.x == 0) q.diag[static_cast<int64_t>(blockIdx.x) * kDiagFields + k] = sum;
+    }
+}
+
+// Energy adjustment (gsph_energy_adjust): block partials of m, m v, 1/2 m v^2 and the shear energy ...
+__global__ void __launch_bounds__(kDiagThreads) k_energy_parts(DevArrays a, DevParams p) {
+    __shared__ double red[32];
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double f[kDiagFields];
+#pragma unroll
+    for (int k = 0; k < kDiagFields; ++k) f[k] = 0.0;
+    if (i < a.n) diag_terms(a, p, i, 0.0, f);
+    const double g[6] = {f[10], f[4], f[5], f[6], f[0], f[3]};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double sum = block_sum(g[k], red);
+        if (threadIdx.x == 0) a.diag[static_cast<int64_t>(blockIdx.x) * kDiagFields + k] = sum;
+    }
+}
+
+// ... then, from the totals: peculiar velocities scaled about the centre-of-mass velocity by
+// lambda_v = sqrt(1 + d_kin / E_kin,com) and the deviatoric stress by lambda_s = sqrt(1 + d_shear / E_shear)
+// (each factor limited to [0.9, 1.1]; 1 when its energy is zero), then the plasticity limiter of the
+// integrator. Momentum is unchanged; the kinetic energy changes by d_kin exactly, the shear energy by
+// d_shear unless the limiter clips a particle.
+__global__ void k_energy_adjust(DevArrays a, DevParams p, const double* __restrict__ tot, double d_kin,
+                                double d_shear) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double M = tot[0];
+    const double vc[3] = {M > 0 ? tot[1] / M : 0.0, M > 0 ? tot[2] / M : 0.0, M > 0 ? tot[3] / M : 0.0};
+    const double ekc = tot[4] - 0.5 * M * (vc[0] * vc[0] + vc[1] * vc[1] + vc[2] * vc[2]);
+    auto factor = [](double e, double d) {
+        if (!(e > 0.0)) return 1.0;
+        return fmin(1.1, fmax(0.9, sqrt(fmax(0.0, 1.0 + d / e))));
+    };
+    const double lv = factor(ekc, d_kin), ls = factor(tot[5], d_shear);
+    float4 vr = a.velrho[i];
+    vr.x = static_cast<float>(vc[0] + lv * (static_cast<double>(vr.x) - vc[0]));
+    vr.y = static_cast<float>(vc[1] + lv * (static_cast<double>(vr.y) - vc[1]));
+    vr.z = static_cast<float>(vc[2] + lv * (static_cast<double>(vr.z) - vc[2]));
+    a.velrho[i] = vr;
+    if (has(p, GSPH_SPH) && has(p, GSPH_SOLIDS) && ls != 1.0) {
+        const float f = static_cast<float>(ls);
+        float4 sa = a.sA[i], sb = a.sB[i];
+        sa.x *= f; sa.y *= f; sa.z *= f; sa.w *= f;
+        sb.x *= f; sb.y *= f;
+        if (has(p, GSPH_PLASTICITY_MC))
+            plasticity(sa, sb, p.tanfr * murnaghan(p, vr.w) + p.cohesion);
+        else if (has(p, GSPH_PLASTICITY_MIESE))
+            plasticity(sa, sb, p.Y);
+        a.sA[i] = sa;
+        a.sB[i] = sb;
     }
 }
 
@@ -394,6 +451,19 @@ cudaError_t launch_state_compare(const DevArrays& q, const DevArrays& p_state, c
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_diag_reduce<<<1, 32, 0, s>>>(qq, static_cast<int>(nb), out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_adjust(const DevArrays& a, const DevParams& p, double d_kin, double d_shear, double* tot_dev,
+                                 cudaStream_t s) {
+    const unsigned nb = blocks_for(a.n, kDiagThreads);
+    k_energy_parts<<<nb, kDiagThreads, 0, s>>>(a, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_diag_reduce<<<1, 32, 0, s>>>(a, static_cast<int>(nb), tot_dev);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_energy_adjust<<<nb, kDiagThreads, 0, s>>>(a, p, tot_dev, d_kin, d_shear);
     return cudaGetLastError();
 }
 

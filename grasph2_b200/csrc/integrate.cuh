@@ -16,6 +16,10 @@ cudaError_t launch_diagnostics_fast(const DevArrays& a, const DevParams& p, doub
 // O(N) comparison of the current state with two saved states (gsph_state_compare); out_dev: 4 doubles
 cudaError_t launch_state_compare(const DevArrays& q, const DevArrays& p_state, const DevArrays& x0, const DevParams& p,
                                  double* scratch, double* out_dev, cudaStream_t s);
+// gsph_energy_adjust: kinetic energy about the centre of mass and shear energy changed by d_kin and
+// d_shear (three launches; tot_dev: kDiagFields doubles of scratch)
+cudaError_t launch_energy_adjust(const DevArrays& a, const DevParams& p, double d_kin, double d_shear, double* tot_dev,
+                                 cudaStream_t s);
 // `ext` (nullable) maps each device slot to the caller's particle index
 cudaError_t launch_pack(const DevArrays& a, int attr, const float* src_dev, const int* ext, cudaStream_t s);
 cudaError_t launch_unpack(const DevArrays& a, int attr, float* dst_dev, const int* ext, cudaStream_t s);

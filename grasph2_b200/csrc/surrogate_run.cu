@@ -10,6 +10,14 @@
 // e_tol in total energy (relative to the energy scale e_ref); the state then continues from the plain
 // result. Otherwise the window's proposals are discarded and the window is re-run by the plain
 // integrator from its start (snapshot slot 0). Slots 1 and 2 hold the judge's start and proposal.
+//
+// Energy correction (optional): an MSE-trained network under-predicts the spread of what it cannot
+// predict, so its proposals lose a little kinetic and shear energy against the plain integrator, the
+// same way every time; over many windows that bias adds up although each judged proposal passes. With
+// the correction on, every proposal is followed by gsph_energy_adjust(-b_kin, -b_shear), and every
+// judged window whose position error passes updates the estimates from the judge's own comparison:
+// b += gain * (E_P - E_Q) per part. The judged proposal is corrected like the others, so the judge
+// measures the residual bias and checks the corrected method.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -38,6 +46,9 @@ struct gsph_surrogate {
     float* out = nullptr;      // [cap][13]
     int64_t cap = 0;
     int64_t launches = 0;      // MLP forward launches
+    bool ecorr = false;        // energy correction
+    double gain = 0.5;
+    double bias[2] = {0.0, 0.0};  // estimated kinetic and shear energy bias of one proposal
     std::string err;
 };
 
@@ -74,6 +85,13 @@ int reserve(gsph_surrogate* s, int64_t n) {
     if (e != cudaSuccess) return sfail(s, GSPH_E_NOMEM, std::string("surrogate buffers: ") + cudaGetErrorString(e));
     s->cap = n;
     return GSPH_OK;
+}
+
+// the energy correction after a proposal (nothing when off or before the first estimate)
+int correct(gsph_surrogate* s, gsph_ctx* ctx, void* stream) {
+    if (!s->ecorr || (s->bias[0] == 0.0 && s->bias[1] == 0.0)) return GSPH_OK;
+    const int rc = gsph_energy_adjust(ctx, -s->bias[0], -s->bias[1], stream);
+    return rc == GSPH_OK ? GSPH_OK : ctx_fail(s, ctx, rc, "propose: energy correction");
 }
 
 }  // namespace
@@ -176,7 +194,8 @@ int gsph_surrogate_propose(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, vo
     if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: derivatives");
     if (!use_net) {
         rc = gsph_surrogate_apply(ctx, nullptr, nullptr, nullptr, s->K, stream);
-        return rc == GSPH_OK ? GSPH_OK : ctx_fail(s, ctx, rc, "propose: apply");
+        if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: apply");
+        return correct(s, ctx, stream);
     }
     int64_t n = 0;
     gsph_size(ctx, &n);
@@ -188,7 +207,8 @@ int gsph_surrogate_propose(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, vo
     if (rc != GSPH_OK) return sfail(s, rc, std::string("propose: MLP: ") + gsph_mlp_last_error(s->net));
     ++s->launches;
     rc = gsph_surrogate_apply(ctx, s->out, s->stats + 2 * kIn, s->stats + 2 * kIn + kOut, s->K, stream);
-    return rc == GSPH_OK ? GSPH_OK : ctx_fail(s, ctx, rc, "propose: apply");
+    if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: apply");
+    return correct(s, ctx, stream);
 }
 
 int gsph_surrogate_judge(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, double e_ref, gsph_surrogate_window* out,
@@ -206,10 +226,11 @@ int gsph_surrogate_judge(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, doub
     if ((rc = gsph_snapshot(ctx, 2, 0, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: snapshot");
     if ((rc = gsph_snapshot(ctx, 1, 1, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: restore");
     if ((rc = gsph_step(ctx, s->K, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: plain steps");
-    double c[4];
-    if ((rc = gsph_state_compare(ctx, 2, 1, c, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: compare");
+    double c[8];
+    if ((rc = gsph_state_compare_parts(ctx, 2, 1, c, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: compare");
     out->pos_error = c[2] > 0.0 ? std::sqrt(c[1] / c[2]) : HUGE_VAL;
     out->energy_error = std::fabs(c[0]) / std::fabs(e_ref);
+    for (int k = 0; k < 4; ++k) out->energy_parts[k] = c[4 + k] / std::fabs(e_ref);
     out->accepted = 0;
     out->reserved = 0;
     return GSPH_OK;
@@ -230,6 +251,10 @@ int gsph_surrogate_advance(gsph_surrogate* s, gsph_ctx* ctx, int32_t nwin, int32
         gsph_surrogate_window r;
         if ((rc = gsph_surrogate_judge(s, ctx, use_net, e_ref, &r, stream)) != GSPH_OK) return rc;
         r.accepted = (r.pos_error <= pos_tol && r.energy_error <= e_tol) ? 1 : 0;
+        if (s->ecorr && r.pos_error <= pos_tol) {  // the judge's residual kinetic and shear bias
+            s->bias[0] += s->gain * r.energy_parts[0] * std::fabs(e_ref);
+            s->bias[1] += s->gain * r.energy_parts[2] * std::fabs(e_ref);
+        }
         if (r.accepted) {
             ++acc;
         } else {  // discard the window's proposals: the plain integrator from the window's start
@@ -239,6 +264,22 @@ int gsph_surrogate_advance(gsph_surrogate* s, gsph_ctx* ctx, int32_t nwin, int32
         if (windows) windows[w] = r;
     }
     if (accepted) *accepted = acc;
+    return GSPH_OK;
+}
+
+int gsph_surrogate_set_energy_correction(gsph_surrogate* s, int32_t on, double gain) {
+    if (!s) return GSPH_E_INVALID;
+    if (!(gain > 0.0 && gain <= 1.0)) return sfail(s, GSPH_E_INVALID, "gain must be in (0, 1]");
+    s->ecorr = on != 0;
+    s->gain = gain;
+    s->bias[0] = s->bias[1] = 0.0;
+    return GSPH_OK;
+}
+
+int gsph_surrogate_energy_bias(const gsph_surrogate* s, double* bias) {
+    if (!s || !bias) return GSPH_E_INVALID;
+    bias[0] = s->bias[0];
+    bias[1] = s->bias[1];
     return GSPH_OK;
 }
 

@@ -17,6 +17,11 @@ window from the same state as judge. The window is accepted when the proposal is
 the plain result in position (relative to the plain displacement over the K substeps) and within
 e_tol in total energy; the state then continues from the plain result. Otherwise every proposal of
 the window is discarded and the window is re-run with the plain integrator from its start.
+
+Surrogate.energy_correction() turns on the judge-calibrated energy correction: the network's
+proposals lose a little kinetic and shear energy against the plain integrator, the same way each
+time, so every proposal is followed by gsph_energy_adjust with running estimates of that bias, which
+every judged window updates from its own comparison.
 """
 
 import ctypes
@@ -183,6 +188,16 @@ class Surrogate:
         """Advance pb by K substeps in one proposal (gsph_surrogate_propose)."""
         self._check(self.lib.gsph_surrogate_propose(self._h, pb.handle, int(bool(use_net)), _stream_handle(stream)))
 
+    def energy_correction(self, on=True, gain=0.5):
+        """Judge-calibrated energy correction (gsph_surrogate_set_energy_correction); resets the estimates."""
+        self._check(self.lib.gsph_surrogate_set_energy_correction(self._h, int(bool(on)), float(gain)))
+
+    def energy_bias(self):
+        """The running estimates of one proposal's kinetic and shear energy bias."""
+        b = (ctypes.c_double * 2)()
+        self._check(self.lib.gsph_surrogate_energy_bias(self._h, b))
+        return b[0], b[1]
+
     def launch_count(self):
         c = ctypes.c_int64(0)
         self._check(self.lib.gsph_surrogate_launch_count(self._h, ctypes.byref(c)))
@@ -221,11 +236,19 @@ def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=Non
     return sur, hist
 
 
-def compare(pb, slot_p, slot_0, stream=None):
-    """gsph_state_compare: (E(P) - E(Q), sum |x_P - x_Q|^2, sum |x_Q - x_0|^2, local energy of Q)."""
-    out = (ctypes.c_double * 4)()
-    pb._check(pb.lib.gsph_state_compare(pb.handle, int(slot_p), int(slot_0), out, _stream_handle(stream)))
+def compare(pb, slot_p, slot_0, stream=None, parts=False):
+    """gsph_state_compare: (E(P) - E(Q), sum |x_P - x_Q|^2, sum |x_Q - x_0|^2, local energy of Q); with
+    parts, gsph_state_compare_parts: the same followed by the kinetic, internal, shear and first-order
+    gravitational parts of E(P) - E(Q)."""
+    out = (ctypes.c_double * (8 if parts else 4))()
+    f = pb.lib.gsph_state_compare_parts if parts else pb.lib.gsph_state_compare
+    pb._check(f(pb.handle, int(slot_p), int(slot_0), out, _stream_handle(stream)))
     return tuple(out)
+
+
+def energy_adjust(pb, d_kin, d_shear, stream=None):
+    """gsph_energy_adjust: change the kinetic energy about the centre of mass and the shear energy."""
+    pb._check(pb.lib.gsph_energy_adjust(pb.handle, float(d_kin), float(d_shear), _stream_handle(stream)))
 
 
 def window_errors(pb, sur, use_net=True, e_ref=None, stream=None):
@@ -258,4 +281,6 @@ def advance(pb, sur, nwin, M=4, pos_tol=1e-3, e_tol=1e-4, use_net=True, stream=N
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     errs = [(wins[k].pos_error, wins[k].energy_error) for k in range(nwin)]
-    return {"substeps": nwin * M * sur.K, "wall_s": wall, "accepted": acc.value, "windows": nwin, "errors": errs}
+    parts = [tuple(wins[k].energy_parts) for k in range(nwin)]
+    return {"substeps": nwin * M * sur.K, "wall_s": wall, "accepted": acc.value, "windows": nwin, "errors": errs,
+            "energy_parts": parts, "accepted_mask": [bool(wins[k].accepted) for k in range(nwin)]}

@@ -342,6 +342,15 @@ int gsph_snapshot(gsph_ctx* ctx, int32_t slot, int32_t restore, void* stream);
  * gravitational acceleration of Q's last derivative evaluation); out[1] = sum |x_P - x_Q|^2;
  * out[2] = sum |x_Q - x_0|^2; out[3] = E_kin + E_int + E_shear of Q. */
 int gsph_state_compare(gsph_ctx* ctx, int32_t slot_p, int32_t slot_0, double* out, void* stream);
+/* The same with out[4..7] = the parts of out[0]: kinetic, internal, shear, and first-order
+ * gravitational energy of P minus Q. */
+int gsph_state_compare_parts(gsph_ctx* ctx, int32_t slot_p, int32_t slot_0, double* out, void* stream);
+/* Change the kinetic energy about the centre of mass by d_kin and the shear energy by d_shear (no
+ * counterpart in the reference; the surrogate's energy correction): peculiar velocities are scaled
+ * about the centre-of-mass velocity and the deviatoric stress is scaled (each factor limited to
+ * [0.9, 1.1]), then the plasticity limiter of the integrator runs. Momentum and positions are
+ * unchanged. Asynchronous on `stream` (three launches). */
+int gsph_energy_adjust(gsph_ctx* ctx, double d_kin, double d_shear, void* stream);
 
 /* The learned surrogate as a native object (no counterpart in the reference): its MLP, the
  * standardisation of the 32 inputs and 13 outputs, and K. A proposal advances a context by K substeps
@@ -358,8 +367,10 @@ int gsph_state_compare(gsph_ctx* ctx, int32_t slot_p, int32_t slot_0, double* ou
  * FP32 statistics. */
 typedef struct gsph_surrogate gsph_surrogate;
 typedef struct gsph_surrogate_window {
-    double pos_error;     /* ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2 of the judged proposal */
-    double energy_error;  /* |E_proposal - E_plain| / |E_ref|                                        */
+    double pos_error;        /* ||x_proposal - x_plain||_2 / ||x_plain - x_start||_2 of the judged proposal */
+    double energy_error;     /* |E_proposal - E_plain| / |E_ref|                                        */
+    double energy_parts[4];  /* signed (E_proposal - E_plain) / |E_ref|: kinetic, internal, shear,
+                                gravitational (first order)                                             */
     int32_t accepted;
     int32_t reserved;
 } gsph_surrogate_window;
@@ -382,6 +393,16 @@ int gsph_surrogate_judge(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, doub
 /* nwin windows; windows (nwin entries) and accepted may be NULL */
 int gsph_surrogate_advance(gsph_surrogate* s, gsph_ctx* ctx, int32_t nwin, int32_t M, double pos_tol, double e_tol,
                            int32_t use_net, gsph_surrogate_window* windows, int32_t* accepted, void* stream);
+/* Energy correction calibrated by the judge (off by default). An MSE-trained network loses a little
+ * kinetic and shear energy in every proposal, the same way each time, which adds up over many windows
+ * although each judged proposal passes. With it on, every proposal is followed by
+ * gsph_energy_adjust(ctx, -b_kin, -b_shear) with the surrogate's running estimates b of one proposal's
+ * bias, and every judged window whose position error is within pos_tol updates them from the judge's
+ * comparison: b += gain * (E_proposal - E_plain) of each part (the judged proposal is corrected too, so
+ * that is the residual). gain in (0, 1]; setting resets the estimates to zero. */
+int gsph_surrogate_set_energy_correction(gsph_surrogate* s, int32_t on, double gain);
+/* bias[2]: the current estimates (kinetic, shear; energy units) */
+int gsph_surrogate_energy_bias(const gsph_surrogate* s, double* bias);
 /* MLP forward launches made by the surrogate (the context counts its own kernels) */
 int gsph_surrogate_launch_count(const gsph_surrogate* s, int64_t* count);
 const char* gsph_surrogate_last_error(const gsph_surrogate* s);

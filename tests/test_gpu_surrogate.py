@@ -305,3 +305,72 @@ def test_committed_model_files_agree():
     np.testing.assert_array_equal(a.net.params(), b.net.params())
     for k in a.stats:
         np.testing.assert_array_equal(a.stats[k], b.stats[k], err_msg=k)
+
+
+def test_energy_adjust_changes_the_requested_energies():
+    """gsph_energy_adjust: kinetic energy about the centre of mass and shear energy change by the requested
+    amounts; momentum and positions do not change."""
+    nb, ns = 7282, 910
+    p = impact_params(nb, ns)
+    st = solid_state(nb + ns, 21)
+    st["vel"] += np.array([0.3, -0.1, 0.05])  # a bulk velocity, kept by the adjustment
+    with DeviceParticleBuffer(p, nb + ns) as pb:
+        pb.upload(st)
+        d0 = pb.diagnostics(0.0)
+        x0 = pb.download_pos64()
+        P0, M = np.array(d0["momentum"]), d0["mass"]
+        ekc = d0["e_kin"] - P0 @ P0 / (2 * M)
+        dk, ds = -0.01 * ekc, -0.02 * d0["e_shear"]  # decreases: the limiter cannot clip
+        S.energy_adjust(pb, dk, ds)
+        d1 = pb.diagnostics(0.0)
+        x1 = pb.download_pos64()
+    np.testing.assert_array_equal(x0, x1)
+    P1 = np.array(d1["momentum"])
+    assert np.abs(P1 - P0).max() <= 1e-6 * np.abs(P0).max()
+    assert abs((d1["e_kin"] - d0["e_kin"]) - dk) <= 1e-4 * abs(dk), (d1["e_kin"] - d0["e_kin"], dk)
+    assert abs((d1["e_shear"] - d0["e_shear"]) - ds) <= 1e-4 * abs(ds), (d1["e_shear"] - d0["e_shear"], ds)
+    assert d1["e_int"] == d0["e_int"]
+
+
+def test_energy_correction_matches_the_primitives():
+    """With the energy correction on, gsph_surrogate_advance equals the rule written out with the
+    primitives: window 1 uncorrected, its judge's kinetic and shear parts update the estimates by
+    gain x part, and every proposal of window 2 is followed by gsph_energy_adjust(-estimates)."""
+    nb, ns = 1800, 225
+    p = impact_params(nb, ns)
+    st = ics.two_sphere_impact(nb, ns, v_rel=0.5, y_offset=0.3, seed=13)
+    sur = _quiet_surrogate()
+    M, K, gain = 3, sur.K, 0.5
+    with DeviceParticleBuffer(p, nb + ns) as a, DeviceParticleBuffer(p, nb + ns) as b:
+        a.upload(st)
+        b.upload(st)
+        sur.energy_correction(True, gain)
+        r = S.advance(a, sur, 2, M=M, pos_tol=1e30, e_tol=1e30)
+        got_bias = sur.energy_bias()
+        sur.energy_correction(False)
+        e_ref = S._energy(b.diagnostics(0.0, fast=True))
+        bias = [0.0, 0.0]
+
+        def propose():
+            sur.propose(b)
+            if bias != [0.0, 0.0]:
+                S.energy_adjust(b, -bias[0], -bias[1])
+
+        for _ in range(2):
+            S.snapshot(b, 0, False)
+            for _ in range(M - 1):
+                propose()
+            S.snapshot(b, 1, False)
+            propose()
+            S.snapshot(b, 2, False)
+            S.snapshot(b, 1, True)
+            b.step(K)
+            c = S.compare(b, 2, 1, parts=True)
+            bias[0] += gain * (c[4] / abs(e_ref)) * abs(e_ref)
+            bias[1] += gain * (c[6] / abs(e_ref)) * abs(e_ref)
+        x, y = a.download(), b.download()
+    assert r["accepted"] == 2
+    assert bias[0] != 0.0 and bias[1] != 0.0
+    assert got_bias == tuple(bias)
+    for k in x:
+        np.testing.assert_array_equal(x[k], y[k], err_msg=k)
