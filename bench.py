@@ -675,7 +675,7 @@ def run_surrogate(args, rank, world, local):
             pb.upload(st)
             pb.step(max(args.warmup, 1))
             if how is not None:
-                sur.energy_correction(how[1], 0.5)
+                sur.energy_correction(how[1], 1.0)
             torch.cuda.synchronize()
             l0 = pb.launch_count() + sur.launch_count()
             wall, acc, errs, series, done = 0.0, 0, [], [], 0

@@ -66,7 +66,8 @@ class GsphOptions(ctypes.Structure):
         ("accum", ctypes.c_int32), ("j_split", ctypes.c_int32), ("j_tile", ctypes.c_int32),
         ("i_per_thread", ctypes.c_int32), ("threads", ctypes.c_int32), ("check_finite", ctypes.c_int32),
         ("no_cull", ctypes.c_int32), ("resort_interval", ctypes.c_int32), ("scalar_fp32", ctypes.c_int32),
-        ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
+        ("precision", ctypes.c_int32), ("gravity_form", ctypes.c_int32), ("gravity_groups", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -82,7 +83,8 @@ _dp = ctypes.POINTER(ctypes.c_double)
 
 class GsphLaunchShape(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in ("cull", "grav_ipt", "grav_jt", "grav_nseg", "grav_x2", "sph_threads",
-                                               "sph_jt", "sph_nseg", "items")] + [("reserved", ctypes.c_int32 * 7)]
+                                               "sph_jt", "sph_nseg", "items", "grav_sym_groups")] + \
+        [("reserved", ctypes.c_int32 * 6)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

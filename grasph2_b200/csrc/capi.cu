@@ -415,6 +415,9 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (o.accum != GSPH_ACCUM_PLAIN && o.accum != GSPH_ACCUM_COMPENSATED)
         return fail(nullptr, GSPH_E_INVALID, "options.accum must be GSPH_ACCUM_PLAIN or GSPH_ACCUM_COMPENSATED");
     if (o.j_tile && !is_pow2_in(o.j_tile, 64, 1024)) return fail(nullptr, GSPH_E_INVALID, "j_tile: power of 2 in [64,1024]");
+    if (o.gravity_form < GSPH_GRAVITY_AUTO || o.gravity_form > GSPH_GRAVITY_SYMMETRIC || o.gravity_groups < 0 ||
+        o.gravity_groups > 1024)
+        return fail(nullptr, GSPH_E_INVALID, "options.gravity_form must be a GSPH_GRAVITY_* value, gravity_groups in [0, 1024]");
     if (o.threads && o.threads != 64 && o.threads != 128 && o.threads != 256)
         return fail(nullptr, GSPH_E_INVALID, "threads: 64, 128 or 256");
     if (o.i_per_thread && o.i_per_thread != 1 && o.i_per_thread != 2 && o.i_per_thread != 4 && o.i_per_thread != 8)
@@ -475,6 +478,12 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         const int slots = c->sm_count * gravity_blocks_per_sm(L.grav_ipt, L.grav_threads, L.grav_jt, comp);
         L.grav_nseg = o.j_split ? std::min(o.j_split, gcap)
                                 : pick_split(n_pad / (int64_t(L.grav_threads) * L.grav_ipt), slots, gcap);
+        // the symmetric form: enough tasks (G(G+1)/2 with G up to 64) to fill the GPU twice
+        const int64_t nblocks = n_pad / 1024;
+        const bool sym = o.gravity_form == GSPH_GRAVITY_SYMMETRIC ||
+                         (o.gravity_form == GSPH_GRAVITY_AUTO && !o.scalar_fp32 && nblocks >= 24);
+        const bool own_kernel = !(p->flags & GSPH_SPH) || L.cull;  // gravity has a kernel of its own
+        if (sym && own_kernel && !c->fp64) sym_groups(nblocks, o.gravity_groups ? o.gravity_groups : 64, L.grav_sym_G, L.grav_sym_gs);
     }
 
     cudaError_t ae = cudaSuccess;
@@ -492,7 +501,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
-        L.item_grid = c->sm_count * 4;      // 56 KB of shared memory per block: 4 resident per SM
+        L.item_grid = c->sm_count * 4;      // 49 KB of shared memory and 120 registers per thread: 4 per SM
         L.density_grid = c->sm_count * 8;
         sp.item_target = 6 * L.item_grid;
         sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 2) * sizeof(int), ae));
@@ -505,6 +514,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         c->item_nb_items = cap;
         sp.item_nb = static_cast<int*>(dalloc(c, cap * kItemNb * kGroup * sizeof(int), ae));
         sp.item_nbcnt = static_cast<int*>(dalloc(c, cap * kGroup * sizeof(int), ae));
+        sp.item_nbover = static_cast<int*>(dalloc(c, cap * sizeof(int), ae));
         sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));
@@ -1010,6 +1020,7 @@ int gsph_autotune(gsph_ctx* c, int32_t reps, void* stream) {
                 for (int k = 0; k < 3; ++k) {
                     if (k > 0 && segs[k] == segs[k - 1]) continue;
                     Launch t = L;
+                    t.grav_sym_G = t.grav_sym_gs = 0;
                     t.grav_ipt = ip;
                     t.grav_jt = jt;
                     t.grav_nseg = segs[k];
@@ -1030,10 +1041,37 @@ int gsph_autotune(gsph_ctx* c, int32_t reps, void* stream) {
                 }
                 if (rc != GSPH_OK) break;
             }
+        // the symmetric form (unless one-sided was asked for) with 32, 64 and 128 groups at most
+        const int64_t nblocks = np / 1024;
+        const int form = c->opt.gravity_form;
+        if (rc == GSPH_OK && form != GSPH_GRAVITY_ONE_SIDED && (form == GSPH_GRAVITY_SYMMETRIC || nblocks >= 8)) {
+            int last_G = -1;
+            for (int target : {32, 64, 128}) {
+                Launch t = best;
+                sym_groups(nblocks, c->opt.gravity_groups ? c->opt.gravity_groups : target, t.grav_sym_G, t.grav_sym_gs);
+                if (t.grav_sym_G == last_G) continue;
+                last_G = t.grav_sym_G;
+                if (L.cull) rc = grow(c, &c->a.gpart, c->gpart_cap, gravity_partial_floats(t, np));
+                else rc = grow(c, &c->a.part, c->part_cap, partial_floats(c->dp, t, np));
+                if (rc != GSPH_OK) break;
+                float ms = 0.0f;
+                rc = time_ms(c, s, reps, [&]() {
+                    const cudaError_t e = L.cull ? launch_gravity_partials(c->a, c->dp, t, s) : launch_gravity(c->a, c->dp, t, s);
+                    return e == cudaSuccess ? GSPH_OK : cuda_fail(c, e, "autotune gravity");
+                }, ms);
+                if (rc != GSPH_OK) break;
+                if (ms < best_ms || form == GSPH_GRAVITY_SYMMETRIC && best.grav_sym_G == 0) {
+                    best_ms = ms;
+                    best = t;
+                }
+            }
+        }
         if (rc == GSPH_OK) {
             L.grav_ipt = best.grav_ipt;
             L.grav_jt = best.grav_jt;
             L.grav_nseg = best.grav_nseg;
+            L.grav_sym_G = best.grav_sym_G;
+            L.grav_sym_gs = best.grav_sym_gs;
         }
     }
     // 2. the SPH passes: work items of the culled kernels, or the all-pairs tile shape
@@ -1072,10 +1110,13 @@ int gsph_autotune(gsph_ctx* c, int32_t reps, void* stream) {
                 const size_t items = static_cast<size_t>(target_mult) * L.item_grid + ngroups;
                 rc = grow(c, &c->sp.item_part, c->item_cap, items * kk * kGroup);
                 if (rc == GSPH_OK && items > c->item_nb_items) {
-                    size_t cap_nb = c->item_nb_items * kItemNb * kGroup, cap_cnt = c->item_nb_items * kGroup;
+                    size_t cap_nb = c->item_nb_items * kItemNb * kGroup, cap_cnt = c->item_nb_items * kGroup,
+                           cap_over = c->item_nb_items;
                     rc = grow(c, reinterpret_cast<float**>(&c->sp.item_nb), cap_nb, items * kItemNb * kGroup);
                     if (rc == GSPH_OK)
                         rc = grow(c, reinterpret_cast<float**>(&c->sp.item_nbcnt), cap_cnt, items * kGroup);
+                    if (rc == GSPH_OK)
+                        rc = grow(c, reinterpret_cast<float**>(&c->sp.item_nbover), cap_over, items);
                     if (rc == GSPH_OK) c->item_nb_items = items;
                 }
                 if (rc != GSPH_OK) break;
@@ -1119,6 +1160,7 @@ int gsph_launch_shape_get(gsph_ctx* c, gsph_launch_shape* out) {
     out->grav_jt = c->L.grav_jt;
     out->grav_nseg = c->L.grav_nseg;
     out->grav_x2 = c->L.grav_x2;
+    out->grav_sym_groups = c->L.grav_sym_G;
     out->sph_threads = c->L.threads;
     out->sph_jt = c->L.jt;
     out->sph_nseg = c->L.nseg;

@@ -148,7 +148,11 @@ __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restri
         float* out = cv.part + static_cast<int64_t>(w) * (COMP ? 2 : 1) * kGroup + threadIdx.x;
         out[0] = rho_s;
         if (COMP) out[kGroup] = rho_c;
-        if (LISTS) cv.nbcnt[static_cast<int64_t>(w) * kGroup + threadIdx.x] = min(cnt, kItemNb + 1);
+        if (LISTS) {
+            cv.nbcnt[static_cast<int64_t>(w) * kGroup + threadIdx.x] = min(cnt, kItemNb + 1);
+            const int over = __syncthreads_or(cnt > kItemNb);  // the SPH passes read one flag per item
+            if (threadIdx.x == 0) cv.nbover[w] = over;
+        }
     }
 }
 
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(256) k_pairs(DevArrays a, DevParams p, int jt,
 // positions of those chunks through shared memory and lets every lane record the indices of its own
 // neighbours (kNbCap per lane, flushed early when a lane's list is nearly full); phase 2 walks the
 // per-lane lists and gathers each neighbour's records from L2, so the SPH terms run lane-dense.
-constexpr int kNbCap = 96;
+constexpr int kNbCap = 80;
 template <int PASS, bool SOLIDS, bool COMP>
 __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p, CullView cv) {
     constexpr uint32_t MASK = field_mask<PASS, false, SOLIDS>();
@@ -318,18 +322,20 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
 #pragma unroll
         for (int f = 0; f < F_COUNT; ++f) S.f[f] = C.f[f] = T.f[f] = 0.0f;
         float maxv = 0.0f;
-        // the density pass's neighbour lists of this item, when every lane's list is complete
-        int lcnt = cv.nb ? cv.nbcnt[static_cast<int64_t>(w) * kGroup + threadIdx.x] : kItemNb + 1;
-        if (!__syncthreads_or(lcnt > kItemNb)) {
+        // the density pass's neighbour lists of this item, when every lane's list is complete (one flag
+        // per item, so no block-wide vote: the warps of a block run through list items independently)
+        if (cv.nb && cv.nbover[w] == 0) {
+            const int lcnt = cv.nbcnt[static_cast<int64_t>(w) * kGroup + threadIdx.x];
             const int* lst = cv.nb + static_cast<int64_t>(w) * kItemNb * kGroup + threadIdx.x;
             const float4 zero = make_float4(0, 0, 0, 0);
-            int jn = lcnt > 0 ? lst[0] : 0;
-            float4 qn = a.posm[jn], vn = a.velrho[jn];
-            float4 an = DO_A ? a.jA[jn] : zero, bn = DO_A ? a.jB[jn] : zero;
-            for (int k = 0; k < lcnt; ++k) {  // software pipeline: neighbour k+1's records in flight
+            const int j0 = lcnt > 0 ? lst[0] : 0;
+            int jn = lcnt > 1 ? lst[kGroup] : 0;  // the index of neighbour k+1
+            float4 qn = a.posm[j0], vn = a.velrho[j0];
+            float4 an = DO_A ? a.jA[j0] : zero, bn = DO_A ? a.jB[j0] : zero;
+            // software pipeline: neighbour k+1's records and neighbour k+2's index in flight during k
+            for (int k = 0; k < lcnt; ++k) {
                 const float4 q = qn, vj = vn, ja = an, jb = bn;
                 if (k + 1 < lcnt) {
-                    jn = lst[(k + 1) * kGroup];
                     qn = a.posm[jn];
                     vn = a.velrho[jn];
                     if (DO_A) {
@@ -337,6 +343,7 @@ __global__ void __launch_bounds__(kGroup) k_pairs_items(DevArrays a, DevParams p
                         bn = a.jB[jn];
                     }
                 }
+                if (k + 2 < lcnt) jn = lst[(k + 2) * kGroup];
                 const float dx = q.x - I.pi.x, dy = q.y - I.pi.y, dz = q.z - I.pi.z;
                 const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
                 sph_neighbour<PASS, SOLIDS>(T, maxv, I, q.w, dx, dy, dz, r2, vj, ja, jb, p);
@@ -445,24 +452,52 @@ __device__ __forceinline__ float seg_sum(const PartView& v, int64_t i, int f) {
     return s;
 }
 
-// gravity partials of the separate all-pairs gravity kernel (culled path), summed like seg_sum
-template <bool COMP>
-__device__ __forceinline__ float gpart_sum(const DevArrays& a, int gnseg, int64_t i, int c) {
-    const int K = COMP ? 6 : 3;
-    if (COMP) {
-        double s = 0.0;
-        for (int k = 0; k < gnseg; ++k)
-            s += static_cast<double>(a.gpart[(k * K + c) * a.n_pad + i]) +
-                 static_cast<double>(a.gpart[(k * K + 3 + c) * a.n_pad + i]);
-        return static_cast<float>(s);
+// gravity partials of an all-pairs gravity kernel (component c of particle i), summed like seg_sum:
+// the one-sided kernel's segments 0 .. nseg-1, or the symmetric kernel's row slots g .. G-1 and then
+// column slots G .. G + g of the particle's group g
+__device__ __forceinline__ void gpart_slots(const GravSum& gs, int64_t i, int& r0, int& r1, int& c0, int& c1) {
+    r0 = 0; r1 = gs.nseg; c0 = c1 = 0;
+    if (gs.sym_G > 0) {
+        const int g = static_cast<int>(i / gs.sym_group);
+        r0 = g; r1 = gs.sym_G;
+        c0 = gs.sym_G; c1 = gs.sym_G + g + 1;
     }
-    float s = 0.0f;
-    for (int k = 0; k < gnseg; ++k) s += a.gpart[(k * K + c) * a.n_pad + i];
-    return s;
+}
+// slots k0 .. k1-1 of all three components at once, unrolled so that several slots' loads are in
+// flight (each component is still summed in slot order)
+template <typename T, bool COMP>
+__device__ __forceinline__ void gpart_range(const float* part, int64_t n_pad, int k0, int k1, int64_t i, T (&s)[3]) {
+    constexpr int K = COMP ? 6 : 3;
+#pragma unroll 4
+    for (int k = k0; k < k1; ++k) {
+        const float* q = part + static_cast<int64_t>(k) * K * n_pad + i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (COMP) s[c] += static_cast<T>(q[c * n_pad]) + static_cast<T>(q[(3 + c) * n_pad]);
+            else s[c] += static_cast<T>(q[c * n_pad]);
+        }
+    }
+}
+// the three components of particle i: FP64 sums of (sum + error) when compensated
+template <bool COMP>
+__device__ __forceinline__ void gpart_sum(const float* part, int64_t n_pad, const GravSum& gs, int64_t i, double (&out)[3]) {
+    int r0, r1, c0, c1;
+    gpart_slots(gs, i, r0, r1, c0, c1);
+    if (COMP) {
+        double s[3] = {0.0, 0.0, 0.0};
+        gpart_range<double, true>(part, n_pad, r0, r1, i, s);
+        gpart_range<double, true>(part, n_pad, c0, c1, i, s);
+        for (int c = 0; c < 3; ++c) out[c] = s[c];
+    } else {
+        float s[3] = {0.0f, 0.0f, 0.0f};
+        gpart_range<float, false>(part, n_pad, r0, r1, i, s);
+        gpart_range<float, false>(part, n_pad, c0, c1, i, s);
+        for (int c = 0; c < 3; ++c) out[c] = s[c];
+    }
 }
 
 template <int PASS, bool GRAV, bool SOLIDS, bool COMP>
-__global__ void k_pairs_finish(DevArrays a, DevParams p, PartView pv, int gnseg) {
+__global__ void k_pairs_finish(DevArrays a, DevParams p, PartView pv, GravSum gsum) {
     constexpr uint32_t MASK = field_mask<PASS, GRAV, SOLIDS>();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (PASS != PASS_VGRAD && has(p, GSPH_VARIABLE_TIMESTEP) && i == 0)
@@ -476,8 +511,10 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, PartView pv, int gnseg)
             g[1] = seg_sum<MASK, COMP>(pv, i, F_GY);
             g[2] = seg_sum<MASK, COMP>(pv, i, F_GZ);
             grav = true;
-        } else if (gnseg > 0) {
-            for (int c = 0; c < 3; ++c) g[c] = gpart_sum<COMP>(a, gnseg, i, c);
+        } else if (gsum.nseg > 0 || gsum.sym_G > 0) {
+            double t[3];
+            gpart_sum<COMP>(a.gpart, a.n_pad, gsum, i, t);
+            for (int c = 0; c < 3; ++c) g[c] = static_cast<float>(t[c]);
             grav = true;
         }
     }
@@ -586,6 +623,250 @@ __global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ p
         }
     }
 }
+// ================================================================================================
+// symmetric all-pairs gravity (Newton's third law): every unordered pair evaluated once
+// ================================================================================================
+// Particles form blocks of kSymB = 128 threads x 8; blocks form G groups of `gs` consecutive blocks.
+// CTA t is the task (ga, gb), ga <= gb (the G(G-1)/2 pairs of distinct groups first, then the G
+// diagonal ones): for every row block a of group ga it sweeps the column blocks of group gb (those
+// after a when ga == gb) in j-tiles of kSymJT through shared memory. One 1/r^3 serves both particles
+// of a pair: the row particle's sum stays in registers (f32x2, two row particles per instruction); the
+// column particle's contribution is summed over the CTA's 1024 row particles -- in the thread, then
+// across the warp by a butterfly that leaves kSymJB column sums spread over the lanes, then over the
+// four warps in shared memory -- and added to its slot in the partials (plain, or two-sum when
+// compensated). The pairs inside a block (the diagonal tile) run one-sided. Row sums go to slot gb and
+// column sums to slot G + ga, so each (slot, particle) has one writer; the finish kernels add a
+// particle's row slots g .. G-1, then its column slots G .. G + g (g its group), in that fixed order,
+// and results do not depend on scheduling. FMA-pipe work per pair interaction: 8 + ~0.4 operations
+// against the one-sided kernel's 12.
+constexpr int kSymT = 128, kSymI = 8, kSymB = kSymT * kSymI, kSymJT = 256;
+constexpr int kSymJB = 8;  // column particles per butterfly (8: 136 registers, three CTAs per SM; 4 fits four
+                           // CTAs but its longer butterflies cost more than the occupancy gains)
+
+// NV values per lane (NV = 4 or 8) -> lane l holds the warp's sum of value (l >> (5 - log2 NV)) & (NV - 1):
+// a butterfly that halves the values at each of the first log2 NV levels (fixed order, so the sums are
+// the same on every run)
+__device__ __forceinline__ void reduce_lanes(float (&v)[8], int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const float send = b4 ? v[m] : v[m + 4], keep = b4 ? v[m + 4] : v[m];
+        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const float send = b3 ? v[m] : v[m + 2], keep = b3 ? v[m + 2] : v[m];
+        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const float send = b2 ? v[0] : v[1], keep = b2 ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+__device__ __forceinline__ void reduce_lanes(float (&v)[4], int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const float send = b4 ? v[m] : v[m + 2], keep = b4 ? v[m + 2] : v[m];
+        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    const float send = b3 ? v[0] : v[1], keep = b3 ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 4);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
+
+__host__ __device__ __forceinline__ void sym_task(int t, int G, int& ga, int& gb) {
+    const int noff = G * (G - 1) / 2;
+    if (t >= noff) {
+        ga = gb = t - noff;
+        return;
+    }
+    int r = 0, rem = t;
+    while (rem >= G - 1 - r) {
+        rem -= G - 1 - r;
+        ++r;
+    }
+    ga = r;
+    gb = r + 1 + rem;
+}
+
+template <int GRAV, bool COMP>
+__global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict__ posm, float* __restrict__ part,
+                                                       int64_t n_pad, int G, int gs, float eps2) {
+    constexpr int P = kSymI / 2;
+    constexpr int K = COMP ? 6 : 3;
+    __shared__ float4 J[kSymJT];
+    __shared__ float js[kSymT / 32][kSymJT][3];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int ga, gb;
+    sym_task(static_cast<int>(blockIdx.x), G, ga, gb);
+    const int nb = static_cast<int>(n_pad / kSymB);
+    const int ra0 = ga * gs, ra1 = min(nb, ra0 + gs);
+    const int cg0 = gb * gs, cg1 = min(nb, cg0 + gs);
+    const bool diag = ga == gb;
+    float* Pi = part + static_cast<int64_t>(gb) * K * n_pad;
+    float* Pj = part + static_cast<int64_t>(G + ga) * K * n_pad;
+    if (diag)  // the group's first block is never a column here: its column slot is zero
+        for (int e = tid; e < kSymB; e += kSymT)
+            for (int c = 0; c < K; ++c) Pj[c * n_pad + static_cast<int64_t>(ra0) * kSymB + e] = 0.0f;
+    const float2 E2 = make_float2(eps2, eps2);
+
+    for (int a = ra0; a < ra1; ++a) {
+        const int64_t base = static_cast<int64_t>(a) * kSymB + tid;
+        float2 X[P], Y[P], Z[P], MI[P], AX[P], AY[P], AZ[P], CX[P], CY[P], CZ[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const float4 u = posm[base + static_cast<int64_t>(2 * k) * kSymT];
+            const float4 w = posm[base + static_cast<int64_t>(2 * k + 1) * kSymT];
+            X[k] = make_float2(u.x, w.x); Y[k] = make_float2(u.y, w.y); Z[k] = make_float2(u.z, w.z);
+            MI[k] = make_float2(-u.w, -w.w);
+            AX[k] = AY[k] = AZ[k] = make_float2(0.0f, 0.0f);
+            CX[k] = CY[k] = CZ[k] = make_float2(0.0f, 0.0f);
+        }
+        // tiles: the block's own (one-sided) when diagonal, then the columns
+        const int64_t d0 = static_cast<int64_t>(a) * kSymB;
+        const int nd = diag ? kSymB / kSymJT : 0;
+        const int64_t c0 = static_cast<int64_t>(diag ? a + 1 : cg0) * kSymB, c1 = static_cast<int64_t>(cg1) * kSymB;
+        const int nc = c1 > c0 ? static_cast<int>((c1 - c0) / kSymJT) : 0;
+        const int total = nd + nc;
+        const bool first = a == ra0;
+        auto src = [&](int k) { return k < nd ? d0 + static_cast<int64_t>(k) * kSymJT : c0 + static_cast<int64_t>(k - nd) * kSymJT; };
+        float4 pf0 = make_float4(0, 0, 0, 0), pf1 = pf0;
+        if (total > 0) {
+            pf0 = posm[src(0) + tid];
+            pf1 = posm[src(0) + kSymT + tid];
+        }
+        for (int k = 0; k < total; ++k) {
+            __syncthreads();  // the previous tile's reads of J and js are done
+            J[tid] = pf0;
+            J[tid + kSymT] = pf1;
+            __syncthreads();
+            if (k + 1 < total) {
+                pf0 = posm[src(k + 1) + tid];
+                pf1 = posm[src(k + 1) + kSymT + tid];
+            }
+            float2 TX[P], TY[P], TZ[P];
+#pragma unroll
+            for (int q = 0; q < P; ++q) TX[q] = TY[q] = TZ[q] = make_float2(0.0f, 0.0f);
+            if (k < nd) {  // one-sided, as k_gravity_x2
+#pragma unroll 4
+                for (int j = 0; j < kSymJT; ++j) {
+                    const float4 q = J[j];
+                    const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y), qz = make_float2(q.z, q.z),
+                                 qm = make_float2(q.w, q.w);
+#pragma unroll
+                    for (int m = 0; m < P; ++m) {
+                        const float2 dx = sub2(qx, X[m]), dy = sub2(qy, Y[m]), dz = sub2(qz, Z[m]);
+                        const float2 r2 = fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, E2)));
+                        float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                        if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
+                        const float2 sj = mul2(qm, mul2(mul2(inv, inv), inv));
+                        if (COMP) {
+                            TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
+                        } else {
+                            AX[m] = fma2(dx, sj, AX[m]); AY[m] = fma2(dy, sj, AY[m]); AZ[m] = fma2(dz, sj, AZ[m]);
+                        }
+                    }
+                }
+            } else {
+#pragma unroll 1
+                for (int j0 = 0; j0 < kSymJT; j0 += kSymJB) {
+                    float vx[kSymJB], vy[kSymJB], vz[kSymJB];
+#pragma unroll
+                    for (int jj = 0; jj < kSymJB; ++jj) {
+                        const float4 q = J[j0 + jj];
+                        const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y),
+                                     qz = make_float2(q.z, q.z), qm = make_float2(q.w, q.w);
+                        float2 tx = make_float2(0.0f, 0.0f), ty = tx, tz = tx;
+#pragma unroll
+                        for (int m = 0; m < P; ++m) {
+                            const float2 dx = sub2(qx, X[m]), dy = sub2(qy, Y[m]), dz = sub2(qz, Z[m]);
+                            const float2 r2 = fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, E2)));
+                            float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+                            if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
+                            const float2 i3 = mul2(mul2(inv, inv), inv);
+                            const float2 sj = mul2(qm, i3), si = mul2(MI[m], i3);
+                            if (COMP) {
+                                TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
+                            } else {
+                                AX[m] = fma2(dx, sj, AX[m]); AY[m] = fma2(dy, sj, AY[m]); AZ[m] = fma2(dz, sj, AZ[m]);
+                            }
+                            tx = fma2(dx, si, tx); ty = fma2(dy, si, ty); tz = fma2(dz, si, tz);
+                        }
+                        vx[jj] = tx.x + tx.y;
+                        vy[jj] = ty.x + ty.y;
+                        vz[jj] = tz.x + tz.y;
+                    }
+                    reduce_lanes(vx, lane);
+                    reduce_lanes(vy, lane);
+                    reduce_lanes(vz, lane);
+                    constexpr int sh = 5 - log2_c(kSymJB);
+                    if ((lane & ((1 << sh) - 1)) == 0) {
+                        const int j = j0 + ((lane >> sh) & (kSymJB - 1));
+                        js[warp][j][0] = vx[0];
+                        js[warp][j][1] = vy[0];
+                        js[warp][j][2] = vz[0];
+                    }
+                }
+            }
+            if (COMP) {
+#pragma unroll
+                for (int m = 0; m < P; ++m) {
+                    fold(AX[m].x, CX[m].x, TX[m].x); fold(AX[m].y, CX[m].y, TX[m].y);
+                    fold(AY[m].x, CY[m].x, TY[m].x); fold(AY[m].y, CY[m].y, TY[m].y);
+                    fold(AZ[m].x, CZ[m].x, TZ[m].x); fold(AZ[m].y, CZ[m].y, TZ[m].y);
+                }
+            }
+            if (k >= nd) {  // this tile's column sums over the CTA's row block, into the column slot
+                __syncthreads();
+                const int64_t jb = c0 + static_cast<int64_t>(k - nd) * kSymJT;
+#pragma unroll
+                for (int h = 0; h < kSymJT / kSymT; ++h) {
+                    const int j = tid + h * kSymT;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float v = (js[0][j][c] + js[1][j][c]) + (js[2][j][c] + js[3][j][c]);
+                        float* dst = Pj + c * n_pad + jb + j;
+                        if (COMP) {
+                            float* cdst = Pj + (3 + c) * n_pad + jb + j;
+                            if (first) {
+                                *dst = v;
+                                *cdst = 0.0f;
+                            } else {
+                                float sv = *dst, cv = *cdst;
+                                fold(sv, cv, v);
+                                *dst = sv;
+                                *cdst = cv;
+                            }
+                        } else {
+                            *dst = first ? v : *dst + v;
+                        }
+                    }
+                }
+            }
+        }
+        // the row sums of block a into its row slot
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float* out = Pi + base + static_cast<int64_t>(2 * m + h) * kSymT;
+                out[0] = h ? AX[m].y : AX[m].x;
+                out[n_pad] = h ? AY[m].y : AY[m].x;
+                out[2 * n_pad] = h ? AZ[m].y : AZ[m].x;
+                if (COMP) {
+                    out[3 * n_pad] = h ? CX[m].y : CX[m].x;
+                    out[4 * n_pad] = h ? CY[m].y : CY[m].x;
+                    out[5 * n_pad] = h ? CZ[m].y : CZ[m].x;
+                }
+            }
+        }
+    }
+}
+
 template <int I, int GRAV, bool COMP>
 __global__ void __launch_bounds__(128) k_gravity(const float4* __restrict__ posm, float* __restrict__ part,
                                                   int64_t n_pad, int jt, int nseg, float eps2, int* status) {
@@ -661,26 +942,16 @@ __global__ void __launch_bounds__(128) k_gravity(const float4* __restrict__ posm
 }
 
 template <bool COMP>
-__global__ void k_gravity_finish(DevArrays a, DevParams p, int nseg) {
+__global__ void k_gravity_finish(DevArrays a, DevParams p, GravSum gsum) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (has(p, GSPH_VARIABLE_TIMESTEP) && i == 0) a.dt_state[1] = p.max_dt;
     if (i >= a.n) return;
-    const int K = COMP ? 6 : 3;
+    double t[3];
+    gpart_sum<COMP>(a.part, a.n_pad, gsum, i, t);
     float acc[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        if (COMP) {
-            double s = 0.0;
-            for (int k = 0; k < nseg; ++k)
-                s += static_cast<double>(a.part[(k * K + c) * a.n_pad + i]) +
-                     static_cast<double>(a.part[(k * K + 3 + c) * a.n_pad + i]);
-            acc[c] = static_cast<float>(s * static_cast<double>(p.G));
-        } else {
-            float s = 0.0f;
-            for (int k = 0; k < nseg; ++k) s += a.part[(k * K + c) * a.n_pad + i];
-            acc[c] = p.G * s;
-        }
-    }
+    for (int c = 0; c < 3; ++c)
+        acc[c] = COMP ? static_cast<float>(t[c] * static_cast<double>(p.G)) : p.G * static_cast<float>(t[c]);
     if (a.grav) a.grav[i] = make_float4(acc[0], acc[1], acc[2], 0.0f);
     environment(p, a.posm[i], a.velrho[i], acc[0], acc[1], acc[2]);
     a.acc[i] = make_float4(acc[0], acc[1], acc[2], 0.0f);
@@ -720,6 +991,7 @@ CullView cull_view(const DevArrays& a, const SpatialArrays& sp) {
     cv.part = sp.item_part;
     cv.nb = nullptr;
     cv.nbcnt = nullptr;
+    cv.nbover = nullptr;
     return cv;
 }
 PartView seg_view(const DevArrays& a, int nseg, int KK) { return PartView{a.part, a.n_pad, nseg, nullptr, KK}; }
@@ -801,6 +1073,7 @@ cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch&
         CullView cvl = cv;
         cvl.nb = sp->item_nb;
         cvl.nbcnt = sp->item_nbcnt;
+        cvl.nbover = sp->item_nbover;
         if (comp) k_density_items<true, true><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cvl, a.status);
         else k_density_items<false, true><<<L.density_grid, kGroup, smem, s>>>(a.posm, p, cvl, a.status);
     } else {
@@ -845,6 +1118,7 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
         if (lists) {
             cv.nb = sp->item_nb;
             cv.nbcnt = sp->item_nbcnt;
+            cv.nbover = sp->item_nbover;
         }
         k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cv);
         cudaError_t e = cudaGetLastError();
@@ -855,7 +1129,7 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
             if (e != cudaSuccess) return e;
         }
         k_pairs_finish<PASS, false, SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(
-            a, p, item_view(a, *sp, COMP ? 2 * K : K), PASS == PASS_VGRAD ? 0 : gnseg);
+            a, p, item_view(a, *sp, COMP ? 2 * K : K), grav_sum(L, PASS == PASS_VGRAD ? 0 : gnseg));
         return cudaGetLastError();
     }
     constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
@@ -873,7 +1147,7 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
     k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(
-        a, p, seg_view(a, L.nseg, COMP ? 2 * K : K), 0);
+        a, p, seg_view(a, L.nseg, COMP ? 2 * K : K), GravSum{});
     return cudaGetLastError();
 }
 
@@ -921,7 +1195,11 @@ cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, c
     const dim3 grid(static_cast<unsigned>(a.n_pad / (static_cast<int64_t>(T) * I)), static_cast<unsigned>(L.grav_nseg));
     const size_t smem = pipe_smem_bytes(1, L.grav_jt);
     GSPH_TIMER_MARK(t, start);
-    if constexpr (I >= 2) {
+    if (L.grav_sym_G > 0) {
+        const int G = L.grav_sym_G;
+        k_gravity_sym<GRAV, COMP><<<static_cast<unsigned>(G * (G + 1) / 2), kSymT, 0, s>>>(
+            a.posm, finish ? a.part : a.gpart, a.n_pad, G, L.grav_sym_gs, p.eps2);
+    } else if constexpr (I >= 2) {
         if (L.grav_x2)
             k_gravity_x2<I, GRAV, COMP><<<grid, T, smem, s>>>(a.posm, finish ? a.part : a.gpart, a.n_pad, L.grav_jt,
                                                                L.grav_nseg, p.eps2, a.status);
@@ -936,7 +1214,7 @@ cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, c
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
     if (!finish) return cudaSuccess;
-    k_gravity_finish<COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, L.grav_nseg);
+    k_gravity_finish<COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, grav_sum(L, L.grav_nseg));
     return cudaGetLastError();
 }
 template <int GRAV, bool COMP>
@@ -960,8 +1238,8 @@ cudaError_t gravity_any(const DevArrays& a, const DevParams& p, const Launch& L,
 cudaError_t launch_gravity(const DevArrays& a, const DevParams& p, const Launch& L, cudaStream_t s, const KTimer* t) {
     const bool comp = L.accum == GSPH_ACCUM_COMPENSATED;
     if (!has(p, GSPH_SELF_GRAVITY)) {  // neither gravity nor SPH: environment terms only
-        if (comp) k_gravity_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 0);
-        else k_gravity_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, 0);
+        if (comp) k_gravity_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, GravSum{});
+        else k_gravity_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, GravSum{});
         return cudaGetLastError();
     }
     return gravity_any(a, p, L, s, t, true);
@@ -1034,7 +1312,7 @@ size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad) {
         k = std::max<size_t>(k, static_cast<size_t>(popc_c(field_mask<PASS_FUSED, true, false>())));
         k *= static_cast<size_t>(std::max(L.nseg, 1));
     } else {
-        k = 3 * static_cast<size_t>(std::max(L.grav_nseg, 1));
+        k = 3 * static_cast<size_t>(L.grav_sym_G > 0 ? 2 * L.grav_sym_G : std::max(L.grav_nseg, 1));
     }
     return k * mult * static_cast<size_t>(n_pad);
 }
@@ -1058,7 +1336,8 @@ int gravity_blocks_per_sm(int ipt, int threads, int jt, bool comp) {
 
 size_t gravity_partial_floats(const Launch& L, int64_t n_pad) {
     const int mult = (L.accum == GSPH_ACCUM_COMPENSATED) ? 2 : 1;
-    return static_cast<size_t>(3) * mult * static_cast<size_t>(std::max(L.grav_nseg, 1)) * static_cast<size_t>(n_pad);
+    const int slots = L.grav_sym_G > 0 ? 2 * L.grav_sym_G : std::max(L.grav_nseg, 1);
+    return static_cast<size_t>(3) * mult * static_cast<size_t>(slots) * static_cast<size_t>(n_pad);
 }
 
 }  // namespace gsph

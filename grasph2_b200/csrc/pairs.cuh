@@ -99,7 +99,8 @@ struct CullView {
     int64_t nchunks;        // row stride of `list`
     float* part;            // [item][field][kGroup]
     int* nb;                // nullable: per item, each lane's neighbour indices [item][kItemNb][kGroup] ...
-    int* nbcnt;             // ... and their count [item][kGroup] (kItemNb + 1: the list overflowed)
+    int* nbcnt;             // ... and their count [item][kGroup] (kItemNb + 1: the list overflowed) ...
+    int* nbover;            // ... and per item whether any lane's list overflowed
     __device__ __forceinline__ int items() const { return item_start[ngroups]; }
     __device__ __forceinline__ void item(int w, int& g, int& c0, int& c1) const {
         int lo = 0, hi = ngroups;  // item_start[lo] <= w < item_start[hi]
@@ -230,6 +231,15 @@ struct KTimer {
 cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s);
 
 // host launchers (pairs.cu)
+// How the finish kernels read a particle's gravity partials: segments 0 .. nseg-1 of the one-sided
+// kernel, or (sym_G > 0) the symmetric kernel's row slots g .. G-1 and column slots G .. G + g of the
+// particle's group g = i / sym_group.
+struct GravSum {
+    int nseg = 0;
+    int sym_G = 0;
+    int64_t sym_group = 1;  // particles per group
+};
+
 struct Launch {
     bool cull;       // SPH passes over near-chunk lists (spatial.cuh) + separate all-pairs gravity
     int threads;     // threads per CTA of the SPH pair kernels
@@ -240,10 +250,32 @@ struct Launch {
     int grav_jt;     // j-tile of the gravity kernel
     bool grav_x2;    // paired FP32 (f32x2) form of the gravity kernel
     int grav_nseg;
+    int grav_sym_G = 0;   // > 0: symmetric gravity kernel over G groups of grav_sym_gs blocks of 1024
+    int grav_sym_gs = 0;
     int accum;       // GSPH_ACCUM_*
     int item_grid;   // persistent grid of the culled SPH kernel (its resident capacity)
     int density_grid;  // persistent grid of the culled density kernel
 };
+
+// the finish kernels' view of the gravity partials of launch shape L; nseg == 0: no gravity partials
+inline GravSum grav_sum(const Launch& L, int nseg) {
+    GravSum g;
+    if (nseg <= 0) return g;
+    if (L.grav_sym_G > 0) {
+        g.sym_G = L.grav_sym_G;
+        g.sym_group = static_cast<int64_t>(L.grav_sym_gs) * 1024;
+    } else {
+        g.nseg = nseg;
+    }
+    return g;
+}
+// the symmetric gravity kernel's group count for blocks of 1024 particles: groups of
+// ceil(nblocks / target) blocks
+inline void sym_groups(int64_t nblocks, int target, int& G, int& gs) {
+    gs = static_cast<int>((nblocks + target - 1) / target);
+    if (gs < 1) gs = 1;
+    G = static_cast<int>((nblocks + gs - 1) / gs);
+}
 
 // With `sp`, the culled density pass also stores every lane's neighbour indices per work item
 // (sp->item_nb), which the SPH passes of the same step then use instead of scanning the chunks again.

@@ -27,6 +27,7 @@ struct SpatialArrays {
     float* item_part;  // [items][fields][kGroup] partial sums of the culled passes
     int* item_nb;      // [items][kItemNb][kGroup] neighbour indices found by the culled density pass
     int* item_nbcnt;   // [items][kGroup]
+    int* item_nbover;  // [items] nonzero: some lane's list of the item overflowed
     int* ext_of_int;   // [n_pad] caller's index of the particle stored at each internal slot
     int* order;        // [n_pad] scratch: sort values / gather map
     unsigned* keys;    // [2 n_pad] sort keys (in, out)

@@ -93,7 +93,7 @@ def params_to_dict(p):
 
 
 def make_options(accum="plain", j_split=0, j_tile=0, i_per_thread=0, threads=0, check_finite=0, cull=True,
-                 resort_interval=0, scalar_fp32=False, precision="single"):
+                 resort_interval=0, scalar_fp32=False, precision="single", gravity="auto", gravity_groups=0):
     o = GsphOptions()
     o.accum = {"plain": ACCUM_PLAIN, "compensated": ACCUM_COMPENSATED}[accum] if isinstance(accum, str) else accum
     o.j_split, o.j_tile, o.i_per_thread, o.threads, o.check_finite = j_split, j_tile, i_per_thread, threads, check_finite
@@ -101,6 +101,8 @@ def make_options(accum="plain", j_split=0, j_tile=0, i_per_thread=0, threads=0, 
     o.resort_interval = resort_interval
     o.scalar_fp32 = 1 if scalar_fp32 else 0
     o.precision = {"single": 0, "double": 1}[precision] if isinstance(precision, str) else int(precision)
+    o.gravity_form = {"auto": 0, "one-sided": 1, "symmetric": 2}[gravity] if isinstance(gravity, str) else int(gravity)
+    o.gravity_groups = gravity_groups
     return o
 
 

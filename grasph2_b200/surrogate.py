@@ -188,7 +188,7 @@ class Surrogate:
         """Advance pb by K substeps in one proposal (gsph_surrogate_propose)."""
         self._check(self.lib.gsph_surrogate_propose(self._h, pb.handle, int(bool(use_net)), _stream_handle(stream)))
 
-    def energy_correction(self, on=True, gain=0.5):
+    def energy_correction(self, on=True, gain=1.0):
         """Judge-calibrated energy correction (gsph_surrogate_set_energy_correction); resets the estimates."""
         self._check(self.lib.gsph_surrogate_set_energy_correction(self._h, int(bool(on)), float(gain)))
 

@@ -174,11 +174,20 @@ typedef struct gsph_options {
                                 SINGLE_PRECISION / DOUBLE_PRECISION switch (settings/precisionSettings.h:16-17).
                                 Double runs every pass in FP64 with plain all-pairs tiles (no culling,
                                 accum ignored); gsph_upload_f64 / gsph_download_f64 pass values unrounded */
-    int32_t reserved[6];
+    int32_t gravity_form;    /* GSPH_GRAVITY_AUTO (default), GSPH_GRAVITY_ONE_SIDED or GSPH_GRAVITY_SYMMETRIC: the
+                                all-pairs gravity kernel evaluates every ordered pair (i gathers from all j), or
+                                every unordered pair once and applies it to both particles (Newton's third law;
+                                2/3 of the FP32 work, partials of 2 x 64 x 3 floats per particle). Auto picks the
+                                symmetric form from 24 blocks of 1024 particles up. Results agree to rounding */
+    int32_t gravity_groups;  /* symmetric form: particle groups G (tasks G(G+1)/2); 0 = up to 64 */
+    int32_t reserved[4];
 } gsph_options;
 
 #define GSPH_PRECISION_SINGLE 0
 #define GSPH_PRECISION_DOUBLE 1
+#define GSPH_GRAVITY_AUTO      0
+#define GSPH_GRAVITY_ONE_SIDED 1
+#define GSPH_GRAVITY_SYMMETRIC 2
 
 int gsph_options_defaults(gsph_options* o);
 
@@ -266,7 +275,8 @@ int gsph_diagnostics_fast(gsph_ctx* ctx, double half_kick, gsph_diag* out, void*
 int gsph_autotune(gsph_ctx* ctx, int32_t reps, void* stream);
 typedef struct gsph_launch_shape {
     int32_t cull, grav_ipt, grav_jt, grav_nseg, grav_x2, sph_threads, sph_jt, sph_nseg, items;
-    int32_t reserved[7];
+    int32_t grav_sym_groups;  /* > 0: the symmetric gravity kernel over this many particle groups */
+    int32_t reserved[6];
 } gsph_launch_shape;
 int gsph_launch_shape_get(gsph_ctx* ctx, gsph_launch_shape* out);
 
