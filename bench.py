@@ -44,11 +44,13 @@ FLUSH_BYTES = 256 << 20
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture of the same workload:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none \
-#       -k regex:"k_gravity_x2|k_pairs_items|k_density_items" -s 9 -c 6 --csv \
+#       -k regex:"k_gravity_sym|k_gravity_x2|k_pairs_items|k_density_items" -s 9 -c 6 --csv \
 #       python bench.py --steps 5 --warmup 3 --no-cpu-baseline --no-e2e --no-peak --drift-steps 0 --no-autotune
-# k_gravity_x2 on the impact: 1.06-1.08 MB read, 0 written (its j-segment partials stay in L2) = the
-# 1.05 MB of j-records: no re-reads.
-MEASURED_TRAFFIC = {("impact", 65536, "gravity"): 1.08e6}
+# (with --gravity one-sided for the one-sided kernel). On the impact the symmetric kernel reads 1.08 MB
+# (the 1.05 MB of j-records: no re-reads) and writes 0.95-2.02 MB of its 100 MB of partial slots (the
+# rest stays in L2); the one-sided kernel reads 1.06-1.08 MB and writes nothing.
+MEASURED_TRAFFIC = {("impact", 65536, "gravity", "symmetric"): 2.56e6,
+                    ("impact", 65536, "gravity", "one-sided"): 1.08e6}
 FLAG_DEAL_WITH_NO_PARTNERS = 1 << 3  # GSPH_DEAL_WITH_NO_PARTNERS
 
 
@@ -75,6 +77,8 @@ def parse():
     ap.add_argument("--no-cull", action="store_true", help="all-pairs SPH sweeps (no chunk culling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--scalar-fp32", action="store_true", help="scalar instead of paired f32x2 gravity kernel")
+    ap.add_argument("--gravity", choices=["auto", "one-sided", "symmetric"], default="auto",
+                    help="all-pairs gravity kernel: every ordered pair, or every unordered pair once")
     ap.add_argument("--drift-steps", type=int, default=-1,
                     help="steps of the energy-drift comparison (plain, compensated, FP64); default 1000 on the "
                          "impact workload, 0 (off) elsewhere")
@@ -822,7 +826,7 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    opts = dict(accum=args.accum, cull=not args.no_cull, scalar_fp32=args.scalar_fp32)
+    opts = dict(accum=args.accum, cull=not args.no_cull, scalar_fp32=args.scalar_fp32, gravity=args.gravity)
     pb = DeviceParticleBuffer(params, n, make_options(**opts))
     pb.upload(st, stream=stream)
     shape = pb.launch_shape() if args.no_autotune else pb.autotune(3, stream)
@@ -926,7 +930,8 @@ def main():
         "kernel_ms_per_step": {k: (v[0] / v[1] if v[1] else None) for k, v in prof.items()},
         "roofline": {"bound": "fp32", "kernel": dominant, "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if (achieved and peak_tflops) else None,
-                     "traffic": MEASURED_TRAFFIC.get((args.workload, n, dominant)),
+                     "traffic": MEASURED_TRAFFIC.get((args.workload, n, dominant,
+                                                      "symmetric" if shape.get("grav_sym_groups") else "one-sided")),
                      "algorithmic_bytes": 16 * n, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
                      "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
         "integrator_roofline": integrator_roofline(prof, n, params),
