@@ -501,8 +501,8 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
-        L.item_grid = c->sm_count * 4;      // 49 KB of shared memory and 120 registers per thread: 4 per SM
-        L.density_grid = c->sm_count * 8;
+        L.item_grid = c->sm_count * 5;      // 41 KB of shared memory and at most 102 registers: 5 per SM
+        L.density_grid = c->sm_count * 12;  // 37 registers and 8 KB of shared memory: 12 fit per SM
         sp.item_target = 6 * L.item_grid;
         sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 2) * sizeof(int), ae));
         // worst case fields per item: fused solids pass without gravity, compensated (x2); items are at
@@ -515,6 +515,8 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         sp.item_nb = static_cast<int*>(dalloc(c, cap * kItemNb * kGroup * sizeof(int), ae));
         sp.item_nbcnt = static_cast<int*>(dalloc(c, cap * kGroup * sizeof(int), ae));
         sp.item_nbover = static_cast<int*>(dalloc(c, cap * sizeof(int), ae));
+        a.jrec = static_cast<float4*>(dalloc(c, 4 * n_pad * sizeof(float4), ae));
+        if (ae == cudaSuccess) ae = cudaMemset(a.jrec, 0, 4 * n_pad * sizeof(float4));
         sp.box_lo = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.box_hi = static_cast<float4*>(dalloc(c, nchunks * sizeof(float4), ae));
         sp.list = static_cast<int*>(dalloc(c, static_cast<size_t>(ngroups) * nchunks * sizeof(int), ae));

@@ -57,6 +57,8 @@ struct DevArrays {
     float* balsara;   // Balsara switch
     float4* jA;       // j-record: sigma/rho^2 (xx, yy, zz, xy)
     float4* jB;       // j-record: sigma/rho^2 (xz, yz), balsara, 0
+    float4* jrec;     // nullable: [n_pad][4] = posm, velrho, jA, jB packed per particle (one 64-byte line
+                      // per neighbour for the culled SPH passes' gathers), rebuilt with jA / jB
     float* part;      // j-split partial sums [segment][component][n_pad]
     float* gpart;     // gravity partial sums of the culled path [segment][component][n_pad]
     float* dt_state;  // variable step: [0] current, [1] next (float bit patterns, positive)

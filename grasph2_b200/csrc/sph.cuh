@@ -232,6 +232,7 @@ __device__ __forceinline__ void sph_finish(const DevArrays& a, const DevParams& 
             float4 jb = a.jB[i];
             jb.z = bal;
             a.jB[i] = jb;
+            if (a.jrec) a.jrec[4 * i + 3] = jb;
         }
         a.balsara[i] = bal;
     }
