@@ -368,6 +368,8 @@ public:
         return w;
     }
     void save(const std::string& modelFile) { chk(gsph_surrogate_save(s_, modelFile.c_str())); }
+    // the judge-calibrated energy correction (gsph_surrogate_set_energy_correction); resets its estimates
+    void energyCorrection(bool on, double gain = 1.0) { chk(gsph_surrogate_set_energy_correction(s_, on ? 1 : 0, gain)); }
     gsph_surrogate* get() { return s_; }
 
 private:

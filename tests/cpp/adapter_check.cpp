@@ -114,6 +114,7 @@ int main(int argc, char** argv) {
         gsph::DeviceParticleBuffer sb(q, n);
         sb = hpb;
         gsph::Surrogate sur(argv[2]);
+        sur.energyCorrection(true);
         const std::vector<gsph_surrogate_window> w = sur.advance(sb, 1, 2);
         if (w.size() != 1 || !(w[0].pos_error >= 0) || !(w[0].energy_error >= 0)) {
             std::printf("surrogate window failed\n");
