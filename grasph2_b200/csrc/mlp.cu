@@ -687,6 +687,8 @@ int gsph_mlp_set_params(gsph_mlp* m, const float* params) {
 
 int gsph_mlp_forward(gsph_mlp* m, const float* x, float* y, int64_t n, void* stream) {
     if (!m || (!x && n) || (!y && n) || n < 0) return mfail(m, GSPH_E_INVALID, "bad argument");
+    // the kernel reads each input row as 16-byte vectors
+    if (reinterpret_cast<uintptr_t>(x) % 16) return mfail(m, GSPH_E_INVALID, "x must be 16-byte aligned");
     if (n == 0) return GSPH_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int64_t tiles = (n + kTileM - 1) / kTileM;

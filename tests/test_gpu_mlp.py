@@ -121,3 +121,18 @@ def test_mlp_training_fits_a_teacher():
             net.adam(lr=2e-3)
         _, l1 = net.gradient(xd, td, wd, n)
     assert l1 < 0.1 * l0, (l0, l1)
+
+
+def test_mlp_forward_rejects_misaligned_inputs():
+    """The input rows are read as 16-byte vectors: an input pointer off a 16-byte boundary is an error,
+    not a fault."""
+    import torch
+    from grasph2_b200.mlp import MLP
+    from grasph2_b200.sim import GsphError
+    p, x, _, _ = _setup(100, 3)
+    xd = torch.from_numpy(np.concatenate([np.zeros(1, np.float32), x.ravel()])).cuda()
+    yd = torch.zeros(100, M.OUT, device="cuda")
+    with MLP(p) as net:
+        with pytest.raises(GsphError) as e:
+            net.forward(xd.data_ptr() + 4, yd, 100)
+        assert e.value.code == -1
