@@ -188,10 +188,12 @@ int gsph_surrogate_load(const char* path, gsph_surrogate** out) {
                                  out);
 }
 
-int gsph_surrogate_propose(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, void* stream) {
-    if (!s || !ctx) return sfail(s, GSPH_E_INVALID, "NULL argument");
-    int rc = gsph_compute_derivatives(ctx, stream);
-    if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: derivatives");
+}  // extern "C"
+
+namespace {
+// a proposal from a state whose derivatives are already computed: features, MLP, apply, correction
+int propose_from_derivatives(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, void* stream) {
+    int rc;
     if (!use_net) {
         rc = gsph_surrogate_apply(ctx, nullptr, nullptr, nullptr, s->K, stream);
         if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: apply");
@@ -210,6 +212,16 @@ int gsph_surrogate_propose(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, vo
     if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: apply");
     return correct(s, ctx, stream);
 }
+}  // namespace
+
+extern "C" {
+
+int gsph_surrogate_propose(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, void* stream) {
+    if (!s || !ctx) return sfail(s, GSPH_E_INVALID, "NULL argument");
+    const int rc = gsph_compute_derivatives(ctx, stream);
+    if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "propose: derivatives");
+    return propose_from_derivatives(s, ctx, use_net, stream);
+}
 
 int gsph_surrogate_judge(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, double e_ref, gsph_surrogate_window* out,
                          void* stream) {
@@ -221,11 +233,15 @@ int gsph_surrogate_judge(gsph_surrogate* s, gsph_ctx* ctx, int32_t use_net, doub
         if (rc != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: energy");
         e_ref = d.e_kin + d.e_grav + d.e_int + d.e_shear;
     }
+    // the start state is saved with its derivatives, which the proposal and the plain integrator's first
+    // step share: the plain path is one integrate and K - 1 full steps (the same arithmetic as K steps)
+    if ((rc = gsph_compute_derivatives(ctx, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: derivatives");
     if ((rc = gsph_snapshot(ctx, 1, 0, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: snapshot");
-    if ((rc = gsph_surrogate_propose(s, ctx, use_net, stream)) != GSPH_OK) return rc;
+    if ((rc = propose_from_derivatives(s, ctx, use_net, stream)) != GSPH_OK) return rc;
     if ((rc = gsph_snapshot(ctx, 2, 0, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: snapshot");
     if ((rc = gsph_snapshot(ctx, 1, 1, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: restore");
-    if ((rc = gsph_step(ctx, s->K, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: plain steps");
+    if ((rc = gsph_integrate(ctx, 1, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: plain steps");
+    if ((rc = gsph_step(ctx, s->K - 1, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: plain steps");
     double c[8];
     if ((rc = gsph_state_compare_parts(ctx, 2, 1, c, stream)) != GSPH_OK) return ctx_fail(s, ctx, rc, "judge: compare");
     out->pos_error = c[2] > 0.0 ? std::sqrt(c[1] / c[2]) : HUGE_VAL;
