@@ -47,7 +47,7 @@ FLUSH_BYTES = 256 << 20
 #       -k regex:"k_gravity_sym|k_gravity_x2|k_pairs_items|k_density_items" -s 9 -c 6 --csv \
 #       python bench.py --steps 5 --warmup 3 --no-cpu-baseline --no-e2e --no-peak --drift-steps 0 --no-autotune
 # (with --gravity one-sided for the one-sided kernel). On the impact the symmetric kernel reads 1.08 MB
-# (the 1.05 MB of j-records: no re-reads) and writes 0.95-2.02 MB of its 100 MB of partial slots (the
+# (the 1.05 MB of j-records: no re-reads) and writes 0.95-2.02 MB of its partial slots (the
 # rest stays in L2); the one-sided kernel reads 1.06-1.08 MB and writes nothing.
 MEASURED_TRAFFIC = {("impact", 65536, "gravity", "symmetric"): 2.56e6,
                     ("impact", 65536, "gravity", "one-sided"): 1.08e6}

@@ -484,13 +484,8 @@ __device__ __forceinline__ float seg_sum(const PartView& v, int64_t i, int f) {
 // gravity partials of an all-pairs gravity kernel (component c of particle i), summed like seg_sum:
 // the one-sided kernel's segments 0 .. nseg-1, or the symmetric kernel's row slots g .. G-1 and then
 // column slots G .. G + g of the particle's group g
-__device__ __forceinline__ void gpart_slots(const GravSum& gs, int64_t i, int& r0, int& r1, int& c0, int& c1) {
+__device__ __forceinline__ void gpart_slots(const GravSum& gs, int64_t, int& r0, int& r1, int& c0, int& c1) {
     r0 = 0; r1 = gs.nseg; c0 = c1 = 0;
-    if (gs.sym_G > 0) {
-        const int g = static_cast<int>(i / gs.sym_group);
-        r0 = g; r1 = gs.sym_G;
-        c0 = gs.sym_G; c1 = gs.sym_G + g + 1;
-    }
 }
 // slots k0 .. k1-1 of all three components at once, unrolled so that several slots' loads are in
 // flight (each component is still summed in slot order)
@@ -510,6 +505,23 @@ __device__ __forceinline__ void gpart_range(const float* part, int64_t n_pad, in
 // the three components of particle i: FP64 sums of (sum + error) when compensated
 template <bool COMP>
 __device__ __forceinline__ void gpart_sum(const float* part, int64_t n_pad, const GravSum& gs, int64_t i, double (&out)[3]) {
+    if (gs.sym_G > 0) {  // the symmetric kernel's G + 1 slots of particle i, contiguous, in slot order
+        constexpr int K = COMP ? 6 : 3;
+        const int S = gs.sym_G + 1;
+        const float* q = part + static_cast<int64_t>(i) * S * K;
+        if (COMP) {
+            double s[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < S; ++k, q += K)
+                for (int c = 0; c < 3; ++c) s[c] += static_cast<double>(q[c]) + static_cast<double>(q[3 + c]);
+            for (int c = 0; c < 3; ++c) out[c] = s[c];
+        } else {
+            float s[3] = {0.0f, 0.0f, 0.0f};
+            for (int k = 0; k < S; ++k, q += K)
+                for (int c = 0; c < 3; ++c) s[c] += q[c];
+            for (int c = 0; c < 3; ++c) out[c] = s[c];
+        }
+        return;
+    }
     int r0, r1, c0, c1;
     gpart_slots(gs, i, r0, r1, c0, c1);
     if (COMP) {
@@ -663,10 +675,10 @@ __global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ p
 // column particle's contribution is summed over the CTA's 1024 row particles -- in the thread, then
 // across the warp by a butterfly that leaves kSymJB column sums spread over the lanes, then over the
 // four warps in shared memory -- and added to its slot in the partials (plain, or two-sum when
-// compensated). The pairs inside a block (the diagonal tile) run one-sided. Row sums go to slot gb and
-// column sums to slot G + ga, so each (slot, particle) has one writer; the finish kernels add a
-// particle's row slots g .. G-1, then its column slots G .. G + g (g its group), in that fixed order,
-// and results do not depend on scheduling. FMA-pipe work per pair interaction: 8 + ~0.4 operations
+// compensated). The pairs inside a block (the diagonal tile) run one-sided. Each particle has G + 1
+// slots, each written by one task (its row sums from tasks (g, gb), its column sums from tasks (ga, g),
+// g its group); the finish kernels add a particle's slots in a fixed order, so results do not depend on
+// scheduling. FMA-pipe work per pair interaction: 8 + ~0.4 operations
 // against the one-sided kernel's 12.
 constexpr int kSymT = 128, kSymI = 8, kSymB = kSymT * kSymI, kSymJT = 256;
 constexpr int kSymJB = 8;  // column particles per butterfly (8: 136 registers, three CTAs per SM; 4 fits four
@@ -736,11 +748,17 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
     const int ra0 = ga * gs, ra1 = min(nb, ra0 + gs);
     const int cg0 = gb * gs, cg1 = min(nb, cg0 + gs);
     const bool diag = ga == gb;
-    float* Pi = part + static_cast<int64_t>(gb) * K * n_pad;
-    float* Pj = part + static_cast<int64_t>(G + ga) * K * n_pad;
+    // partials per particle: G + 1 slots of K floats, a particle of group g holding its row sums from
+    // tasks (g, gb), gb = g .. G-1, in slots 0 .. G-1-g and its column sums from tasks (ga, g), ga = 0 .. g,
+    // in slots G-g .. G (so the finish reads one contiguous run per particle, in a fixed order)
+    const int64_t S = G + 1;
+    const int s_row = gb - ga, s_col = G - gb + ga;
+    auto slot = [&](int64_t particle, int sl) { return part + (particle * S + sl) * K; };
     if (diag)  // the group's first block is never a column here: its column slot is zero
-        for (int e = tid; e < kSymB; e += kSymT)
-            for (int c = 0; c < K; ++c) Pj[c * n_pad + static_cast<int64_t>(ra0) * kSymB + e] = 0.0f;
+        for (int e = tid; e < kSymB; e += kSymT) {
+            float* q = slot(static_cast<int64_t>(ra0) * kSymB + e, s_col);
+            for (int c = 0; c < K; ++c) q[c] = 0.0f;
+        }
     const float2 E2 = make_float2(eps2, eps2);
 
     for (int a = ra0; a < ra1; ++a) {
@@ -858,9 +876,9 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const float v = (js[0][j][c] + js[1][j][c]) + (js[2][j][c] + js[3][j][c]);
-                        float* dst = Pj + c * n_pad + jb + j;
+                        float* dst = slot(jb + j, s_col) + c;
                         if (COMP) {
-                            float* cdst = Pj + (3 + c) * n_pad + jb + j;
+                            float* cdst = dst + 3;
                             if (first) {
                                 *dst = v;
                                 *cdst = 0.0f;
@@ -882,14 +900,14 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
         for (int m = 0; m < P; ++m) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                float* out = Pi + base + static_cast<int64_t>(2 * m + h) * kSymT;
+                float* out = slot(base + static_cast<int64_t>(2 * m + h) * kSymT, s_row);
                 out[0] = h ? AX[m].y : AX[m].x;
-                out[n_pad] = h ? AY[m].y : AY[m].x;
-                out[2 * n_pad] = h ? AZ[m].y : AZ[m].x;
+                out[1] = h ? AY[m].y : AY[m].x;
+                out[2] = h ? AZ[m].y : AZ[m].x;
                 if (COMP) {
-                    out[3 * n_pad] = h ? CX[m].y : CX[m].x;
-                    out[4 * n_pad] = h ? CY[m].y : CY[m].x;
-                    out[5 * n_pad] = h ? CZ[m].y : CZ[m].x;
+                    out[3] = h ? CX[m].y : CX[m].x;
+                    out[4] = h ? CY[m].y : CY[m].x;
+                    out[5] = h ? CZ[m].y : CZ[m].x;
                 }
             }
         }
@@ -1341,7 +1359,7 @@ size_t partial_floats(const DevParams& p, const Launch& L, int64_t n_pad) {
         k = std::max<size_t>(k, static_cast<size_t>(popc_c(field_mask<PASS_FUSED, true, false>())));
         k *= static_cast<size_t>(std::max(L.nseg, 1));
     } else {
-        k = 3 * static_cast<size_t>(L.grav_sym_G > 0 ? 2 * L.grav_sym_G : std::max(L.grav_nseg, 1));
+        k = 3 * static_cast<size_t>(L.grav_sym_G > 0 ? L.grav_sym_G + 1 : std::max(L.grav_nseg, 1));
     }
     return k * mult * static_cast<size_t>(n_pad);
 }
@@ -1365,7 +1383,7 @@ int gravity_blocks_per_sm(int ipt, int threads, int jt, bool comp) {
 
 size_t gravity_partial_floats(const Launch& L, int64_t n_pad) {
     const int mult = (L.accum == GSPH_ACCUM_COMPENSATED) ? 2 : 1;
-    const int slots = L.grav_sym_G > 0 ? 2 * L.grav_sym_G : std::max(L.grav_nseg, 1);
+    const int slots = L.grav_sym_G > 0 ? L.grav_sym_G + 1 : std::max(L.grav_nseg, 1);
     return static_cast<size_t>(3) * mult * static_cast<size_t>(slots) * static_cast<size_t>(n_pad);
 }
 

@@ -232,12 +232,11 @@ cudaError_t timer_record(cudaEvent_t ev, cudaStream_t s);
 
 // host launchers (pairs.cu)
 // How the finish kernels read a particle's gravity partials: segments 0 .. nseg-1 of the one-sided
-// kernel, or (sym_G > 0) the symmetric kernel's row slots g .. G-1 and column slots G .. G + g of the
-// particle's group g = i / sym_group.
+// kernel ([segment][component][particle]), or (sym_G > 0) the symmetric kernel's G + 1 slots of the
+// particle ([particle][slot][component]).
 struct GravSum {
     int nseg = 0;
     int sym_G = 0;
-    int64_t sym_group = 1;  // particles per group
 };
 
 struct Launch {
@@ -263,7 +262,6 @@ inline GravSum grav_sum(const Launch& L, int nseg) {
     if (nseg <= 0) return g;
     if (L.grav_sym_G > 0) {
         g.sym_G = L.grav_sym_G;
-        g.sym_group = static_cast<int64_t>(L.grav_sym_gs) * 1024;
     } else {
         g.nseg = nseg;
     }

@@ -177,7 +177,7 @@ typedef struct gsph_options {
     int32_t gravity_form;    /* GSPH_GRAVITY_AUTO (default), GSPH_GRAVITY_ONE_SIDED or GSPH_GRAVITY_SYMMETRIC: the
                                 all-pairs gravity kernel evaluates every ordered pair (i gathers from all j), or
                                 every unordered pair once and applies it to both particles (Newton's third law;
-                                2/3 of the FP32 work, partials of 2 x 64 x 3 floats per particle). Auto picks the
+                                2/3 of the FP32 work, partials of 65 x 3 floats per particle). Auto picks the
                                 symmetric form from 24 blocks of 1024 particles up. Results agree to rounding */
     int32_t gravity_groups;  /* symmetric form: particle groups G (tasks G(G+1)/2); 0 = up to 64 */
     int32_t reserved[4];
