@@ -224,6 +224,8 @@ _SIGNATURES = {
     "gsph_mlp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_gravity_accel_static_status": (ctypes.c_int, [ctypes.c_void_p]),
+    "gsph_inject_static_timeout": (ctypes.c_int, [ctypes.c_int]),
     "gsph_surrogate_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float)] * 5 +
                               [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "gsph_surrogate_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),

@@ -8,6 +8,7 @@
 // j-records and the j-split partial sums -- in one file-scope device array of a fixed size.
 #include <algorithm>
 #include <initializer_list>
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -30,10 +31,14 @@ static __device__ __align__(256) unsigned char g_gravity_scratch[kStaticScratchB
 
 std::mutex g_lock;
 void* g_scratch_addr[kMaxDevices] = {};
+std::atomic<int> g_inject_timeout{0};  // test hook: the next call starts with the timeout bit set
 
-// The device address of the array for the current device, looked up once per device: in host code
-// the array's name stands for a host-side shadow, not a device address.
-int scratch_address(void** out) {
+// The device address of the array for the current device. In host code the array's name stands for
+// a host-side shadow, not a device address, so the address is looked up with cudaGetSymbolAddress:
+// afresh on every call outside stream capture (a device reset reloads the module and moves the
+// array), and from the last lookup while `s` is capturing (the first call on a device must come
+// before any capture).
+int scratch_address(cudaStream_t s, void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) {
@@ -44,8 +49,18 @@ int scratch_address(void** out) {
         set_global_error("device index out of range for the static scratch table");
         return GSPH_E_UNSUPPORTED;
     }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) {
+        set_global_error(std::string("cudaStreamIsCapturing failed: ") + cudaGetErrorString(e));
+        return GSPH_E_CUDA;
+    }
     std::lock_guard<std::mutex> lk(g_lock);
-    if (!g_scratch_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone || !g_scratch_addr[dev]) {
+        if (cap != cudaStreamCaptureStatusNone) {
+            set_global_error("the first call on a device must come before any stream capture");
+            return GSPH_E_INVALID;
+        }
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_gravity_scratch);
         if (e != cudaSuccess || !p) {
@@ -59,18 +74,28 @@ int scratch_address(void** out) {
     return GSPH_OK;
 }
 
-// the caller's n records, then inert padding (zero mass, far away) up to n_pad
-__global__ void k_static_pad(const float4* __restrict__ in, float4* __restrict__ out, int64_t n, int64_t n_pad) {
+// the caller's n records, then inert padding (zero mass, far away) up to n_pad; the status word
+// starts at `status0`
+__global__ void k_static_pad(const float4* __restrict__ in, float4* __restrict__ out, int64_t n, int64_t n_pad,
+                             int* status, int status0) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i == 0) *status = status0;
     if (i >= n_pad) return;
     out[i] = (i < n) ? in[i] : make_float4(1e18f, 1e18f, 1e18f, 0.0f);
 }
 
-// a_i = G * (sum of the segments, fixed order)
+// a_i = G * (sum of the segments, fixed order). If a bounded wait of the gravity kernel gave up
+// (timeout bit in the status word), some j-tiles were never summed: every output is NaN instead, so a
+// partial result cannot pass for a correct one.
 __global__ void k_static_finish(const float* __restrict__ part, float4* __restrict__ acc, int64_t n, int64_t n_pad,
-                                int nseg, float G) {
+                                int nseg, float G, const int* __restrict__ status) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (*status & GSPH_DEV_ERR_TIMEOUT) {
+        const float q = __int_as_float(0x7fc00000);
+        acc[i] = make_float4(q, q, q, q);
+        return;
+    }
     float s[3] = {0.0f, 0.0f, 0.0f};
     for (int k = 0; k < nseg; ++k)
 #pragma unroll
@@ -97,8 +122,9 @@ extern "C" int gsph_gravity_accel_static(const void* posm, int64_t n, double G, 
         set_global_error("eps must be >= 0 and G a number");
         return GSPH_E_INVALID;
     }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     void* base = nullptr;
-    const int rc = scratch_address(&base);
+    const int rc = scratch_address(s, &base);
     if (rc != GSPH_OK) return rc;
 
     const int64_t n_pad = (n + kPad - 1) / kPad * kPad;
@@ -114,24 +140,46 @@ extern "C" int gsph_gravity_accel_static(const void* posm, int64_t n, double G, 
     int* status = reinterpret_cast<int*>(b);
     float4* rec = reinterpret_cast<float4*>(b + kStatusBytes);
     float* part = reinterpret_cast<float*>(b + kStatusBytes + rec_bytes);
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
-    cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
-    if (e == cudaSuccess) {
-        k_static_pad<<<static_cast<unsigned>((n_pad + 255) / 256), 256, 0, s>>>(static_cast<const float4*>(posm), rec, n,
-                                                                                 n_pad);
-        e = cudaGetLastError();
-    }
+    // the status word starts at zero (or, for the failure-path test, with the timeout bit set)
+    const int status0 = g_inject_timeout.exchange(0) ? GSPH_DEV_ERR_TIMEOUT : 0;
+    k_static_pad<<<static_cast<unsigned>((n_pad + 255) / 256), 256, 0, s>>>(static_cast<const float4*>(posm), rec, n,
+                                                                             n_pad, status, status0);
+    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
         e = launch_gravity_raw(rec, part, n_pad, ipt, jt, nseg, static_cast<float>(eps * eps), status, s);
     if (e == cudaSuccess) {
         k_static_finish<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(part, static_cast<float4*>(acc), n, n_pad,
-                                                                                nseg, static_cast<float>(G));
+                                                                                nseg, static_cast<float>(G), status);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {
         set_global_error(std::string("gravity launch failed: ") + cudaGetErrorString(e));
         return GSPH_E_CUDA;
     }
+    return GSPH_OK;
+}
+
+extern "C" int gsph_gravity_accel_static_status(void* stream) {
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    void* base = nullptr;
+    const int rc = scratch_address(s, &base);
+    if (rc != GSPH_OK) return rc;
+    int st = 0;
+    cudaError_t e = cudaMemcpyAsync(&st, base, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_global_error(std::string("status read failed: ") + cudaGetErrorString(e));
+        return GSPH_E_CUDA;
+    }
+    if (st & GSPH_DEV_ERR_TIMEOUT) {
+        set_global_error("a device-side wait of gsph_gravity_accel_static gave up; its accelerations are NaN");
+        return GSPH_E_TIMEOUT;
+    }
+    return GSPH_OK;
+}
+
+extern "C" int gsph_inject_static_timeout(int on) {
+    g_inject_timeout.store(on ? 1 : 0);
     return GSPH_OK;
 }

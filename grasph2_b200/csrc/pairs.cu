@@ -514,10 +514,10 @@ __device__ __forceinline__ void gpart_sum(const float* part, int64_t n_pad, cons
             for (int k = 0; k < S; ++k, q += K)
                 for (int c = 0; c < 3; ++c) s[c] += static_cast<double>(q[c]) + static_cast<double>(q[3 + c]);
             for (int c = 0; c < 3; ++c) out[c] = s[c];
-        } else {
-            float s[3] = {0.0f, 0.0f, 0.0f};
+        } else {  // FP64: the slot sums can be large and cancel (a particle near the centre of mass)
+            double s[3] = {0.0, 0.0, 0.0};
             for (int k = 0; k < S; ++k, q += K)
-                for (int c = 0; c < 3; ++c) s[c] += q[c];
+                for (int c = 0; c < 3; ++c) s[c] += static_cast<double>(q[c]);
             for (int c = 0; c < 3; ++c) out[c] = s[c];
         }
         return;
@@ -583,6 +583,11 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) {
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) {
     uint64_t d;
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(u64_of(a)), "l"(u64_of(b)));
+    return f2_of(d);
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(u64_of(a)), "l"(u64_of(b)));
     return f2_of(d);
 }
 
@@ -671,8 +676,10 @@ __global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ p
 // CTA t is the task (ga, gb), ga <= gb (the G(G-1)/2 pairs of distinct groups first, then the G
 // diagonal ones): for every row block a of group ga it sweeps the column blocks of group gb (those
 // after a when ga == gb) in j-tiles of kSymJT through shared memory. One 1/r^3 serves both particles
-// of a pair: the row particle's sum stays in registers (f32x2, two row particles per instruction); the
-// column particle's contribution is summed over the CTA's 1024 row particles -- in the thread, then
+// of a pair: the row particle's sum stays in registers (f32x2, two row particles per instruction),
+// accumulated per j-tile and then added to the running sum (plain: a sum of 256-term sums, whose
+// rounding error grows with the tile count instead of the pair count; compensated: a two-sum fold whose
+// error terms live in shared memory); the column particle's contribution is summed over the CTA's 1024 row particles -- in the thread, then
 // across the warp by a butterfly that leaves kSymJB column sums spread over the lanes, then over the
 // four warps in shared memory -- and added to its slot in the partials (plain, or two-sum when
 // compensated). The pairs inside a block (the diagonal tile) run one-sided. Each particle has G + 1
@@ -681,8 +688,12 @@ __global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ p
 // scheduling. FMA-pipe work per pair interaction: 8 + ~0.4 operations
 // against the one-sided kernel's 12.
 constexpr int kSymT = 128, kSymI = 8, kSymB = kSymT * kSymI, kSymJT = 256;
-constexpr int kSymJB = 8;  // column particles per butterfly (8: 136 registers, three CTAs per SM; 4 fits four
-                           // CTAs but its longer butterflies cost more than the occupancy gains)
+// CTAs per SM the register budget is set for. Three: at four (128 registers) the pair loop spills a
+// little and the kernel runs no faster (Plummer N = 2^20: 337.9 vs 339.6 ms plain, 346.8 vs 343.5 ms
+// compensated)
+constexpr int kSymCtas = 3;
+constexpr int kSymJB = 8;  // column particles per butterfly (8: three CTAs per SM; 4 fits four CTAs but its
+                           // longer butterflies cost more than the occupancy gains)
 
 // NV values per lane (NV = 4 or 8) -> lane l holds the warp's sum of value (l >> (5 - log2 NV)) & (NV - 1):
 // a butterfly that halves the values at each of the first log2 NV levels (fixed order, so the sums are
@@ -735,12 +746,16 @@ __host__ __device__ __forceinline__ void sym_task(int t, int G, int& ga, int& gb
 }
 
 template <int GRAV, bool COMP>
-__global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict__ posm, float* __restrict__ part,
+__global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* __restrict__ posm, float* __restrict__ part,
                                                        int64_t n_pad, int G, int gs, float eps2) {
     constexpr int P = kSymI / 2;
     constexpr int K = COMP ? 6 : 3;
     __shared__ float4 J[kSymJT];
     __shared__ float js[kSymT / 32][kSymJT][3];
+    // the row particles' running sums (and, compensated, their rounding-error terms) stay in shared
+    // memory, touched once per j-tile; the pair loop keeps only the tile's partials in registers
+    __shared__ float2 rsh[3 * P][kSymT];
+    __shared__ float2 csh[COMP ? 3 * P : 1][kSymT];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int ga, gb;
     sym_task(static_cast<int>(blockIdx.x), G, ga, gb);
@@ -763,15 +778,15 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
 
     for (int a = ra0; a < ra1; ++a) {
         const int64_t base = static_cast<int64_t>(a) * kSymB + tid;
-        float2 X[P], Y[P], Z[P], MI[P], AX[P], AY[P], AZ[P], CX[P], CY[P], CZ[P];
+        float2 X[P], Y[P], Z[P], MI[P];
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const float4 u = posm[base + static_cast<int64_t>(2 * k) * kSymT];
             const float4 w = posm[base + static_cast<int64_t>(2 * k + 1) * kSymT];
             X[k] = make_float2(u.x, w.x); Y[k] = make_float2(u.y, w.y); Z[k] = make_float2(u.z, w.z);
             MI[k] = make_float2(-u.w, -w.w);
-            AX[k] = AY[k] = AZ[k] = make_float2(0.0f, 0.0f);
-            CX[k] = CY[k] = CZ[k] = make_float2(0.0f, 0.0f);
+            rsh[k][tid] = rsh[P + k][tid] = rsh[2 * P + k][tid] = make_float2(0.0f, 0.0f);
+            if (COMP) csh[k][tid] = csh[P + k][tid] = csh[2 * P + k][tid] = make_float2(0.0f, 0.0f);
         }
         // tiles: the block's own (one-sided) when diagonal, then the columns
         const int64_t d0 = static_cast<int64_t>(a) * kSymB;
@@ -811,11 +826,7 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
                         float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
                         if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
                         const float2 sj = mul2(qm, mul2(mul2(inv, inv), inv));
-                        if (COMP) {
-                            TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
-                        } else {
-                            AX[m] = fma2(dx, sj, AX[m]); AY[m] = fma2(dy, sj, AY[m]); AZ[m] = fma2(dz, sj, AZ[m]);
-                        }
+                        TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
                     }
                 }
             } else {
@@ -836,11 +847,7 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
                             if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
                             const float2 i3 = mul2(mul2(inv, inv), inv);
                             const float2 sj = mul2(qm, i3), si = mul2(MI[m], i3);
-                            if (COMP) {
-                                TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
-                            } else {
-                                AX[m] = fma2(dx, sj, AX[m]); AY[m] = fma2(dy, sj, AY[m]); AZ[m] = fma2(dz, sj, AZ[m]);
-                            }
+                            TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
                             tx = fma2(dx, si, tx); ty = fma2(dy, si, ty); tz = fma2(dz, si, tz);
                         }
                         vx[jj] = tx.x + tx.y;
@@ -859,13 +866,21 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
                     }
                 }
             }
-            if (COMP) {
+            // the tile's row partials into the running sums: a two-sum fold (compensated), or one add
+            // (plain: a sum of 256-term tile sums, not one running sum over the whole column group)
 #pragma unroll
-                for (int m = 0; m < P; ++m) {
-                    fold(AX[m].x, CX[m].x, TX[m].x); fold(AX[m].y, CX[m].y, TX[m].y);
-                    fold(AY[m].x, CY[m].x, TY[m].x); fold(AY[m].y, CY[m].y, TY[m].y);
-                    fold(AZ[m].x, CZ[m].x, TZ[m].x); fold(AZ[m].y, CZ[m].y, TZ[m].y);
+            for (int m = 0; m < P; ++m) {
+                float2 ax = rsh[m][tid], ay = rsh[P + m][tid], az = rsh[2 * P + m][tid];
+                if (COMP) {
+                    float2 cx = csh[m][tid], cy = csh[P + m][tid], cz = csh[2 * P + m][tid];
+                    fold(ax.x, cx.x, TX[m].x); fold(ax.y, cx.y, TX[m].y);
+                    fold(ay.x, cy.x, TY[m].x); fold(ay.y, cy.y, TY[m].y);
+                    fold(az.x, cz.x, TZ[m].x); fold(az.y, cz.y, TZ[m].y);
+                    csh[m][tid] = cx; csh[P + m][tid] = cy; csh[2 * P + m][tid] = cz;
+                } else {
+                    ax = add2(ax, TX[m]); ay = add2(ay, TY[m]); az = add2(az, TZ[m]);
                 }
+                rsh[m][tid] = ax; rsh[P + m][tid] = ay; rsh[2 * P + m][tid] = az;
             }
             if (k >= nd) {  // this tile's column sums over the CTA's row block, into the column slot
                 __syncthreads();
@@ -901,13 +916,13 @@ __global__ void __launch_bounds__(kSymT) k_gravity_sym(const float4* __restrict_
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 float* out = slot(base + static_cast<int64_t>(2 * m + h) * kSymT, s_row);
-                out[0] = h ? AX[m].y : AX[m].x;
-                out[1] = h ? AY[m].y : AY[m].x;
-                out[2] = h ? AZ[m].y : AZ[m].x;
+                out[0] = h ? rsh[m][tid].y : rsh[m][tid].x;
+                out[1] = h ? rsh[P + m][tid].y : rsh[P + m][tid].x;
+                out[2] = h ? rsh[2 * P + m][tid].y : rsh[2 * P + m][tid].x;
                 if (COMP) {
-                    out[3] = h ? CX[m].y : CX[m].x;
-                    out[4] = h ? CY[m].y : CY[m].x;
-                    out[5] = h ? CZ[m].y : CZ[m].x;
+                    out[3] = h ? csh[m][tid].y : csh[m][tid].x;
+                    out[4] = h ? csh[P + m][tid].y : csh[P + m][tid].x;
+                    out[5] = h ? csh[2 * P + m][tid].y : csh[2 * P + m][tid].x;
                 }
             }
         }

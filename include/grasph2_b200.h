@@ -523,8 +523,20 @@ int gsph_profile_reset(gsph_ctx* ctx);
  * GSPH_E_INVALID and a message in gsph_last_error(NULL). The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress); make that first call before any stream capture.
  * Every call on a device shares the array and leaves the last call's data in it: calls whose
- * kernels may overlap on the GPU (different streams without ordering) race. Asynchronous on `stream`. */
+ * kernels may overlap on the GPU (different streams without ordering) race. Asynchronous on `stream`.
+ * Outside stream capture every call looks the address up again (a device reset moves the array).
+ * Failure: if a bounded device-side wait of the gravity kernel gave up (2 s), part of the sum is
+ * missing; the call then writes NaN into every component of acc instead of a partial result, and
+ * gsph_gravity_accel_static_status reports GSPH_E_TIMEOUT. */
 int gsph_gravity_accel_static(const void* posm, int64_t n, double G, double eps, void* acc, void* stream);
+/* Status of the last gsph_gravity_accel_static call on the current device: synchronises `stream`
+ * and returns GSPH_OK, or GSPH_E_TIMEOUT when a device-side wait of that call gave up (allocates
+ * nothing). */
+int gsph_gravity_accel_static_status(void* stream);
+/* Failure-path test hook: with on != 0, the next gsph_gravity_accel_static call starts with the
+ * timeout bit already set in its status word, as if a device-side wait had given up (no wait is
+ * made to run out). One-shot. */
+int gsph_inject_static_timeout(int on);
 
 /* FP32 FFMA throughput of the current device, measured by a dependent-chain-free FMA kernel
  * running for about `seconds` (the roofline denominator of the FP32-bound pair kernels).

@@ -24,7 +24,8 @@ from grasph2_b200._abi import FLAG_BITS as F
 from grasph2_b200.params import config0_params, config1_params, config2_params, make_options, make_params
 from grasph2_b200.sim import DeviceParticleBuffer, GsphError
 from grasph2_b200.state import as_dtype
-from helpers import check_within, copy_state, f32_exact, fp32_sensitivity, golden_state, rel_max
+from helpers import (NORM_LOG, check_within, copy_state, f32_exact, fp32_sensitivity, golden_state, rel_max,
+                     vec_rel)
 
 pytestmark = pytest.mark.gpu
 
@@ -205,17 +206,20 @@ def test_config1_subsample_vs_oracle(oracle):
 
 @pytest.mark.slow
 def test_config2_gravity_subsample_vs_oracle(oracle):
-    """Plummer sphere N=1,048,576: accelerations of 1024 seeded targets vs FP64 (all sources). The
-    compensated form meets 1e-5; plain FP32 accumulation of 2^20 terms is held to 5e-5 and its error
-    is reported by the error study."""
+    """Plummer sphere N=1,048,576: accelerations of a seeded 16,384-particle target subsample vs FP64
+    (all N sources); both the plain and the compensated FP32 forms are held to the 1e-5 norm-wise bound
+    and their errors are logged."""
     p = config2_params()
     st = f32_exact(ics.plummer_sphere(1 << 20, seed=20261205))
-    idx = np.random.default_rng(1).choice(1 << 20, 1024, replace=False)
+    idx = np.random.default_rng(1).choice(1 << 20, 16384, replace=False)
     ref = oracle.gravity_targets(p, st["pos"], st["mass"], idx)
-    for accum, tol in (("compensated", TOL_ACC), ("plain", 5e-5)):
+    for accum in ("plain", "compensated"):
         got = gpu_derivatives(p, st, accum)
         e = rel_max(got["acc"][idx], ref)
-        assert e <= tol, "config2 %s: %.3e > %.1e" % (accum, e, tol)
+        v = vec_rel(got["acc"][idx], ref)
+        NORM_LOG.append("config2 Plummer N=2^20 %-11s acc: max|da|/max|a| %.3e, max_i |da_i|/rms|a| %.3e "
+                        "(16384 targets)" % (accum, e, v))
+        assert e <= TOL_ACC, "config2 %s: %.3e > %.1e" % (accum, e, TOL_ACC)
 
 
 def test_graph_step_matches_eager():
