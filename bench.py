@@ -1,12 +1,17 @@
 """Benchmark of the per-step hot path: one JSON line on rank 0.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload impact|fluid|plummer]
-                    [--accum plain|compensated] [--no-cpu-baseline]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload plummer|impact|fluid|ensemble|surrogate|mlp] [--accum plain|compensated]
+                    [--legs auto|none|impact,ensemble,surrogate] [--no-cpu-baseline]
 
-Workload (default): the elastic-plastic two-sphere impact at N = 65,536 (R = 1 with 58,254 particles and
-R = 0.5 with 7,282, relative velocity 0.5 along x, y-offset 0.3, rho0 = 1, Murnaghan K = 10, shear 5,
-von Mises Y = 0.5, AV alpha = 1 beta = 2, h = 2.5 x mean spacing, G = 1, eps = 0.01, dt = 1e-4), seeded
-synthetic initial conditions. A step is computeDerivatives + integrate (the captured step graph).
+Workload (default): the pure N-body Plummer sphere at N = 1,048,576 (scale radius a = 1, masses 1/N,
+velocities from the Plummer distribution function, G = 1, eps = 0.01, dt = 1e-3), seeded synthetic
+initial conditions: the plain FP32 all-pairs path whose throughput is quoted against the FP32 peak. A
+step is computeDerivatives + integrate (the captured step graph). At one GPU the default run adds the
+other workloads as legs of the same line ("workloads"): the elastic-plastic two-sphere impact at
+N = 65,536 with its energy drift over 1,000 steps against the FP64 form, the batched ensemble of 512
+spheres against the same simulations run one by one, and the learned K = 8 surrogate at N = 262,144
+against the plain solver.
 
 Timing: W untimed steps, then K steps, each bracketed by CUDA events on the launching stream, with a
 256 MiB write between steps (outside the events) to flush the 126 MB L2; barrier + synchronize on both
@@ -14,7 +19,8 @@ sides; the max over ranks. N > 1 runs independent replicas (the path is not shar
 reports the whole-job rate.
 
 --impl reference times GraSPH2's own CPU hot path (its job headers compiled for the host with OpenMP,
-oracle/_ref) on this machine's cores, on bounded row samples of the same workload, extrapolated.
+oracle/_ref) on this machine's cores, on bounded row samples of the same workload, extrapolated. The
+cpu_baseline of our arm is that same reference arm, run as a child process.
 """
 
 import argparse
@@ -23,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -32,8 +39,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "steps/s & pair-interactions/s, chosen vs plain form at ≤1e-4 energy drift"
 
-# Algorithmic flop model (frozen; derivation in DESIGN.md): per pair of the N^2 sweep and per
-# neighbour pair (0 < r <= h) of the SPH passes.
+# Algorithmic flop model (frozen): per pair of the N^2 sweep and per neighbour pair (0 < r <= h) of
+# the SPH passes.
 FLOP_GRAV_PAIR = 20        # softened gravity, the GPU Gems 3 ch. 31 convention
 FLOP_DENS_PAIR = 8         # distance test of the density sum
 FLOP_DENS_NB = 10          # W(r) and the accumulation per neighbour
@@ -42,26 +49,30 @@ FLOP_ACC_NB = 60           # pressure acceleration + AV per neighbour (fluid, ac
 
 FLUSH_BYTES = 256 << 20
 
-# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture of the same workload:
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none \
-#       -k regex:"k_gravity_sym|k_gravity_x2|k_pairs_items|k_density_items" -s 9 -c 6 --csv \
-#       python bench.py --steps 5 --warmup 3 --no-cpu-baseline --no-e2e --no-peak --drift-steps 0 --no-autotune
-# (with --gravity one-sided for the one-sided kernel). On the impact the symmetric kernel reads 1.08 MB
-# (the 1.05 MB of j-records: no re-reads) and writes 0.95-2.02 MB of its partial slots (the
-# rest stays in L2); the one-sided kernel reads 1.06-1.08 MB and writes nothing.
-MEASURED_TRAFFIC = {("impact", 65536, "gravity", "symmetric"): 2.56e6,
-                    ("impact", 65536, "gravity", "one-sided"): 1.08e6}
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture of the same kernel
+# and launch shape on a smaller case (profiles/ holds the command): key (workload, kernel slot, gravity
+# form, symmetric groups) -> (bytes per launch, particles of the captured case). The symmetric gravity
+# kernel's traffic is its j-records (16 B per particle, read once from DRAM, then from L2) plus its
+# partial slots ((G + 1) x 12 B per particle, written once), so at fixed G it scales with N.
+MEASURED_TRAFFIC = {
+    ("plummer", "gravity", "symmetric", 128): (682673280.0, 262144),  # ncu, N = 262,144, 2 launches (mean)
+}
 FLAG_DEAL_WITH_NO_PARTNERS = 1 << 3  # GSPH_DEAL_WITH_NO_PARTNERS
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
-    ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["impact", "fluid", "plummer", "ensemble", "surrogate", "mlp"],
-                    default="impact")
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-cuda"], default="ours",
+                    help="ours; reference = GraSPH2's CPU hot path on the host cores (the reference arm); "
+                         "reference-cuda = GraSPH2's own CUDA path built for sm_100a (N % 256 == 0 only)")
+    ap.add_argument("--workload", choices=["plummer", "impact", "fluid", "ensemble", "surrogate", "mlp"],
+                    default="plummer")
+    ap.add_argument("--legs", default="auto",
+                    help="other workloads measured in the same run at one GPU (comma list of impact, ensemble, "
+                         "surrogate; 'auto' = all three for the default Plummer workload, 'none' = off)")
     ap.add_argument("--windows", type=int, default=8, help="surrogate: windows of M proposals")
     ap.add_argument("--model", default=os.path.join(ROOT, "grasph2_b200", "data", "surrogate_impact_n262144.npz"),
                     help="surrogate: trained model (grasph2_b200/train_surrogate.py)")
@@ -70,7 +81,10 @@ def parse():
                     help="ensemble: skip timing the simulations one by one in their own contexts")
     ap.add_argument("--accum", choices=["plain", "compensated"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of CPU work for the cpu_baseline (the reference arm run as a child process)")
+    ap.add_argument("--ref-budget", type=float, default=100.0,
+                    help="--impl reference: seconds of CPU work over all warm-up and timed steps")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak probe (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="particle count of the fluid / plummer workloads")
@@ -79,15 +93,17 @@ def parse():
     ap.add_argument("--scalar-fp32", action="store_true", help="scalar instead of paired f32x2 gravity kernel")
     ap.add_argument("--gravity", choices=["auto", "one-sided", "symmetric"], default="auto",
                     help="all-pairs gravity kernel: every ordered pair, or every unordered pair once")
+    ap.add_argument("--gravity-groups", type=int, default=0, help="symmetric gravity: particle groups (0 = auto)")
     ap.add_argument("--drift-steps", type=int, default=-1,
                     help="steps of the energy-drift comparison (plain, compensated, FP64); default 1000 on the "
                          "impact workload, 0 (off) elsewhere")
     ap.add_argument("--drift-every", type=int, default=100, help="steps between energy samples of the drift run")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ---- workloads ------------------------------------------------------------------------------------
 def workload(name, n=0):
+    """(params, state, description, reference variant) of a single-context workload."""
     from grasph2_b200 import ics
     from grasph2_b200.params import config0_params, config1_params, config2_params
     if name == "impact":
@@ -101,7 +117,7 @@ def workload(name, n=0):
         return config0_params(), st, "SPH + self-gravity fluid sphere, N=%d, h=0.15, eps=0.02" % n, "fluid"
     n = n or (1 << 20)
     st = ics.plummer_sphere(n, seed=20261203)
-    return config2_params(), st, "Plummer sphere N-body, N=%d, a=1, eps=0.01, dt=1e-3" % n, "nbody"
+    return config2_params(), st, "Plummer sphere N-body, N=%d, a=1, eps=0.01, dt=1e-3" % n, "plummer"
 
 
 def flops_per_step(params, st, counts, culled):
@@ -151,8 +167,7 @@ class ClockSampler:
 
     def __init__(self, device_index):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        self.path = os.path.join(tempfile.gettempdir(), "grasph2_clocks_%d.csv" % os.getpid())
         sel = self._selector(device_index)
         try:
             self.fh = open(self.path, "w")
@@ -182,7 +197,13 @@ class ClockSampler:
             self.proc.kill()
         self.fh.close()
         rows = []
-        for line in open(self.path):
+        with open(self.path) as fh:
+            lines = fh.readlines()
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 8:
                 continue
@@ -204,110 +225,190 @@ class ClockSampler:
 
 
 # ---- CPU reference timing ------------------------------------------------------------------------
-def cpu_reference_sample(variant, st, budget_s, rows_hint=None):
-    """Time the reference's own hot path (oracle/_ref, FP32 as shipped, OpenMP on all host cores) on
-    target-row samples of the workload; return (steps/s extrapolated, description, cores, kind)."""
+def reference_step_sampler(variant, st):
+    """A timing sampler of the reference's own hot path (oracle/_ref, FP32 as shipped, OpenMP on all host
+    cores): sample(m) runs computeDerivatives over target rows [0, m) (every pass, the density sum
+    included) and integrate over all N, and returns (seconds of the row pass, seconds of integrate).
+    Falls back to the FP64 oracle port (kind "port") where the reference build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from grasph2_b200.state import as_dtype
-    n = st["mass"].shape[0]
-    cores = os.cpu_count() or 1
     if pyoracle.ref_available(variant):
         R = pyoracle.RefBuild(variant, double=False)
         s32 = as_dtype(st, np.float32)
-        kind = "reference"
 
         def sample(m):
             t0 = time.perf_counter()
             R.compute_derivatives_rows(s32, 0, m)
-            return time.perf_counter() - t0
+            t1 = time.perf_counter()
+            R.integrate(s32, True)
+            return t1 - t0, time.perf_counter() - t1
+        return sample, "reference"
+    if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
+        return None, None
+    O = pyoracle.Oracle()
+    params = workload(variant, st["mass"].shape[0])[0]
+    s64 = as_dtype(st, np.float64)
 
+    def sample(m):
         t0 = time.perf_counter()
-        R.integrate(as_dtype(st, np.float32), True)
-        t_int = time.perf_counter() - t0
-    else:
-        O = pyoracle.Oracle()
-        kind = "port"
-        from grasph2_b200.params import config1_params
-        p = config1_params()
-        s64 = as_dtype(st, np.float64)
+        O.compute_derivatives(params, s64, 0, m)
+        t1 = time.perf_counter()
+        O.integrate(params, s64, True)
+        return t1 - t0, time.perf_counter() - t1
+    return sample, "port"
 
-        def sample(m):
-            t0 = time.perf_counter()
-            O.compute_derivatives(p, s64, 0, m)
-            return time.perf_counter() - t0
 
-        t_int = 0.0
-    m = rows_hint or 64
-    t = sample(m)
-    while t < 0.2 * budget_s and m < n:
-        m = min(n, int(m * max(2.0, 0.5 * budget_s / max(t, 1e-3))))
-        t = sample(m)
-    per_step = t * n / m + t_int
-    desc = ("computeDerivatives on target rows [0, %d) of N=%d (all passes), %.2f s, plus integrate of all N; "
-            "extrapolated x N/rows" % (m, n, t))
-    return 1.0 / per_step, desc, cores, kind, m
+def rows_for_budget(sample, n, budget_s):
+    """Target rows whose row pass takes about budget_s seconds (doubling from 64 rows)."""
+    m = 64
+    t = sample(m)[0]
+    while t < 0.5 * budget_s and m < n:
+        m = min(n, int(m * max(2.0, 0.7 * budget_s / max(t, 1e-3))))
+        t = sample(m)[0]
+    return m
+
+
+def cpu_baseline_child(workload_name, n, budget_s):
+    """The reference arm (--impl reference) on the same workload, run as a child process so that it has
+    the host to itself (no CUDA context or GPU-side threads in the process): its steps/s is the
+    cpu_baseline of our arm."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", workload_name,
+           "--steps", "3", "--warmup", "1", "--ref-budget", str(budget_s)]
+    if n:
+        cmd += ["--n", str(n)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE")}
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=30 + 6 * budget_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "reference arm timed out"}
+    for line in reversed(r.stdout.strip().splitlines()):
+        try:
+            d = json.loads(line)
+        except ValueError:
+            continue
+        if "cpu_baseline" in d:
+            return dict(d["cpu_baseline"], child="bench.py --impl reference --steps 3 --warmup 1 --ref-budget %g"
+                        % budget_s)
+        if "unavailable" in d:
+            return {"unavailable": d["unavailable"]}
+    return {"unavailable": "reference arm printed no line (rc %d): %s" % (r.returncode, r.stderr[-300:])}
+
+
+def reference_line(args, value, t_rows, t_int, m, n, cores, kind, desc, workload_desc, pairs):
+    return {
+        "metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": dict(workload_desc, sample=desc),
+        "pair_interactions_per_s": pairs * value,
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind, "sample": desc,
+                         "row_pass_s": t_rows, "integrate_s": t_int},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
 
 
 def run_reference_arm(args, rank, world):
+    """GraSPH2's own CPU hot path on this host's cores, on the workload of our arm: each step times
+    computeDerivatives over a bounded row sample (extrapolated x N/rows, as the pair passes cost N per
+    row) plus integrate over all N; steps/s = 1 / the mean of those step times."""
     if world > 1 and rank != 0:
-        return
+        return None
+    cores = os.cpu_count() or 1
+    if args.workload in ("surrogate", "mlp"):
+        return {"impl": "reference", "unavailable": "the reference has no %s" % args.workload}
     if args.workload == "ensemble":  # the reference's host path on the largest simulation, scaled by sum N_k^2
         params, sizes, states, desc = ensemble_workload(args.nsims)
         big = int(np.argmax(sizes))
         scale = float((sizes.astype(np.float64) ** 2).sum()) / float(sizes[big]) ** 2
-        rate, sdesc, cores, kind, _ = cpu_reference_sample("fluid", states[big], 20.0)
-        value = rate / scale
-        line = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": desc, "nsims": int(len(sizes)), "n_total": int(sizes.sum())},
-            "pair_interactions_per_s": float((sizes.astype(np.float64) ** 2).sum()) * value,
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
-                             "sample": "largest simulation N=%d: %s; scaled by sum N_k^2 / N^2 = %.1f"
-                                       % (int(sizes[big]), sdesc, scale)},
-            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line))
-        return
-    params, st, desc, variant = workload(args.workload, args.n)
+        st = states[big]
+        variant = "fluid"
+        wdesc = {"workload": desc, "nsims": int(len(sizes)), "n_total": int(sizes.sum())}
+        pairs = float((sizes.astype(np.float64) ** 2).sum())
+    else:
+        params, st, desc, variant = workload(args.workload, args.n)
+        scale = 1.0
+        wdesc = {"workload": desc, "n": int(st["mass"].shape[0])}
+        pairs = flops_pairs(params, st["mass"].shape[0])
+    sample, kind = reference_step_sampler(variant, st)
+    if sample is None:
+        return {"impl": "reference", "unavailable": "neither oracle/_ref nor oracle/liboracle.so is built"}
     n = st["mass"].shape[0]
+    per = max(0.05, args.ref_budget / float(args.steps + args.warmup + 2))
+    m = rows_for_budget(sample, n, per)
+    rows, ints = [], []
+    for k in range(args.warmup + args.steps):
+        tr, ti = sample(m)
+        if k >= args.warmup:
+            rows.append(tr)
+            ints.append(ti)
+    t_rows = sum(rows) / len(rows)
+    t_int = sum(ints) / len(ints)
+    t_step = (t_rows * n / m + t_int) * scale
+    value = 1.0 / t_step
+    sdesc = ("GraSPH2 host jobs (FP32, OpenMP, %d threads): computeDerivatives on target rows [0,%d) of N=%d per "
+             "step, extrapolated x N/rows, plus integrate of all N" % (cores, m, n))
+    if kind == "port":
+        sdesc = sdesc.replace("GraSPH2 host jobs (FP32,", "FP64 oracle port (")
+    if scale != 1.0:
+        sdesc += "; the largest simulation, scaled by sum N_k^2 / N^2 = %.1f" % scale
+    return reference_line(args, value, t_rows, t_int, m, n, cores, kind, sdesc, wdesc, pairs)
+
+
+def run_reference_cuda(args, rank, world):
+    """GraSPH2's own CUDA path (oracle/_ref/libref_cuda_<variant>.so: its tile kernels, jobs and
+    integrator compiled for sm_100a) on our arm's workload, where the reference can express it (its
+    softening is eps == h and its AV signal coefficient 3; the cost per pair is the same). Steps are
+    {computeDerivatives; integrate(true)} timed with CUDA events; valid for N % 256 == 0 only."""
+    if world > 1 and rank != 0:
+        return None
+    if args.workload not in ("plummer", "impact", "fluid"):
+        return {"impl": "reference-cuda", "unavailable": "no single-simulation reference run for %s" % args.workload}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    if not pyoracle.ref_available(variant) and not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
-        print(json.dumps({"impl": "reference", "unavailable": "neither oracle/_ref nor oracle/liboracle.so is built"}))
-        return
-    total_budget = 150.0
-    per = max(0.05, total_budget / float(args.steps + args.warmup + 2))
-    rate0, _, cores, kind, m = cpu_reference_sample(variant, st, per)
-    times = []
+    import torch
     from grasph2_b200.state import as_dtype
-    if kind == "reference":
-        R = pyoracle.RefBuild(variant, double=False)
-        s32 = as_dtype(st, np.float32)
-        for k in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            R.compute_derivatives_rows(s32, 0, m)
-            dt = time.perf_counter() - t0
-            if k >= args.warmup:
-                times.append(dt)
-    else:
-        times = [1.0 / rate0] * args.steps
-    t_step = (sum(times) / len(times)) * n / m
-    value = 1.0 / t_step
-    pairs = flops_pairs(params, n)
-    line = {
-        "metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": desc, "n": n, "sample": "rows [0,%d) per step, extrapolated x N/rows" % m},
-        "pair_interactions_per_s": pairs * value,
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
-                         "sample": "GraSPH2 host jobs (FP32, OpenMP) on rows [0,%d) of N=%d per step" % (m, n)},
-        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line))
+    params, st, desc, variant = workload(args.workload, args.n)
+    n = st["mass"].shape[0]
+    if not pyoracle.ref_cuda_available(variant):
+        return {"impl": "reference-cuda", "unavailable": "oracle/_ref/libref_cuda_%s.so is not built" % variant}
+    if n % 256:
+        return {"impl": "reference-cuda", "unavailable": "N=%d is not a multiple of 256 (algorithms.h:285-301)" % n}
+    torch.cuda.init()
+    with pyoracle.RefCuda(variant, n) as r:
+        r.upload(as_dtype(st, np.float32))
+        r.set_timestep(0.0, 0.0)
+        t1 = r.time_steps(1)  # warm-up, and the size of one step
+        steps = int(max(1, min(args.steps, 4000.0 / max(t1, 1e-3))))
+        ms = r.time_steps(steps)
+    value = steps / (ms * 1e-3)
+    return {"metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference-cuda", "n_gpus": 1,
+            "steps": steps, "warmup": 1, "ms_per_step": ms / steps, "higher_is_better": True, "dtype": "f32",
+            "config": {"workload": desc, "n": n, "reference_variant": variant},
+            "pair_interactions_per_s": flops_pairs(params, n) * value,
+            "note": "GraSPH2's CUDA path recompiled for sm_100a (one thread per particle, 256-particle shared-memory "
+                    "tiles), the reference's physics constants of this workload (eps == h, AV signal coefficient 3)"}
+
+
+def reference_cuda_child(workload_name, n, steps):
+    """run_reference_cuda in a child process: the reference's CUDA module stays out of our arm's process."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference-cuda", "--workload", workload_name,
+           "--steps", str(steps), "--warmup", "1"]
+    if n:
+        cmd += ["--n", str(n)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE")}
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=300)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "reference CUDA run timed out"}
+    for line in reversed(r.stdout.strip().splitlines()):
+        try:
+            d = json.loads(line)
+        except ValueError:
+            continue
+        d.pop("metric", None)
+        return d
+    return {"unavailable": "reference CUDA run printed no line (rc %d): %s" % (r.returncode, r.stderr[-300:])}
 
 
 def max_over_ranks(x, dist=None, device=None):
@@ -581,19 +682,14 @@ def run_ensemble(args, rank, world, local):
         ens.close()
         if dist is not None:
             dist.destroy_process_group()
-        return
+        return None
     value = whole_job_rate(args.steps, world, total_ms)
     nb = sum(neighbour_pairs(s["pos"], params.H, dev) for s in states[::8]) * 8
     flops = FLOP_GRAV_PAIR * pairs + FLOP_DENS_PAIR * pairs + (FLOP_DENS_NB + FLOP_ACC_NB) * nb
     achieved = flops / (ms_per_step * 1e-3) / 1e12
     cpu = None
     if not args.no_cpu_baseline:
-        big = int(np.argmax(sizes))
-        rate, sdesc, cores, kind, _ = cpu_reference_sample("fluid", states[big], args.cpu_budget)
-        scale = pairs / float(sizes[big]) ** 2
-        cpu = {"value": rate / scale, "unit": "steps/s", "cores": cores, "kind": kind,
-               "sample": "the largest simulation (N=%d): %s; the ensemble step scaled by sum N_k^2 / N^2 = %.1f"
-                         % (int(sizes[big]), sdesc, scale)}
+        cpu = cpu_baseline_child("ensemble", 0, args.cpu_budget)
     drift = None
     if args.drift_steps != 0:
         nd = args.drift_steps if args.drift_steps > 0 else 1000
@@ -636,10 +732,10 @@ def run_ensemble(args, rank, world, local):
                  "d2h_bytes_per_step": d2h} if e2e_steps else None),
         "gpu_launches": gpu_launches,
     }
-    print(json.dumps(line))
     ens.close()
     if dist is not None:
         dist.destroy_process_group()
+    return line
 
 
 def run_surrogate(args, rank, world, local):
@@ -657,10 +753,9 @@ def run_surrogate(args, rank, world, local):
     from grasph2_b200.params import CONFIG4_N_BIG, CONFIG4_N_SMALL, config4_params
     from grasph2_b200.sim import DeviceParticleBuffer
     if rank != 0:
-        return
+        return None
     if not os.path.exists(args.model):
-        print(json.dumps({"metric": METRIC, "error": "trained model missing: %s" % args.model}))
-        sys.exit(1)
+        raise RuntimeError("trained model missing: %s" % args.model)
     sur = S.Surrogate.load(args.model)
     p = config4_params()
     n = CONFIG4_N_BIG + CONFIG4_N_SMALL
@@ -731,7 +826,7 @@ def run_surrogate(args, rank, world, local):
         "clocks": clocks,
         "gpu_launches": out["surrogate"]["library_launches"],
     }
-    print(json.dumps(line))
+    return line
 
 
 MLP_FWD_FLOPS = 2 * (32 * 128 + 2 * 128 * 128 + 128 * 13)                  # per row
@@ -745,7 +840,7 @@ def run_mlp(args, rank, world, local):
     torch.cuda.set_device(local)
     from grasph2_b200.mlp import MLP, init_params
     if rank != 0:
-        return
+        return None
     nf, nt = 1 << 20, 1 << 18
     g = torch.Generator(device="cuda").manual_seed(1)
     x = torch.randn(nf, 32, device="cuda", generator=g)
@@ -782,54 +877,59 @@ def run_mlp(args, rank, world, local):
                          "unit": "TFLOP/s", "frac": res["forward"]["tflops"] / peak, "traffic": None,
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS burst)"},
             "gpu_launches": args.steps * 3}
-    print(json.dumps(line))
+    return line
 
 
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        run_reference_arm(args, rank, world)
-        return
+_PEAK = {}
 
-    if args.workload == "ensemble":
-        run_ensemble(args, rank, world, local)
-        return
-    if args.workload == "surrogate":
-        run_surrogate(args, rank, world, local)
-        return
-    if args.workload == "mlp":
-        run_mlp(args, rank, world, local)
-        return
+
+def fp32_peak(args):
+    """FFMA throughput of this GPU (gsph_measure_fp32_peak), measured once per process."""
+    if args.no_peak:
+        return None
+    if "tflops" not in _PEAK:
+        from grasph2_b200.sim import measure_fp32_peak
+        _PEAK["tflops"] = measure_fp32_peak(0.5)
+    return _PEAK["tflops"]
+
+
+def shape_options(shape, opts):
+    """Options that reproduce an autotuned all-pairs gravity shape (gravity-only workloads)."""
+    o = dict(opts)
+    if shape.get("grav_sym_groups"):
+        o.update(gravity="symmetric", gravity_groups=int(shape["grav_sym_groups"]))
+    else:
+        o.update(gravity="one-sided", i_per_thread=int(shape["grav_ipt"]), j_tile=int(shape["grav_jt"]),
+                 j_split=int(shape["grav_nseg"]))
+    return o
+
+
+def run_context(args, rank, world, local, dist=None):
+    """One simulation context (the Plummer, impact or fluid workload): the timed steps, the e2e leg, the
+    roofline of the dominant kernel, the CPU baseline and (impact) the energy drift. Returns the line
+    on rank 0."""
     import torch
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-
     from grasph2_b200.params import make_options
-    from grasph2_b200.sim import DeviceParticleBuffer, measure_fp32_peak
+    from grasph2_b200.sim import DeviceParticleBuffer
 
     params, st, desc, variant = workload(args.workload, args.n)
     n = st["mass"].shape[0]
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
-
-    peak_tflops = None if args.no_peak else measure_fp32_peak(0.5)
+    peak_tflops = fp32_peak(args)
+    gravity_only = not (params.flags & 2)
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    opts = dict(accum=args.accum, cull=not args.no_cull, scalar_fp32=args.scalar_fp32, gravity=args.gravity)
+    opts = dict(accum=args.accum, cull=not args.no_cull, scalar_fp32=args.scalar_fp32, gravity=args.gravity,
+                gravity_groups=args.gravity_groups)
     pb = DeviceParticleBuffer(params, n, make_options(**opts))
     pb.upload(st, stream=stream)
-    shape = pb.launch_shape() if args.no_autotune else pb.autotune(3, stream)
+    # gravity-only at large N: each candidate launch is a full N^2 sweep, so one timed launch per shape
+    shape = pb.launch_shape() if args.no_autotune else pb.autotune(1 if gravity_only and n > 65536 else 3, stream)
     pb.profile_enable(True)
     for _ in range(args.warmup):
         flush.zero_()
@@ -859,8 +959,8 @@ def main():
     prof = pb.profile_read()
 
     # e2e: the public API with host buffers (pinned): upload inputs, one step, download the result
-    up_names = ["pos", "mass", "vel", "density", "dstress"]
-    down_names = ["pos", "vel", "acc", "density", "dstress"]
+    up_names = ["pos", "mass", "vel"] + ([] if gravity_only else ["density", "dstress"])
+    down_names = ["pos", "vel", "acc"] + ([] if gravity_only else ["density", "dstress"])
     from grasph2_b200.state import new_state
     pinned_in = {k: torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float32)).pin_memory().numpy()
                  for k in up_names}
@@ -868,14 +968,17 @@ def main():
     pinned_out = {k: torch.empty(host_out[k].shape, dtype=torch.float32).pin_memory().numpy() for k in down_names}
     h2d = sum(a.nbytes for a in pinned_in.values())
     d2h = sum(a.nbytes for a in pinned_out.values())
-    e2e_steps = 0 if args.no_e2e else max(5, min(args.steps, 50))
+    e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 50 if n <= 262144 else 5))
     pb.profile_enable(False)
-    pb2 = DeviceParticleBuffer(params, n, make_options(**opts))
-    if not args.no_autotune and e2e_steps:
-        pb2.upload(pinned_in, stream=stream)
-        pb2.autotune(3, stream)
+    if gravity_only and e2e_steps:  # the same launch shape as the timed context, without re-tuning
+        pb2 = DeviceParticleBuffer(params, n, make_options(**shape_options(shape, opts)))
+    else:
+        pb2 = DeviceParticleBuffer(params, n, make_options(**opts))
+        if not args.no_autotune and e2e_steps:
+            pb2.upload(pinned_in, stream=stream)
+            pb2.autotune(3, stream)
     e2e_ms = 0.0
-    for k in range(e2e_steps + 3 if e2e_steps else 0):
+    for k in range(e2e_steps + 2 if e2e_steps else 0):
         flush.zero_()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
@@ -885,30 +988,33 @@ def main():
         pb2.download(down_names, stream=stream, out=pinned_out)
         b.record(stream)
         b.synchronize()
-        if k >= 3:
+        if k >= 2:
             e2e_ms += a.elapsed_time(b)
     pb2.close()
 
     if rank != 0:
         pb.close()
-        if dist is not None:
-            dist.destroy_process_group()
-        return
+        return None
 
     value = whole_job_rate(args.steps, world, total_ms)
     ms_per_step = total_ms / args.steps
-    nb = neighbour_pairs(st["pos"], params.H, dev) if (params.flags & 2) else 0
+    nb = 0 if gravity_only else neighbour_pairs(st["pos"], params.H, dev)
     fl = flops_per_step(params, st, nb, culled=not args.no_cull)
     timed = {k: prof[k][0] / prof[k][1] for k in fl if prof[k][1]}
     dominant = max(timed, key=lambda k: timed[k]) if timed else max(fl, key=lambda k: fl[k])
     ms_dom, cnt_dom = prof[dominant]
     achieved = fl[dominant] / (ms_dom / cnt_dom * 1e-3) / 1e12 if cnt_dom else None
     pairs_per_step = flops_pairs(params, n)
+    sym_g = int(shape.get("grav_sym_groups") or 0)
+    traffic = MEASURED_TRAFFIC.get((args.workload, dominant, "symmetric" if sym_g else "one-sided", sym_g))
+    if traffic is not None:
+        traffic = traffic[0] * n / traffic[1]  # bytes per particle of the captured case x N
 
     cpu = None
-    if not args.no_cpu_baseline:
-        rate, sdesc, cores, kind, _ = cpu_reference_sample(variant, st, args.cpu_budget)
-        cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": kind, "sample": sdesc}
+    ref_cuda = None
+    if not args.no_cpu_baseline and world == 1:
+        cpu = cpu_baseline_child(args.workload, args.n, args.cpu_budget)
+        ref_cuda = reference_cuda_child(args.workload, args.n, 50)
 
     drift = None
     if args.drift_steps < 0:
@@ -930,22 +1036,97 @@ def main():
         "kernel_ms_per_step": {k: (v[0] / v[1] if v[1] else None) for k, v in prof.items()},
         "roofline": {"bound": "fp32", "kernel": dominant, "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if (achieved and peak_tflops) else None,
-                     "traffic": MEASURED_TRAFFIC.get((args.workload, n, dominant,
-                                                      "symmetric" if shape.get("grav_sym_groups") else "one-sided")),
-                     "algorithmic_bytes": 16 * n, "flops_per_launch": fl[dominant], "neighbour_pairs": nb,
+                     "traffic": traffic, "algorithmic_bytes": 16 * n, "flops_per_launch": fl[dominant],
+                     "neighbour_pairs": nb,
                      "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
         "integrator_roofline": integrator_roofline(prof, n, params),
         "cpu_baseline": cpu,
+        "reference_cuda": ref_cuda,
         "clocks": clocks,
         "e2e": ({"value": e2e_steps / (e2e_ms * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
                  "d2h_bytes_per_step": d2h} if e2e_steps else None),
         "gpu_launches": gpu_launches,
         "energy_drift": drift,
     }
-    print(json.dumps(line))
     pb.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    return line
+
+
+def leg_args(args, **over):
+    a = argparse.Namespace(**vars(args))
+    for k, v in over.items():
+        setattr(a, k, v)
+    return a
+
+
+def run_legs(args, rank, world, local):
+    """The other workloads of the default run (one GPU): each as its own line under "workloads"."""
+    legs = args.legs
+    if legs == "none" or world > 1 or rank != 0:
+        return None
+    if legs == "auto":
+        if args.workload != "plummer" or args.n:
+            return None
+        legs = "impact,ensemble,surrogate"
+    out = {}
+    for leg in [x.strip() for x in legs.split(",") if x.strip()]:
+        t0 = time.perf_counter()
+        try:
+            if leg == "impact":
+                a = leg_args(args, workload="impact", n=0, steps=300, warmup=10, drift_steps=1000, gravity="auto",
+                             gravity_groups=0, cpu_budget=min(args.cpu_budget, 10.0))
+                line = run_context(a, rank, 1, local)
+            elif leg == "ensemble":
+                a = leg_args(args, workload="ensemble", steps=5, warmup=3, drift_steps=0,
+                             cpu_budget=min(args.cpu_budget, 10.0))
+                line = run_ensemble(a, rank, 1, local)
+            elif leg == "surrogate":
+                a = leg_args(args, workload="surrogate", warmup=1, windows=8)
+                line = run_surrogate(a, rank, 1, local)
+            else:
+                line = {"error": "unknown leg %s" % leg}
+        except Exception as e:  # a failing leg is reported, the headline line stands
+            line = {"error": "%s: %s" % (type(e).__name__, e)}
+        line["leg_wall_s"] = time.perf_counter() - t0
+        out[leg] = line
+    return out
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl in ("reference", "reference-cuda"):
+        line = (run_reference_arm if args.impl == "reference" else run_reference_cuda)(args, rank, world)
+        if line is not None:
+            print(json.dumps(line))
+        return
+
+    if args.workload == "ensemble":
+        line = run_ensemble(args, rank, world, local)
+    elif args.workload == "surrogate":
+        line = run_surrogate(args, rank, world, local)
+    elif args.workload == "mlp":
+        line = run_mlp(args, rank, world, local)
+    else:
+        import torch
+        torch.cuda.set_device(local)
+        dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        line = run_context(args, rank, world, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        if line is not None:
+            legs = run_legs(args, rank, world, local)
+            if legs:
+                line["workloads"] = legs
+    if line is not None:
+        print(json.dumps(line))
 
 
 if __name__ == "__main__":

@@ -3,6 +3,8 @@
 Oracle      -- oracle/liboracle.so, the FP64 restatement (oracle/oracle.cpp)
 RefBuild    -- oracle/_ref/libref_<variant>_<fp32|fp64>.so, GraSPH2's own job headers built for the
                host (oracle/ref_driver.cpp); one library per physics variant (oracle/ref_variants.py)
+RefCuda     -- oracle/_ref/libref_cuda_<variant>.so, GraSPH2's own CUDA path built for sm_100a
+               (oracle/ref_cuda_driver.cu), FP32; valid for N a multiple of 256
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
 """
@@ -190,3 +192,102 @@ class RefBuild:
         for _ in range(nsteps):
             self.compute_derivatives(state)
             self.integrate(state, not_first_step, variable)
+
+
+def ref_cuda_library_path(variant):
+    return os.path.join(REF_DIR, "libref_cuda_%s.so" % variant)
+
+
+def ref_cuda_available(variant="fluid"):
+    return os.path.exists(ref_cuda_library_path(variant))
+
+
+class RefCuda:
+    """GraSPH2's own CUDA computeDerivatives / integrate on the current device, one buffer of n particles
+    (the reference's layout); FP32 as the reference ships. Its tile loop is only correct for n a multiple
+    of 256 (src/particles/algorithms.h:285-301)."""
+
+    _libs = {}
+
+    def __init__(self, variant, n):
+        path = ref_cuda_library_path(variant)
+        if not os.path.exists(path):
+            raise RuntimeError("reference CUDA build missing: %s" % path)
+        if path not in RefCuda._libs:
+            L = ctypes.CDLL(path)
+            self.struct_type = type("RefCudaParticles", (ctypes.Structure,),
+                                    {"_fields_": [(nm, ctypes.POINTER(ctypes.c_float)) for nm, _ in
+                                                  OracleParticles._fields_]})
+            P = ctypes.POINTER(self.struct_type)
+            L.refcu_create.restype = ctypes.c_void_p
+            L.refcu_create.argtypes = [ctypes.c_int64]
+            L.refcu_destroy.restype = None
+            L.refcu_destroy.argtypes = [ctypes.c_void_p]
+            L.refcu_upload.argtypes = [ctypes.c_void_p, P]
+            L.refcu_download.argtypes = [ctypes.c_void_p, P]
+            L.refcu_compute_derivatives.argtypes = [ctypes.c_void_p]
+            L.refcu_integrate.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            L.refcu_current_timestep.restype = ctypes.c_double
+            L.refcu_current_timestep.argtypes = []
+            L.refcu_time_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+            L.refcu_last_error.restype = ctypes.c_char_p
+            L.refcu_set_timestep.argtypes = [ctypes.c_double, ctypes.c_double]
+            RefCuda._libs[path] = (L, self.struct_type)
+        self.lib, self.struct_type = RefCuda._libs[path]
+        self.n = int(n)
+        self.h = self.lib.refcu_create(self.n)
+        if not self.h:
+            raise RuntimeError("refcu_create: %s" % self.lib.refcu_last_error().decode())
+
+    def close(self):
+        if self.h:
+            self.lib.refcu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("%s: %s" % (what, self.lib.refcu_last_error().decode()))
+
+    def upload(self, state):
+        from grasph2_b200.state import new_state
+        full = new_state(self.n, np.float32)
+        for k, a in state.items():
+            if k in full:
+                full[k][:] = a
+        self._keep = full
+        s = pointer_struct(full, self.struct_type, ctypes.c_float)
+        self._check(self.lib.refcu_upload(self.h, ctypes.byref(s)), "refcu_upload")
+
+    def download(self):
+        from grasph2_b200.state import new_state
+        out = new_state(self.n, np.float32)
+        s = pointer_struct(out, self.struct_type, ctypes.c_float)
+        self._check(self.lib.refcu_download(self.h, ctypes.byref(s)), "refcu_download")
+        return out
+
+    def compute_derivatives(self):
+        self._check(self.lib.refcu_compute_derivatives(self.h), "computeDerivatives")
+
+    def integrate(self, not_first_step=True):
+        self._check(self.lib.refcu_integrate(self.h, int(not_first_step)), "integrate")
+
+    def current_timestep(self):
+        return self.lib.refcu_current_timestep()
+
+    def set_timestep(self, current, nxt):
+        self._check(self.lib.refcu_set_timestep(current, nxt), "set_timestep")
+
+    def time_steps(self, steps):
+        """Device milliseconds of `steps` x {computeDerivatives; integrate(true)} (CUDA events)."""
+        ms = ctypes.c_double(0.0)
+        self._check(self.lib.refcu_time_steps(self.h, int(steps), ctypes.byref(ms)), "time_steps")
+        return ms.value

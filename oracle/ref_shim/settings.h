@@ -8,7 +8,7 @@
 #define GRASPH2_SETTINGS_H
 
 #include "types.h"
-#include "particles/Particles.h"
+#include <particles/Particles.h>  /* the host or the CUDA stand-in, by include path */
 
 constexpr Dim dimension = Dim::three;
 
@@ -28,10 +28,15 @@ constexpr Dim dimension = Dim::three;
 #define SOLIDS
 #endif
 
-/* The variable-step kernels of src/integration.h:130-217 are called directly by the parity driver;
- * integrate()'s own variable-step branch launches them with <<<>>>, which a host compiler cannot
- * parse, so the fixed-step branch is always the one compiled. */
+/* Host build: the variable-step kernels of src/integration.h:130-217 are called directly by the
+ * parity driver; integrate()'s own variable-step branch launches them with <<<>>>, which a host
+ * compiler cannot parse, so the fixed-step branch is the one compiled. CUDA build: integrate()
+ * dispatches as the reference does. */
+#if defined(__CUDACC__) && REF_VARIABLE_TIMESTEP
+#define VARIABLE_TIMESTEP_LEAPFROG
+#else
 #define FIXED_TIMESTEP_LEAPFROG
+#endif
 constexpr f1_t fixed_timestep = REF_FIXED_DT;
 constexpr f1_t initial_timestep = REF_INITIAL_DT;
 constexpr f1_t min_timestep = REF_MIN_DT;

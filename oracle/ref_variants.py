@@ -53,8 +53,10 @@ VARIANTS = {
     # as the reference can express it (eps == H, AV signal coefficient 3): the CPU timing baseline
     "impact": _v("impact", ["SELF_GRAVITY", "SPH", "SOLIDS", "ARTIFICIAL_VISCOSITY", "PLASTICITY_MIESE"],
                  H=2.5 * (4.0 / 3.0 * math.pi * 1.125 / 65536) ** (1.0 / 3.0), fixed_dt=1e-4),
-    # config-2 physics: pure N-body (softening == H in the reference)
+    # pure N-body (softening == H in the reference)
     "nbody": _v("nbody", ["SELF_GRAVITY"], H=0.05),
+    # config-2 physics: the Plummer sphere's softening eps = 0.01 (== H), dt = 1e-3
+    "plummer": _v("plummer", ["SELF_GRAVITY"], H=0.01, fixed_dt=1e-3),
     # gravity with the environment terms (Clohessy-Wiltshire, constant acceleration) and the box
     "nbody_env": _v("nbody_env", ["SELF_GRAVITY", "CLOHESSY_WILTSHIRE", "CONSTANT_ACCELERATION",
                                   "SIMPLE_BOX_BOUNDARY"], H=0.05, box_min=-0.95, box_max=0.95),

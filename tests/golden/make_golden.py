@@ -39,7 +39,9 @@ def golden_input(name, n=N, seed=7):
     """Seeded input state of variant `name`, rounded to float32-representable values."""
     v = ref_variants.VARIANTS[name]
     rng = np.random.default_rng(seed)
-    if "SOLIDS" in v["switches"]:
+    if name == "plummer":
+        st = ics.plummer_sphere(n, seed=seed)
+    elif "SOLIDS" in v["switches"]:
         nb = (n * 8) // 9
         st = ics.two_sphere_impact(n_big=nb, n_small=n - nb, v_rel=0.5, y_offset=0.3, rho0=v["rho0"], seed=seed)
         S = rng.normal(size=(n, 3, 3)) * 0.05
@@ -84,10 +86,10 @@ def run(name):
     return out
 
 
-def main():
+def main(names=None):
     build_ref.build_oracle()
     build_ref.build_ref()
-    for name in ref_variants.VARIANTS:
+    for name in names or ref_variants.VARIANTS:
         out = run(name)
         path = os.path.join(HERE, "ref_%s.npz" % name)
         np.savez_compressed(path, **out)
@@ -95,4 +97,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -77,15 +77,15 @@ SLACK_LOG = []
 NORM_LOG = []  # error lines the tests add (norm-wise errors of the plain and compensated forms per config)
 
 
-def check_within(got, want, sens, tol, what, factor=COND_FACTOR):
-    """Per value: |got - want| <= tol * max|want| + factor * sensitivity. Returns the norm-wise error,
-    and records how many values needed the sensitivity term (SLACK_LOG)."""
+def check_within(got, want, sens, tol, what, factor=COND_FACTOR, extra=0.0):
+    """Per value: |got - want| <= tol * max|want| + factor * sensitivity + extra. Returns the norm-wise
+    error, and records how many values needed the sensitivity (and extra) terms (SLACK_LOG)."""
     got = np.asarray(got, np.float64)
     want = np.asarray(want, np.float64)
     sens = np.asarray(sens, np.float64)
     scale = np.abs(want).max()
     err = np.abs(got - want)
-    allowed = tol * scale + factor * sens
+    allowed = tol * scale + factor * sens + extra
     if scale == 0:
         allowed = allowed + tol
     base = tol * scale if scale > 0 else tol
