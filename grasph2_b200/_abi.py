@@ -67,7 +67,7 @@ class GsphOptions(ctypes.Structure):
         ("i_per_thread", ctypes.c_int32), ("threads", ctypes.c_int32), ("check_finite", ctypes.c_int32),
         ("no_cull", ctypes.c_int32), ("resort_interval", ctypes.c_int32), ("scalar_fp32", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("gravity_form", ctypes.c_int32), ("gravity_groups", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("wait_limit_us", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -195,6 +195,7 @@ _SIGNATURES = {
                                               ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
     "gsph_ensemble_launch_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_ensemble_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gsph_ensemble_inject_stall": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "gsph_tc_gemm_check": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "gsph_surrogate_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

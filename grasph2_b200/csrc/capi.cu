@@ -207,7 +207,12 @@ int check_status(gsph_ctx* c, cudaStream_t s) {
     int st = 0;
     GSPH_CK(c, cudaMemcpyAsync(&st, c->a.status, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
     GSPH_CK(c, cudaStreamSynchronize(s), "stream synchronize");
-    if (st & GSPH_DEV_ERR_TIMEOUT) return fail(c, GSPH_E_TIMEOUT, "a device-side wait gave up (j-tile pipeline)");
+    if (st & GSPH_DEV_ERR_TIMEOUT) {  // report once: this call's results are incomplete, the context stays usable
+        const int cleared = st & ~GSPH_DEV_ERR_TIMEOUT;
+        cudaMemcpyAsync(c->a.status, &cleared, sizeof(int), cudaMemcpyHostToDevice, s);
+        cudaStreamSynchronize(s);
+        return fail(c, GSPH_E_TIMEOUT, "a device-side wait gave up (j-tile pipeline)");
+    }
     if (st & 2) {  // a host-requested scan: report once, then clear the flag
         const int cleared = st & ~2;
         cudaMemcpyAsync(c->a.status, &cleared, sizeof(int), cudaMemcpyHostToDevice, s);

@@ -65,6 +65,8 @@ struct EnsView {
     int64_t n;
     float kick_dt;
     int tile;            // j-particles per shared-memory stage of the DENS sweep
+    int stall_sim;       // failure-path test: this simulation's SPH items wait for one DENS item more than
+                         // exist, so their waits run out (-1: none)
 };
 
 // ---- paired FP32 (PTX ISA 8.6, sm_100+): two lanes per instruction, IEEE single precision ---------
@@ -107,15 +109,18 @@ __device__ __forceinline__ void signal_done(int* ctr) {
         atomicAdd(ctr, 1);
     }
 }
-// wait until *ctr >= target (bounded by kWaitLimitNs); false, with the status word set, if it gave up
+// wait until *ctr >= target; false, with the status word set, if it gave up. The bound is status[1]
+// microseconds when set (gsph_options.wait_limit_us), else kWaitLimitNs.
 __device__ __forceinline__ bool wait_count(const int* ctr, int target, int* status, int* s_flag) {
     if (threadIdx.x == 0) {
         int ok = 1;
         if (ld_acquire(ctr) < target) {
+            const int lim_us = status[1];
+            const uint64_t limit = lim_us > 0 ? static_cast<uint64_t>(lim_us) * 1000ull : kWaitLimitNs;
             const uint64_t t0 = global_timer_ns();
             while (ld_acquire(ctr) < target) {
-                if (global_timer_ns() - t0 > kWaitLimitNs) {
-                    atomicExch(status, GSPH_DEV_ERR_TIMEOUT);
+                if (global_timer_ns() - t0 > limit) {
+                    atomicOr(status, GSPH_DEV_ERR_TIMEOUT);
                     ok = 0;
                     break;
                 }
@@ -448,7 +453,7 @@ __global__ void __launch_bounds__(kEnsThreads) k_ensemble(DevArrays a, DevParams
             if (!dens_item<GRAV, SPH, COMP>(a, p, v, pipe, grp, sm, s_box)) return;
             signal_done(v.done + sim);
         } else if (stage == ST_SPH) {
-            if (!wait_count(v.done + sim, sm.w, a.status, &s_flag)) return;
+            if (!wait_count(v.done + sim, sm.w + (sim == v.stall_sim ? 1 : 0), a.status, &s_flag)) return;
             sph_item<GRAV, PASS, SOLIDS>(a, p, v, grp, sm);
             signal_done(v.done + v.nsims + sim);
         } else {
@@ -680,6 +685,7 @@ struct gsph_ensemble {
     int4* groups = nullptr;         // device tables
     int4* sims = nullptr;
     int* counters = nullptr;        // [1 + 2 S]
+    int inject_stall = -1;          // failure-path test: stall this simulation's SPH items once
     int* nb = nullptr;
     int* nbcnt = nullptr;
     double* diag_part = nullptr;    // [G][kEnsDiagF]
@@ -764,6 +770,7 @@ EnsView view_of(const gsph_ensemble* e, const int* stages, int nstages) {
     v.n = e->a.n;
     v.kick_dt = e->dp.fixed_dt;
     v.tile = e->tile;
+    v.stall_sim = -1;
     return v;
 }
 
@@ -771,6 +778,8 @@ EnsView view_of(const gsph_ensemble* e, const int* stages, int nstages) {
 int run_stages(gsph_ensemble* e, const int* stages, int nstages, float kick_dt, cudaStream_t s) {
     EnsView v = view_of(e, stages, nstages);
     v.kick_dt = kick_dt;
+    v.stall_sim = e->inject_stall;  // one-shot failure-path test hook
+    e->inject_stall = -1;
     ENS_CK(e, cudaMemsetAsync(e->counters, 0, (1 + 2 * static_cast<size_t>(e->nsims)) * sizeof(int), s), "counter reset");
     ENS_CK(e, launch_ensemble(e->a, e->dp, v, e->opt.accum == GSPH_ACCUM_COMPENSATED, e->sm_count, e->per_sm_cap, s),
            "ensemble launch");
@@ -789,7 +798,13 @@ int ens_status(gsph_ensemble* e, cudaStream_t s) {
     int st = 0;
     ENS_CK(e, cudaMemcpyAsync(&st, e->a.status, sizeof(int), cudaMemcpyDeviceToHost, s), "status read");
     ENS_CK(e, cudaStreamSynchronize(s), "stream synchronize");
-    if (st & GSPH_DEV_ERR_TIMEOUT) return efail(e, GSPH_E_TIMEOUT, "a device-side wait gave up (ensemble queue)");
+    if (st & GSPH_DEV_ERR_TIMEOUT) {  // report once: the state is incomplete, the context stays usable
+        const int cleared = st & ~GSPH_DEV_ERR_TIMEOUT;
+        ENS_CK(e, cudaMemcpyAsync(e->a.status, &cleared, sizeof(int), cudaMemcpyHostToDevice, s), "status clear");
+        ENS_CK(e, cudaStreamSynchronize(s), "stream synchronize");
+        return efail(e, GSPH_E_TIMEOUT, "a device-side wait gave up (ensemble queue); the results of this call are "
+                                        "incomplete");
+    }
     return GSPH_OK;
 }
 
@@ -912,6 +927,10 @@ int gsph_ensemble_create(const gsph_params* p, const gsph_options* opt, int32_t 
     e->bbox = static_cast<float*>(ens_alloc(e, static_cast<size_t>(nsims) * 8 * sizeof(float), ae));
     if (ae == cudaSuccess) ae = cudaMemcpy(e->groups, groups.data(), groups.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (ae == cudaSuccess) ae = cudaMemcpy(e->sims, sims.data(), sims.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (ae == cudaSuccess) {  // status[1]: the dependency-wait bound in microseconds (0: the default)
+        const int lim = std::max(0, o.wait_limit_us);
+        ae = cudaMemcpy(a.status + 1, &lim, sizeof(int), cudaMemcpyHostToDevice);
+    }
     if (ae == cudaSuccess) ae = launch_init_padding(a, 0);
     if (ae == cudaSuccess) {
         k_ens_iota<<<static_cast<unsigned>((n_pad + 255) / 256), 256>>>(e->ext, n_pad);
@@ -1145,6 +1164,13 @@ int gsph_ensemble_autotune(gsph_ensemble* e, int32_t reps, int32_t* tile, int32_
 int gsph_ensemble_launch_count(const gsph_ensemble* e, int64_t* count) {
     if (!e || !count) return GSPH_E_INVALID;
     *count = e->launches;
+    return GSPH_OK;
+}
+
+int gsph_ensemble_inject_stall(gsph_ensemble* e, int32_t sim) {
+    if (!e) return GSPH_E_INVALID;
+    if (sim < 0 || sim >= e->nsims) return efail(e, GSPH_E_INVALID, "sim out of range");
+    e->inject_stall = sim;
     return GSPH_OK;
 }
 

@@ -93,7 +93,8 @@ def params_to_dict(p):
 
 
 def make_options(accum="plain", j_split=0, j_tile=0, i_per_thread=0, threads=0, check_finite=0, cull=True,
-                 resort_interval=0, scalar_fp32=False, precision="single", gravity="auto", gravity_groups=0):
+                 resort_interval=0, scalar_fp32=False, precision="single", gravity="auto", gravity_groups=0,
+                 wait_limit_us=0):
     o = GsphOptions()
     o.accum = {"plain": ACCUM_PLAIN, "compensated": ACCUM_COMPENSATED}[accum] if isinstance(accum, str) else accum
     o.j_split, o.j_tile, o.i_per_thread, o.threads, o.check_finite = j_split, j_tile, i_per_thread, threads, check_finite
@@ -103,6 +104,7 @@ def make_options(accum="plain", j_split=0, j_tile=0, i_per_thread=0, threads=0, 
     o.precision = {"single": 0, "double": 1}[precision] if isinstance(precision, str) else int(precision)
     o.gravity_form = {"auto": 0, "one-sided": 1, "symmetric": 2}[gravity] if isinstance(gravity, str) else int(gravity)
     o.gravity_groups = gravity_groups
+    o.wait_limit_us = wait_limit_us
     return o
 
 

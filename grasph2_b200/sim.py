@@ -323,6 +323,11 @@ class Ensemble:
     def compute_derivatives(self, stream=None):
         self._check(self.lib.gsph_ensemble_compute_derivatives(self._h, _stream_handle(stream)))
 
+    def inject_stall(self, sim):
+        """Failure-path test hook: the next compute_derivatives stalls simulation `sim`'s SPH items until
+        their device-side waits run out (gsph_ensemble_inject_stall)."""
+        self._check(self.lib.gsph_ensemble_inject_stall(self._h, int(sim)))
+
     def integrate(self, not_first_step=True, stream=None):
         self._check(self.lib.gsph_ensemble_integrate(self._h, int(bool(not_first_step)), _stream_handle(stream)))
 

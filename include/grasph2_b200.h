@@ -180,7 +180,11 @@ typedef struct gsph_options {
                                 2/3 of the FP32 work, partials of 65 x 3 floats per particle). Auto picks the
                                 symmetric form from 24 blocks of 1024 particles up. Results agree to rounding */
     int32_t gravity_groups;  /* symmetric form: particle groups G (tasks G(G+1)/2); 0 = up to 64 */
-    int32_t reserved[4];
+    int32_t wait_limit_us;   /* batched ensemble: a work item that waits for another item's result (a device-side
+                                spin on a counter) gives up after this many microseconds, sets the timeout bit
+                                and its call returns GSPH_E_TIMEOUT (0 = 2 s). Waits for a bulk copy to land
+                                keep the fixed 2 s bound */
+    int32_t reserved[3];
 } gsph_options;
 
 #define GSPH_PRECISION_SINGLE 0
@@ -484,6 +488,12 @@ int gsph_ensemble_autotune(gsph_ensemble* e, int32_t reps, int32_t* tile, int32_
 int gsph_ensemble_launch_count(const gsph_ensemble* e, int64_t* count);
 /* text of the last failure on `e` (or of the last failed gsph_ensemble_create when e is NULL) */
 const char* gsph_ensemble_last_error(const gsph_ensemble* e);
+/* Failure-path test hook (no counterpart in the reference): the next gsph_ensemble_compute_derivatives
+ * makes simulation `sim`'s SPH work items wait for one density item more than exists, so their
+ * device-side waits run out after options.wait_limit_us; that call returns GSPH_E_TIMEOUT with
+ * incomplete results, and the ensemble stays usable (upload a state and call again). One-shot; only
+ * the host sets up the failure, no GPU fault is involved. */
+int gsph_ensemble_inject_stall(gsph_ensemble* e, int32_t sim);
 
 /* ---------------------------------------------------------------------------------------------
  * measurement hooks (no reference counterpart: the reference has no kernel timers; its console

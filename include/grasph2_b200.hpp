@@ -406,7 +406,9 @@ inline HostParticleBuffer readTextFile(const std::string& filename, uint32_t mas
                     if (!std::getline(ls, tok, sep)) throw Error(GSPH_E_INVALID, "Error parsing input file at line " +
                                                                                      std::to_string(i));
                 } while (tok.find_first_not_of(" \t") == std::string::npos);
-                a[k * i + c] = std::stof(tok);
+                // as the reference's TextFile reader: the token as a double, then rounded to float
+                // (src/initialConditions/particleSources/TextFile.h:127-129)
+                a[k * i + c] = static_cast<float>(std::stod(tok));
             }
         }
     }

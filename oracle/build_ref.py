@@ -9,6 +9,10 @@ oracle/_ref/libref_<variant>_<fp32|fp64>.so
                       g++ -O3 -march=native -fopenmp against the stand-ins in oracle/ref_shim/
                       (mpUtils is not vendored with the reference and not installed). Needs the
                       reference source tree; skipped with a message when it is absent.
+oracle/_ref/libref_io.so
+                      GraSPH2's tsv snapshot writer (src/ResultStorageManager.cu) and tsv particle
+                      source (src/initialConditions/particleSources/TextFile.h), compiled in place
+                      for the host against oracle/ref_shim/ref_io.h (oracle/ref_io_driver.cpp).
 oracle/_ref/libref_cuda_<variant>.so
                       GraSPH2's own CUDA path (the tile kernels of src/particles/algorithms.h, the
                       jobs of src/computeDerivatives.h, the integrator of src/integration.h) compiled
@@ -88,6 +92,23 @@ def build_ref(force=False, march="native"):
     return outs
 
 
+def build_ref_io(force=False):
+    """GraSPH2's tsv writer and reader (src/ResultStorageManager.cu, TextFile.h) for the host."""
+    src_dir = _reference_src()
+    if src_dir is None:
+        return []
+    out = os.path.join(HERE, "_ref", "libref_io.so")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    deps = [os.path.join(HERE, "ref_io_driver.cpp"), os.path.join(HERE, "ref_shim", "ref_io.h"),
+            os.path.join(HERE, "ref_shim", "settings.h"), os.path.join(HERE, "ref_variants.py")]
+    if force or _stale(out, deps):
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-w", "-I", os.path.join(HERE, "ref_shim"),
+               "-I", src_dir, "-o", out, os.path.join(HERE, "ref_io_driver.cpp"), "-lpthread"]
+        cmd += ref_variants.compile_defines(ref_variants.VARIANTS["nbody"], False)
+        _run(cmd)
+    return [out]
+
+
 def build_ref_cuda(force=False):
     """GraSPH2's CUDA path for sm_100a, one FP32 library per physics variant (built in parallel)."""
     src_dir = _reference_src()
@@ -127,7 +148,7 @@ def main():
     a = ap.parse_args()
     print(build_oracle(a.force))
     if not a.oracle:
-        for o in build_ref(a.force) + build_ref_cuda(a.force):
+        for o in build_ref(a.force) + build_ref_io(a.force) + build_ref_cuda(a.force):
             print(o)
 
 

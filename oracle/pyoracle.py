@@ -210,6 +210,7 @@ class RefCuda:
     _libs = {}
 
     def __init__(self, variant, n):
+        self.h = None
         path = ref_cuda_library_path(variant)
         if not os.path.exists(path):
             raise RuntimeError("reference CUDA build missing: %s" % path)

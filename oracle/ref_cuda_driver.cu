@@ -23,10 +23,8 @@
 #include "settings.h"
 #include "computeDerivatives.h"
 
-namespace {
-std::string g_err;
-
-struct host_particles {  // the layout of oracle_particles (oracle/oracle.cpp)
+/* the caller's host arrays: the layout of oracle_particles (oracle/oracle.cpp) */
+struct refcu_particles {
     f1_t* pos;
     f1_t* mass;
     f1_t* vel;
@@ -39,6 +37,9 @@ struct host_particles {  // the layout of oracle_particles (oracle/oracle.cpp)
     f1_t* dstress_dt;
     f1_t* maxvsig;
 };
+
+namespace {
+std::string g_err;
 
 using Buffer = DeviceParticleBuffer<>;
 
@@ -77,7 +78,7 @@ void* refcu_create(int64_t n) {
 
 void refcu_destroy(void* h) { delete static_cast<Buffer*>(h); }
 
-int refcu_upload(void* h, const host_particles* s) {
+int refcu_upload(void* h, const refcu_particles* s) {
     Buffer* b = static_cast<Buffer*>(h);
     if (!b || !s) return -1;
     return guarded([&] {
@@ -106,7 +107,7 @@ int refcu_upload(void* h, const host_particles* s) {
     });
 }
 
-int refcu_download(void* h, host_particles* s) {
+int refcu_download(void* h, refcu_particles* s) {
     Buffer* b = static_cast<Buffer*>(h);
     if (!b || !s) return -1;
     return guarded([&] {

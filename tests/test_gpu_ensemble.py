@@ -237,3 +237,32 @@ def test_ensemble_autotune_keeps_results(oracle):
         ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st, trials=1)
         for f, tol in fields(p).items():
             check_within(got[k][f], ref[f], sens[f], tol, "autotuned sim %d %s" % (k, f))
+
+
+def test_dependency_wait_runs_out_and_the_ensemble_recovers(oracle):
+    """Failure detection without a GPU fault: the host makes one simulation's SPH items wait for a
+    density item that does not exist (gsph_ensemble_inject_stall); with a 1 ms bound the device-side
+    waits give up, set the timeout bit and return, the call reports GSPH_E_TIMEOUT, and after a fresh
+    upload the same ensemble computes correct derivatives again."""
+    import time
+    from grasph2_b200._abi import GSPH_E_TIMEOUT
+    p = VARIANTS["fluid"]()
+    sizes = [700, 1500, 300]
+    states = [sim_state(n, seed=400 + k, rho0=p.rho0) for k, n in enumerate(sizes)]
+    with Ensemble(p, sizes, make_options(wait_limit_us=1000)) as ens:
+        ens.upload(pack_states(states))
+        ens.inject_stall(1)
+        t0 = time.perf_counter()
+        with pytest.raises(GsphError) as exc:
+            ens.compute_derivatives()
+        elapsed = time.perf_counter() - t0
+        assert exc.value.code == GSPH_E_TIMEOUT
+        assert "gave up" in str(exc.value)
+        assert elapsed < 5.0, elapsed  # every wait bounded by 1 ms; launch and report overhead only
+        ens.upload(pack_states(states))  # the context stays usable
+        ens.compute_derivatives()
+        got = ens.split(ens.download())
+    for k, st in enumerate(states):
+        ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st, trials=1)
+        for f, tol in fields(p).items():
+            check_within(got[k][f], ref[f], sens[f], tol, "after timeout sim %d %s" % (k, f))
