@@ -118,6 +118,16 @@ class GsphProfile(ctypes.Structure):
     _fields_ = [("ms", ctypes.c_double * KSLOTS), ("launches", ctypes.c_int64 * KSLOTS)]
 
 
+class GsphIcOp(ctypes.Structure):
+    """gsph_ic_op"""
+    _fields_ = [("kind", ctypes.c_int32), ("attr", ctypes.c_uint32), ("seed", ctypes.c_uint64),
+                ("v", ctypes.c_double * 9)]
+
+
+IC_MOVE, IC_ROTATE, IC_POS_NOISE, IC_ANGULAR_VEL, IC_LINEAR_VEL, IC_RANDOM_VEL, IC_SET_CONSTANT = range(1, 8)
+IC_MAX_OPS = 16
+
+
 class GsphDeviceView(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("posm", ctypes.c_void_p), ("velrho", ctypes.c_void_p),
                 ("acc", ctypes.c_void_p), ("pos64", ctypes.c_void_p)]
@@ -149,6 +159,10 @@ _SIGNATURES = {
                                        ctypes.c_void_p]),
     "gsph_ic_com_correct": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_ic_com_set": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _dp, _dp,
+                                       ctypes.c_void_p, ctypes.c_void_p]),
+    "gsph_ic_modify": (ctypes.c_int, [ctypes.c_int64, ctypes.POINTER(GsphIcOp), ctypes.c_int32,
+                                      ctypes.POINTER(GsphHostParticles), _dp, _dp, ctypes.c_void_p]),
     "gsph_upload_f64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles64),
                                        ctypes.c_void_p]),
     "gsph_download_f64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles64),

@@ -1,7 +1,8 @@
-// ics.cu -- initial conditions generated on the device: uniform spheres, Plummer spheres and the
-// centre-of-mass correction (the reference's particle sources, src/initialConditions/particleSources/
-// UniformSphere.cu and PlummerSphere.cu, and InitGenerator.h:113-152), so large inputs need no host
-// generation or transfer.
+// ics.cu -- initial conditions generated on the device: uniform spheres, Plummer spheres, the
+// particle-source modifiers (move, rotate, positional noise, angular / linear / random velocity,
+// constant attributes) and the centre-of-mass correction (the reference's particle sources,
+// src/initialConditions/particleSources/UniformSphere.cu and PlummerSphere.cu, ParticleSource.h, and
+// InitGenerator.h:113-152), so large inputs need no host generation or transfer.
 //
 // Random numbers are counter-based: value k of particle i under seed s is
 //     u = (splitmix64(splitmix64(s + k) + i) >> 11) * 2^-53        (Steele, Lea & Flood 2014)
@@ -109,20 +110,96 @@ __global__ void k_com_partial(int64_t n, const float* pos, const float* vel, con
     }
 }
 
-__global__ void k_com_apply(int64_t n, float* pos, float* vel, const double* part, int nparts) {
+// shift by (target - mean): the targets are zero for gsph_ic_com_correct; a NULL target leaves that field
+struct ComTarget {
+    double com[3], vcom[3];
+    int set_com, set_vcom;
+};
+__global__ void k_com_apply(int64_t n, float* pos, float* vel, const double* part, int nparts, ComTarget t) {
     __shared__ double c[7];
     if (threadIdx.x < 7) {
-        double t = 0.0;
-        for (int b = 0; b < nparts; ++b) t += part[b * 7 + threadIdx.x];
-        c[threadIdx.x] = t;
+        double s = 0.0;
+        for (int b = 0; b < nparts; ++b) s += part[b * 7 + threadIdx.x];
+        c[threadIdx.x] = s;
     }
     __syncthreads();
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n || c[0] == 0.0) return;
     for (int k = 0; k < 3; ++k) {
-        pos[3 * i + k] = static_cast<float>(pos[3 * i + k] - c[1 + k] / c[0]);
-        if (vel) vel[3 * i + k] = static_cast<float>(vel[3 * i + k] - c[4 + k] / c[0]);
+        if (t.set_com) pos[3 * i + k] = static_cast<float>(pos[3 * i + k] + (t.com[k] - c[1 + k] / c[0]));
+        if (vel && t.set_vcom) vel[3 * i + k] = static_cast<float>(vel[3 * i + k] + (t.vcom[k] - c[4 + k] / c[0]));
     }
+}
+
+// the modifier list of a particle source, applied per particle in order (arithmetic in FP64, stored FP32)
+struct IcOps {
+    int n;
+    gsph_ic_op op[GSPH_IC_MAX_OPS];
+};
+struct IcArrays {
+    float* a[11];  // gsph_host_particles in attribute-bit order
+};
+__global__ void k_ic_modify(int64_t n, IcOps ops, IcArrays arr) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* pos = arr.a[0];
+    float* vel = arr.a[2];
+    double x[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+    if (pos)
+        for (int c = 0; c < 3; ++c) x[c] = pos[3 * i + c];
+    if (vel)
+        for (int c = 0; c < 3; ++c) v[c] = vel[3 * i + c];
+    for (int k = 0; k < ops.n; ++k) {
+        const gsph_ic_op& o = ops.op[k];
+        switch (o.kind) {
+            case GSPH_IC_MOVE:
+                for (int c = 0; c < 3; ++c) x[c] += o.v[c];
+                break;
+            case GSPH_IC_ROTATE: {  // v[0..8]: the rotation matrix, row-major (built on the host)
+                double y[3], w[3];
+                for (int r = 0; r < 3; ++r) {
+                    y[r] = o.v[3 * r] * x[0] + o.v[3 * r + 1] * x[1] + o.v[3 * r + 2] * x[2];
+                    w[r] = o.v[3 * r] * v[0] + o.v[3 * r + 1] * v[1] + o.v[3 * r + 2] * v[2];
+                }
+                for (int c = 0; c < 3; ++c) {
+                    x[c] = y[c];
+                    v[c] = w[c];
+                }
+                break;
+            }
+            case GSPH_IC_POS_NOISE:
+                for (int c = 0; c < 3; ++c) x[c] += o.v[0] * (2.0 * uniform(o.seed, c, i) - 1.0);
+                break;
+            case GSPH_IC_ANGULAR_VEL:
+                v[0] += o.v[1] * x[2] - o.v[2] * x[1];
+                v[1] += o.v[2] * x[0] - o.v[0] * x[2];
+                v[2] += o.v[0] * x[1] - o.v[1] * x[0];
+                break;
+            case GSPH_IC_LINEAR_VEL:
+                for (int c = 0; c < 3; ++c) v[c] += o.v[c];
+                break;
+            case GSPH_IC_RANDOM_VEL:
+                for (int c = 0; c < 3; ++c) v[c] += o.v[0] * (2.0 * uniform(o.seed, c, i) - 1.0);
+                break;
+            case GSPH_IC_SET_CONSTANT: {
+                const int b = __ffs(static_cast<int>(o.attr)) - 1;
+                const int kc = (b == 8 || b == 9) ? 9 : ((b == 0 || b == 2 || b == 3 || b == 5) ? 3 : 1);
+                if (b == 0)
+                    for (int c = 0; c < 3; ++c) x[c] = o.v[c];
+                else if (b == 2)
+                    for (int c = 0; c < 3; ++c) v[c] = o.v[c];
+                else
+                    for (int c = 0; c < kc; ++c) arr.a[b][kc * i + c] = static_cast<float>(o.v[c]);
+                break;
+            }
+            default:
+                break;
+        }
+    }
+    if (pos)
+        for (int c = 0; c < 3; ++c) pos[3 * i + c] = static_cast<float>(x[c]);
+    if (vel)
+        for (int c = 0; c < 3; ++c) vel[3 * i + c] = static_cast<float>(v[c]);
 }
 
 inline unsigned blocks_for(int64_t n, int t) { return static_cast<unsigned>((n + t - 1) / t); }
@@ -170,9 +247,111 @@ int gsph_ic_com_correct(int64_t n, float* pos, float* vel, const float* mass, do
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int parts = 256;
     k_com_partial<<<parts, 256, 0, s>>>(n, pos, vel, mass, scratch);
-    k_com_apply<<<blocks_for(n, 256), 256, 0, s>>>(n, pos, vel, scratch, parts);
+    k_com_apply<<<blocks_for(n, 256), 256, 0, s>>>(n, pos, vel, scratch, parts, ComTarget{{0, 0, 0}, {0, 0, 0}, 1, 1});
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GSPH_OK : ic_fail(e, "gsph_ic_com_correct");
+}
+
+int gsph_ic_com_set(int64_t n, float* pos, float* vel, const float* mass, const double* com, const double* vcom,
+                    double* scratch, void* stream) {
+    if (n < 1 || !pos || !mass || !scratch || (vcom && !vel)) {
+        set_global_error("gsph_ic_com_set: n >= 1, pos, mass and scratch are required (and vel with vcom)");
+        return GSPH_E_INVALID;
+    }
+    ComTarget t{};
+    t.set_com = com != nullptr;
+    t.set_vcom = vcom != nullptr;
+    for (int c = 0; c < 3; ++c) {
+        t.com[c] = com ? com[c] : 0.0;
+        t.vcom[c] = vcom ? vcom[c] : 0.0;
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int parts = 256;
+    k_com_partial<<<parts, 256, 0, s>>>(n, pos, vel, mass, scratch);
+    k_com_apply<<<blocks_for(n, 256), 256, 0, s>>>(n, pos, vel, scratch, parts, t);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GSPH_OK : ic_fail(e, "gsph_ic_com_set");
+}
+
+int gsph_ic_modify(int64_t n, const gsph_ic_op* ops, int32_t nops, const gsph_host_particles* dev, double* desired_com,
+                   double* desired_vcom, void* stream) {
+    if (n < 1 || !dev || nops < 0 || nops > GSPH_IC_MAX_OPS || (nops > 0 && !ops)) {
+        set_global_error("gsph_ic_modify: n >= 1, dev and 0 <= nops <= GSPH_IC_MAX_OPS ops are required");
+        return GSPH_E_INVALID;
+    }
+    IcArrays arr;
+    float* const src[11] = {dev->pos, dev->mass, dev->vel, dev->acc, dev->balsara, dev->xvel,
+                            dev->density, dev->density_dt, dev->dstress, dev->dstress_dt, dev->maxvsig};
+    for (int b = 0; b < 11; ++b) arr.a[b] = src[b];
+    IcOps list{};
+    list.n = nops;
+    double com[3] = {0, 0, 0}, vcom[3] = {0, 0, 0};
+    for (int c = 0; c < 3; ++c) {
+        com[c] = desired_com ? desired_com[c] : 0.0;
+        vcom[c] = desired_vcom ? desired_vcom[c] : 0.0;
+    }
+    for (int k = 0; k < nops; ++k) {
+        gsph_ic_op o = ops[k];
+        const bool needs_pos = o.kind == GSPH_IC_MOVE || o.kind == GSPH_IC_ROTATE || o.kind == GSPH_IC_POS_NOISE ||
+                               o.kind == GSPH_IC_ANGULAR_VEL;
+        const bool needs_vel = o.kind == GSPH_IC_ROTATE || o.kind == GSPH_IC_ANGULAR_VEL ||
+                               o.kind == GSPH_IC_LINEAR_VEL || o.kind == GSPH_IC_RANDOM_VEL;
+        if (o.kind < GSPH_IC_MOVE || o.kind > GSPH_IC_SET_CONSTANT) {
+            set_global_error("gsph_ic_modify: unknown op kind " + std::to_string(o.kind));
+            return GSPH_E_INVALID;
+        }
+        if ((needs_pos && !dev->pos) || (needs_vel && !dev->vel)) {
+            set_global_error("gsph_ic_modify: op " + std::to_string(k) + " needs the pos / vel arrays");
+            return GSPH_E_INVALID;
+        }
+        if (o.kind == GSPH_IC_SET_CONSTANT) {
+            const uint32_t a = o.attr;
+            if (a == 0 || (a & (a - 1)) || a > GSPH_MAXVSIG || !src[__builtin_ctz(a)]) {
+                set_global_error("gsph_ic_modify: setConstant needs one attribute bit whose array is given");
+                return GSPH_E_INVALID;
+            }
+        }
+        if (o.kind == GSPH_IC_ROTATE) {  // R = c I + (1 - c) a a^T + s [a]x, a the unit axis
+            const double ax = o.v[0], ay = o.v[1], az = o.v[2], ang = o.v[3];
+            const double l = std::sqrt(ax * ax + ay * ay + az * az);
+            if (!(l > 0.0)) {
+                set_global_error("gsph_ic_modify: rotate needs a nonzero axis");
+                return GSPH_E_INVALID;
+            }
+            const double u[3] = {ax / l, ay / l, az / l}, c = std::cos(ang), sn = std::sin(ang);
+            const double K[9] = {0, -u[2], u[1], u[2], 0, -u[0], -u[1], u[0], 0};
+            for (int r = 0; r < 3; ++r)
+                for (int q = 0; q < 3; ++q) o.v[3 * r + q] = (r == q ? c : 0.0) + (1.0 - c) * u[r] * u[q] + sn * K[3 * r + q];
+            double y[3], w[3];
+            for (int r = 0; r < 3; ++r) {
+                y[r] = o.v[3 * r] * com[0] + o.v[3 * r + 1] * com[1] + o.v[3 * r + 2] * com[2];
+                w[r] = o.v[3 * r] * vcom[0] + o.v[3 * r + 1] * vcom[1] + o.v[3 * r + 2] * vcom[2];
+            }
+            for (int r = 0; r < 3; ++r) {
+                com[r] = y[r];
+                vcom[r] = w[r];
+            }
+        } else if (o.kind == GSPH_IC_MOVE) {
+            for (int c = 0; c < 3; ++c) com[c] += o.v[c];
+        } else if (o.kind == GSPH_IC_ANGULAR_VEL) {
+            vcom[0] += o.v[1] * com[2] - o.v[2] * com[1];
+            vcom[1] += o.v[2] * com[0] - o.v[0] * com[2];
+            vcom[2] += o.v[0] * com[1] - o.v[1] * com[0];
+        } else if (o.kind == GSPH_IC_LINEAR_VEL) {
+            for (int c = 0; c < 3; ++c) vcom[c] += o.v[c];
+        }
+        list.op[k] = o;
+    }
+    if (nops > 0) {
+        k_ic_modify<<<blocks_for(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(n, list, arr);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return ic_fail(e, "gsph_ic_modify");
+    }
+    for (int c = 0; c < 3; ++c) {
+        if (desired_com) desired_com[c] = com[c];
+        if (desired_vcom) desired_vcom[c] = vcom[c];
+    }
+    return GSPH_OK;
 }
 
 }  // extern "C"

@@ -149,3 +149,117 @@ def plummer_sphere_device(n, a=1.0, total_mass=1.0, G=1.0, seed=0, com_correct=T
     if com_correct:
         _com(lib, n, st)
     return st
+
+
+# ---- particle-source modifiers on the device (gsph_ic_modify; ParticleSource.h:65-74) ---------------
+def op_move(dx):
+    """pos += dx (ParticleSource::move)"""
+    return ("move", tuple(float(x) for x in dx), 0)
+
+
+def op_rotate(axis, angle):
+    """pos = R pos, vel = R vel about `axis` by `angle` radians (ParticleSource::rotate)"""
+    return ("rotate", tuple(float(x) for x in axis) + (float(angle),), 0)
+
+
+def op_positional_noise(strength, seed):
+    """pos += uniform in [-strength, strength) per component (ParticleSource::addPositionalNoise)"""
+    return ("pos_noise", (float(strength),), int(seed))
+
+
+def op_angular_velocity(omega):
+    """vel += omega x pos (ParticleSource::addAngularVelocity)"""
+    return ("angular_vel", tuple(float(x) for x in omega), 0)
+
+
+def op_linear_velocity(v):
+    """vel += v (ParticleSource::addLinearVelocity)"""
+    return ("linear_vel", tuple(float(x) for x in v), 0)
+
+
+def op_random_velocity(strength, seed):
+    """vel += uniform in [-strength, strength) per component (ParticleSource::addRandomVelocity)"""
+    return ("random_vel", (float(strength),), int(seed))
+
+
+def op_set_constant(attribute, value):
+    """attribute (a state name, e.g. "density") = value for every particle (ParticleSource::setConstant)"""
+    return ("set_constant:" + attribute, tuple(float(x) for x in np.atleast_1d(value)), 0)
+
+
+_OP_KIND = {"move": 1, "rotate": 2, "pos_noise": 3, "angular_vel": 4, "linear_vel": 5, "random_vel": 6,
+            "set_constant": 7}
+
+
+def modify_device(st, ops, desired_com=(0.0, 0.0, 0.0), desired_vel_of_com=(0.0, 0.0, 0.0)):
+    """Apply the modifiers `ops` (op_* tuples, in order) to the device state `st` (torch CUDA tensors in the
+    host layout) on the GPU. Returns the desired centre of mass and its velocity after the ops (the
+    reference's m_desiredCOM / m_desiredVelOfCOM), the targets of com_set_device."""
+    import ctypes
+    from ._abi import ATTR_BITS, GsphHostParticles, GsphIcOp, load_library
+    lib = load_library()
+    arr = (GsphIcOp * max(1, len(ops)))()
+    for k, (kind, v, seed) in enumerate(ops):
+        name, _, attr = kind.partition(":")
+        arr[k].kind = _OP_KIND[name]
+        arr[k].attr = ATTR_BITS[attr] if attr else 0
+        arr[k].seed = seed
+        for j, x in enumerate(v):
+            arr[k].v[j] = x
+    view = GsphHostParticles()
+    for name, t in st.items():
+        setattr(view, name, ctypes.cast(ctypes.c_void_p(t.data_ptr()), ctypes.POINTER(ctypes.c_float)))
+    com = (ctypes.c_double * 3)(*desired_com)
+    vcom = (ctypes.c_double * 3)(*desired_vel_of_com)
+    rc = lib.gsph_ic_modify(st["mass"].shape[0] if "mass" in st else st["pos"].shape[0], arr, len(ops),
+                            ctypes.byref(view), com, vcom, None)
+    if rc != 0:
+        raise RuntimeError(lib.gsph_last_error(None).decode())
+    return tuple(com), tuple(vcom)
+
+
+def com_set_device(st, com=None, vel_of_com=None):
+    """Shift the device state's mass-weighted mean position / velocity to com / vel_of_com (None: leave)
+    (the per-source correction of InitGenerator.h:113-152)."""
+    import ctypes
+    import torch
+    from ._abi import load_library
+    lib = load_library()
+    scratch = torch.empty(7 * 256, dtype=torch.float64, device="cuda")
+    c = (ctypes.c_double * 3)(*com) if com is not None else None
+    v = (ctypes.c_double * 3)(*vel_of_com) if vel_of_com is not None else None
+    rc = lib.gsph_ic_com_set(st["mass"].shape[0], ctypes.c_void_p(st["pos"].data_ptr()),
+                             ctypes.c_void_p(st["vel"].data_ptr()), ctypes.c_void_p(st["mass"].data_ptr()), c, v,
+                             ctypes.c_void_p(scratch.data_ptr()), None)
+    if rc != 0:
+        raise RuntimeError(lib.gsph_last_error(None).decode())
+
+
+def two_sphere_impact_device(n_big=58254, n_small=7282, r_big=1.0, r_small=0.5, v_rel=0.5, y_offset=0.3, rho0=1.0,
+                             seed=0):
+    """The two-sphere impact assembled on the GPU as the reference's initial-condition generator would: two
+    uniform sphere sources of equal number density, the small one moved to touch the big one's surface at
+    y-offset `y_offset` and given velocity v_rel along x, each source's centre of mass and its velocity
+    corrected to the desired values its modifiers imply (InitGenerator.h:113-152)."""
+    import torch
+    n = n_big + n_small
+    vol_big = 4.0 / 3.0 * math.pi * r_big ** 3
+    m = rho0 * vol_big / n_big
+    st = {"pos": _dev(n, 3), "vel": _dev(n, 3), "mass": _dev(n), "density": _dev(n)}
+    parts = []
+    for (nk, rk, sk) in ((n_big, r_big, seed), (n_small, r_small, seed + 1)):
+        part = uniform_sphere_device(nk, radius=rk, total_mass=m * nk, rho0=rho0, seed=sk, com_correct=False)
+        parts.append(part)
+    dx = -math.sqrt(max(0.0, (r_big + r_small) ** 2 - y_offset ** 2))
+    for part, ops in ((parts[0], []),
+                      (parts[1], [op_move((dx, y_offset, 0.0)), op_linear_velocity((v_rel, 0.0, 0.0))])):
+        com, vcom = modify_device(part, ops)
+        com_set_device(part, com, vcom)
+    off = 0
+    for part in parts:
+        k = part["mass"].shape[0]
+        for key in st:
+            st[key][off:off + k] = part[key]
+        off += k
+    torch.cuda.synchronize()
+    return st

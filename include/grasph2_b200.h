@@ -434,6 +434,38 @@ int gsph_ic_plummer(int64_t n, double a, double total_mass, double G, uint64_t s
                     float* mass, void* stream);
 /* subtract the mass-weighted mean position and velocity (vel may be NULL); scratch: 7 * 256 device doubles */
 int gsph_ic_com_correct(int64_t n, float* pos, float* vel, const float* mass, double* scratch, void* stream);
+/* shift positions and/or velocities so that their mass-weighted means become com[3] / vcom[3] (either may
+ * be NULL: left as is): the per-source correction of InitGenerator.h:113-152, whose targets are the
+ * desired centre of mass and its velocity that gsph_ic_modify tracks; scratch: 7 * 256 device doubles */
+int gsph_ic_com_set(int64_t n, float* pos, float* vel, const float* mass, const double* com, const double* vcom,
+                    double* scratch, void* stream);
+
+/* Modifiers of a particle source (ParticleSource, src/initialConditions/ParticleSource.h:65-74 and
+ * :93-203), applied on the device to every particle in list order, as the reference applies its
+ * m_operations to each generated particle. */
+#define GSPH_IC_MOVE         1  /* pos += v[0..2]                                          (move)               */
+#define GSPH_IC_ROTATE       2  /* pos = R pos, vel = R vel; axis v[0..2], angle v[3] (rad)  (rotate)             */
+#define GSPH_IC_POS_NOISE    3  /* pos += three draws uniform in [-v[0], v[0]) from `seed`   (addPositionalNoise) */
+#define GSPH_IC_ANGULAR_VEL  4  /* vel += omega x pos, omega = v[0..2]                       (addAngularVelocity) */
+#define GSPH_IC_LINEAR_VEL   5  /* vel += v[0..2]                                            (addLinearVelocity)  */
+#define GSPH_IC_RANDOM_VEL   6  /* vel += three draws uniform in [-v[0], v[0]) from `seed`   (addRandomVelocity)  */
+#define GSPH_IC_SET_CONSTANT 7  /* attribute `attr` (one GSPH_* bit) = v[0..k-1], k its components (setConstant) */
+typedef struct gsph_ic_op {
+    int32_t kind;   /* GSPH_IC_* */
+    uint32_t attr;  /* GSPH_IC_SET_CONSTANT: the attribute bit */
+    uint64_t seed;  /* the random modifiers: draw j of particle i is splitmix64-based, (seed, j, i) */
+    double v[9];
+} gsph_ic_op;
+#define GSPH_IC_MAX_OPS 16
+/* Apply ops[0..nops-1] (nops <= GSPH_IC_MAX_OPS) to the n particles of `dev` (device arrays in the host
+ * layout; an op whose attribute array is NULL fails with GSPH_E_INVALID). desired_com / desired_vcom
+ * (host double[3], in/out, may be NULL) are transformed as the reference's m_desiredCOM /
+ * m_desiredVelOfCOM: move adds to the COM, rotate rotates both, the velocity modifiers add their
+ * (deterministic) part to the COM velocity. The random modifiers draw the reference's distribution
+ * (uniform in [-s, s) per component) from counter-based draws instead of std::default_random_engine's
+ * sequence, so values are reproducible for any launch shape but not bit-equal to the reference's. */
+int gsph_ic_modify(int64_t n, const gsph_ic_op* ops, int32_t nops, const gsph_host_particles* dev,
+                   double* desired_com, double* desired_vcom, void* stream);
 /* gsph_upload from device arrays in the host layout (e.g. the generators above) */
 int gsph_upload_device(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_particles* src, void* stream);
 

