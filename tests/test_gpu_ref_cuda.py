@@ -190,7 +190,7 @@ def test_product_matches_reference_cuda_impact_n65536(oracle):
             r = ref[k][i0:i1]
             e_got = check_within(got[k][i0:i1], r, sens[k][i0:i1], tol, "impact[%d:%d] %s vs FP64" % (i0, i1, k))
             ref_dev = np.abs(want[k][i0:i1] - r)
-            e_ref = float(ref_dev.max() / np.abs(r).max())
+            e_ref = float(ref_dev.max() / np.abs(r).max()) if np.abs(r).max() > 0 else float(ref_dev.max())
             check_within(got[k][i0:i1], want[k][i0:i1], sens[k][i0:i1], tol,
                          "vs reference CUDA impact[%d:%d] %s" % (i0, i1, k), extra=ref_dev)
             errs.append("%s[%d:%d] ours %.2e, reference CUDA %.2e" % (k, i0, i1, e_got, e_ref))
