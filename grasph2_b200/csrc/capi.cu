@@ -503,6 +503,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
     c->gpart_cap = L.cull ? gravity_partial_floats(L, n_pad) : 4;
     a.part = static_cast<float*>(dalloc(c, c->part_cap * sizeof(float), ae));
     a.gpart = static_cast<float*>(dalloc(c, c->gpart_cap * sizeof(float), ae));
+    a.gfold = static_cast<double*>(dalloc(c, (L.cull ? 3 * n_pad : 4) * sizeof(double), ae));
     if (L.cull) {
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;

@@ -61,6 +61,7 @@ struct DevArrays {
                       // per neighbour for the culled SPH passes' gathers), rebuilt with jA / jB
     float* part;      // j-split partial sums [segment][component][n_pad]
     float* gpart;     // gravity partial sums of the culled path [segment][component][n_pad]
+    double* gfold;    // [3][n_pad]: FP64 sums of those partials (k_gravity_fold), read by the SPH finish
     float* dt_state;  // variable step: [0] current, [1] next (float bit patterns, positive)
     float4* grav;     // gravitational acceleration of the last derivative evaluation (nullable)
     double* diag;     // diagnostics scratch

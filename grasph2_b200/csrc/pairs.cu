@@ -481,60 +481,55 @@ __device__ __forceinline__ float seg_sum(const PartView& v, int64_t i, int f) {
     return s;
 }
 
-// gravity partials of an all-pairs gravity kernel (component c of particle i), summed like seg_sum:
-// the one-sided kernel's segments 0 .. nseg-1, or the symmetric kernel's row slots g .. G-1 and then
-// column slots G .. G + g of the particle's group g
-__device__ __forceinline__ void gpart_slots(const GravSum& gs, int64_t, int& r0, int& r1, int& c0, int& c1) {
-    r0 = 0; r1 = gs.nseg; c0 = c1 = 0;
-}
-// slots k0 .. k1-1 of all three components at once, unrolled so that several slots' loads are in
-// flight (each component is still summed in slot order)
-template <typename T, bool COMP>
-__device__ __forceinline__ void gpart_range(const float* part, int64_t n_pad, int k0, int k1, int64_t i, T (&s)[3]) {
-    constexpr int K = COMP ? 6 : 3;
-#pragma unroll 4
-    for (int k = k0; k < k1; ++k) {
-        const float* q = part + static_cast<int64_t>(k) * K * n_pad + i;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            if (COMP) s[c] += static_cast<T>(q[c * n_pad]) + static_cast<T>(q[(3 + c) * n_pad]);
-            else s[c] += static_cast<T>(q[c * n_pad]);
-        }
-    }
-}
-// the three components of particle i: FP64 sums of (sum + error) when compensated
+// ---- the FP64 fold of the gravity partials ---------------------------------------------------------
+// Both all-pairs gravity kernels leave per-particle partial sums [slot][component][n_pad]: the one-sided
+// kernel's j-segments, or the symmetric kernel's G + 1 slots (its row and column sums, each written by
+// one task). kFoldT threads fold one particle: thread q sums the slots [q R, (q + 1) R) in FP64 (with the
+// error terms of the compensated form), then the runs are added in the order q = 0, 1, 2, 3 -- a fixed
+// order, so results are deterministic. Eight particles per warp: for a slot, the eight lanes of a run
+// read 32 contiguous bytes.
+constexpr int kFoldT = 4;
 template <bool COMP>
-__device__ __forceinline__ void gpart_sum(const float* part, int64_t n_pad, const GravSum& gs, int64_t i, double (&out)[3]) {
-    if (gs.sym_G > 0) {  // the symmetric kernel's G + 1 slots of particle i, contiguous, in slot order
-        constexpr int K = COMP ? 6 : 3;
-        const int S = gs.sym_G + 1;
-        const float* q = part + static_cast<int64_t>(i) * S * K;
-        if (COMP) {
-            double s[3] = {0.0, 0.0, 0.0};
-            for (int k = 0; k < S; ++k, q += K)
-                for (int c = 0; c < 3; ++c) s[c] += static_cast<double>(q[c]) + static_cast<double>(q[3 + c]);
-            for (int c = 0; c < 3; ++c) out[c] = s[c];
-        } else {  // FP64: the slot sums can be large and cancel (a particle near the centre of mass)
-            double s[3] = {0.0, 0.0, 0.0};
-            for (int k = 0; k < S; ++k, q += K)
-                for (int c = 0; c < 3; ++c) s[c] += static_cast<double>(q[c]);
-            for (int c = 0; c < 3; ++c) out[c] = s[c];
+__device__ __forceinline__ void fold_slots(const float* __restrict__ part, int64_t n_pad, int S, int64_t i, bool valid,
+                                           double (&out)[3]) {
+    constexpr int K = COMP ? 6 : 3;
+    const int lane = threadIdx.x & 31, q = lane >> 3;
+    const int R = (S + kFoldT - 1) / kFoldT;
+    const int k0 = min(S, q * R), k1 = min(S, k0 + R);
+    double s[3] = {0.0, 0.0, 0.0};
+    if (valid) {
+#pragma unroll 4
+        for (int k = k0; k < k1; ++k) {
+            const float* p = part + static_cast<int64_t>(k) * K * n_pad + i;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                s[c] += static_cast<double>(__ldg(p + c * n_pad));
+                if (COMP) s[c] += static_cast<double>(__ldg(p + (3 + c) * n_pad));
+            }
         }
-        return;
     }
-    int r0, r1, c0, c1;
-    gpart_slots(gs, i, r0, r1, c0, c1);
-    if (COMP) {
-        double s[3] = {0.0, 0.0, 0.0};
-        gpart_range<double, true>(part, n_pad, r0, r1, i, s);
-        gpart_range<double, true>(part, n_pad, c0, c1, i, s);
-        for (int c = 0; c < 3; ++c) out[c] = s[c];
-    } else {
-        float s[3] = {0.0f, 0.0f, 0.0f};
-        gpart_range<float, false>(part, n_pad, r0, r1, i, s);
-        gpart_range<float, false>(part, n_pad, c0, c1, i, s);
-        for (int c = 0; c < 3; ++c) out[c] = s[c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {  // runs 0 + 1 + 2 + 3, in this order, on the lanes of run 0
+        double t = s[c];
+        t += __shfl_down_sync(0xffffffffu, s[c], 8);
+        t += __shfl_down_sync(0xffffffffu, s[c], 16);
+        t += __shfl_down_sync(0xffffffffu, s[c], 24);
+        out[c] = t;
     }
+}
+__device__ __forceinline__ int64_t fold_particle() {
+    return (static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u)) / kFoldT + (threadIdx.x & 7);
+}
+
+// the culled path: the fold of the gravity partials into gfold[3][n_pad], on the gravity kernel's stream
+template <bool COMP>
+__global__ void __launch_bounds__(256) k_gravity_fold(const float* __restrict__ part, int64_t n, int64_t n_pad, int S,
+                                                      double* __restrict__ gfold) {
+    const int64_t i = fold_particle();
+    double t[3];
+    fold_slots<COMP>(part, n_pad, S, i, i < n, t);
+    if ((threadIdx.x & 31) < 8 && i < n)
+        for (int c = 0; c < 3; ++c) gfold[c * n_pad + i] = t[c];
 }
 
 template <int PASS, bool GRAV, bool SOLIDS, bool COMP>
@@ -552,10 +547,8 @@ __global__ void k_pairs_finish(DevArrays a, DevParams p, PartView pv, GravSum gs
             g[1] = seg_sum<MASK, COMP>(pv, i, F_GY);
             g[2] = seg_sum<MASK, COMP>(pv, i, F_GZ);
             grav = true;
-        } else if (gsum.nseg > 0 || gsum.sym_G > 0) {
-            double t[3];
-            gpart_sum<COMP>(a.gpart, a.n_pad, gsum, i, t);
-            for (int c = 0; c < 3; ++c) g[c] = static_cast<float>(t[c]);
+        } else if (gsum.nseg > 0 || gsum.sym_G > 0) {  // folded on the gravity stream (k_gravity_fold)
+            for (int c = 0; c < 3; ++c) g[c] = static_cast<float>(a.gfold[c * a.n_pad + i]);
             grav = true;
         }
     }
@@ -763,17 +756,15 @@ __global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* _
     const int ra0 = ga * gs, ra1 = min(nb, ra0 + gs);
     const int cg0 = gb * gs, cg1 = min(nb, cg0 + gs);
     const bool diag = ga == gb;
-    // partials per particle: G + 1 slots of K floats, a particle of group g holding its row sums from
-    // tasks (g, gb), gb = g .. G-1, in slots 0 .. G-1-g and its column sums from tasks (ga, g), ga = 0 .. g,
-    // in slots G-g .. G (so the finish reads one contiguous run per particle, in a fixed order)
-    const int64_t S = G + 1;
+    // partials: G + 1 slots per particle, stored [slot][component][n_pad] so that a warp's 32 consecutive
+    // particles write (and the fold kernel reads) 128 contiguous bytes; a particle of group g holds its row
+    // sums from tasks (g, gb), gb = g .. G-1, in slots 0 .. G-1-g and its column sums from tasks (ga, g),
+    // ga = 0 .. g, in slots G-g .. G, each slot written by exactly one task
     const int s_row = gb - ga, s_col = G - gb + ga;
-    auto slot = [&](int64_t particle, int sl) { return part + (particle * S + sl) * K; };
+    auto slot = [&](int64_t particle, int sl, int c) { return part + (static_cast<int64_t>(sl) * K + c) * n_pad + particle; };
     if (diag)  // the group's first block is never a column here: its column slot is zero
-        for (int e = tid; e < kSymB; e += kSymT) {
-            float* q = slot(static_cast<int64_t>(ra0) * kSymB + e, s_col);
-            for (int c = 0; c < K; ++c) q[c] = 0.0f;
-        }
+        for (int e = tid; e < kSymB; e += kSymT)
+            for (int c = 0; c < K; ++c) *slot(static_cast<int64_t>(ra0) * kSymB + e, s_col, c) = 0.0f;
     const float2 E2 = make_float2(eps2, eps2);
 
     for (int a = ra0; a < ra1; ++a) {
@@ -891,9 +882,9 @@ __global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* _
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const float v = (js[0][j][c] + js[1][j][c]) + (js[2][j][c] + js[3][j][c]);
-                        float* dst = slot(jb + j, s_col) + c;
+                        float* dst = slot(jb + j, s_col, c);
                         if (COMP) {
-                            float* cdst = dst + 3;
+                            float* cdst = slot(jb + j, s_col, 3 + c);
                             if (first) {
                                 *dst = v;
                                 *cdst = 0.0f;
@@ -915,14 +906,14 @@ __global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* _
         for (int m = 0; m < P; ++m) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                float* out = slot(base + static_cast<int64_t>(2 * m + h) * kSymT, s_row);
-                out[0] = h ? rsh[m][tid].y : rsh[m][tid].x;
-                out[1] = h ? rsh[P + m][tid].y : rsh[P + m][tid].x;
-                out[2] = h ? rsh[2 * P + m][tid].y : rsh[2 * P + m][tid].x;
+                const int64_t pr = base + static_cast<int64_t>(2 * m + h) * kSymT;
+                *slot(pr, s_row, 0) = h ? rsh[m][tid].y : rsh[m][tid].x;
+                *slot(pr, s_row, 1) = h ? rsh[P + m][tid].y : rsh[P + m][tid].x;
+                *slot(pr, s_row, 2) = h ? rsh[2 * P + m][tid].y : rsh[2 * P + m][tid].x;
                 if (COMP) {
-                    out[3] = h ? csh[m][tid].y : csh[m][tid].x;
-                    out[4] = h ? csh[P + m][tid].y : csh[P + m][tid].x;
-                    out[5] = h ? csh[2 * P + m][tid].y : csh[2 * P + m][tid].x;
+                    *slot(pr, s_row, 3) = h ? csh[m][tid].y : csh[m][tid].x;
+                    *slot(pr, s_row, 4) = h ? csh[P + m][tid].y : csh[P + m][tid].x;
+                    *slot(pr, s_row, 5) = h ? csh[2 * P + m][tid].y : csh[2 * P + m][tid].x;
                 }
             }
         }
@@ -1004,12 +995,12 @@ __global__ void __launch_bounds__(128) k_gravity(const float4* __restrict__ posm
 }
 
 template <bool COMP>
-__global__ void k_gravity_finish(DevArrays a, DevParams p, GravSum gsum) {
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (has(p, GSPH_VARIABLE_TIMESTEP) && i == 0) a.dt_state[1] = p.max_dt;
-    if (i >= a.n) return;
+__global__ void __launch_bounds__(256) k_gravity_finish(DevArrays a, DevParams p, GravSum gsum) {
+    const int64_t i = fold_particle();
+    if (has(p, GSPH_VARIABLE_TIMESTEP) && blockIdx.x == 0 && threadIdx.x == 0) a.dt_state[1] = p.max_dt;
     double t[3];
-    gpart_sum<COMP>(a.part, a.n_pad, gsum, i, t);
+    fold_slots<COMP>(a.part, a.n_pad, gsum.sym_G > 0 ? gsum.sym_G + 1 : gsum.nseg, i, i < a.n, t);
+    if ((threadIdx.x & 31) >= 8 || i >= a.n) return;
     float acc[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -1275,8 +1266,13 @@ cudaError_t gravity_t(const DevArrays& a, const DevParams& p, const Launch& L, c
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
-    if (!finish) return cudaSuccess;
-    k_gravity_finish<COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, grav_sum(L, L.grav_nseg));
+    const int S = L.grav_sym_G > 0 ? L.grav_sym_G + 1 : L.grav_nseg;
+    const unsigned fold_blocks = blocks_for(a.n * kFoldT, 256);  // kFoldT threads per particle
+    if (!finish) {  // the culled path: fold on this (the gravity) stream, the SPH finish reads a.gfold
+        k_gravity_fold<COMP><<<fold_blocks, 256, 0, s>>>(a.gpart, a.n, a.n_pad, S, a.gfold);
+        return cudaGetLastError();
+    }
+    k_gravity_finish<COMP><<<fold_blocks, 256, 0, s>>>(a, p, grav_sum(L, L.grav_nseg));
     return cudaGetLastError();
 }
 template <int GRAV, bool COMP>

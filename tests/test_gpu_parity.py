@@ -311,9 +311,9 @@ def test_profile_and_launch_count():
         pb.step(1)
         pb.profile_collect()
         pr = pb.profile_read()
-        # gravity (side stream), chunk bounds + lists + work items, density + finish, SPH pass + finish,
-        # leapfrog
-        assert pb.launch_count() - c0 == 9
+        # gravity + the FP64 fold of its partials (side stream), chunk bounds + lists + work items,
+        # density + finish, SPH pass + finish, leapfrog
+        assert pb.launch_count() - c0 == 10
         assert pr["pairs"][1] == 1 and pr["pairs"][0] > 0 and pr["density"][1] == 1 and pr["gravity"][1] == 1
         assert pr["step"][0] >= pr["pairs"][0] + pr["gravity"][0]
 
