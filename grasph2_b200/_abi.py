@@ -218,6 +218,11 @@ _SIGNATURES = {
                                             ctypes.c_int32, ctypes.c_void_p]),
     "gsph_snapshot": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     "gsph_state_compare": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _dp, ctypes.c_void_p]),
+    "gsph_h5_available": (ctypes.c_int, []),
+    "gsph_h5_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.POINTER(GsphHostParticles),
+                                     ctypes.c_uint32]),
+    "gsph_h5_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.POINTER(GsphHostParticles),
+                                    ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "gsph_writer_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32,
                                           ctypes.POINTER(ctypes.c_void_p)]),
     "gsph_writer_write": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]),

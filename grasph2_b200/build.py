@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libgrasph2_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["capi.cu", "pairs.cu", "integrate.cu", "spatial.cu", "noalloc.cu", "fp64.cu", "ensemble.cu", "mlp.cu", "surrogate.cu", "surrogate_run.cu", "ics.cu", "writer.cu"]
+SOURCES = ["capi.cu", "pairs.cu", "integrate.cu", "spatial.cu", "noalloc.cu", "fp64.cu", "ensemble.cu", "mlp.cu", "surrogate.cu", "surrogate_run.cu", "ics.cu", "writer.cu", "h5io.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
                      "--expt-relaxed-constexpr", "-I", INCLUDE]

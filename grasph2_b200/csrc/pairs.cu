@@ -33,6 +33,7 @@ struct PartView {
     int nseg;
     const int* item_start;  // non-null: item layout
     int KK;
+    bool err;               // compensation terms stored after the K sums (all-pairs segments, compensated)
     __device__ __forceinline__ void range(int64_t i, int& b, int& e) const {
         if (item_start) {
             const int64_t g = i / kGroup;
@@ -473,7 +474,10 @@ __device__ __forceinline__ float seg_sum(const PartView& v, int64_t i, int f) {
     }
     if (COMP) {
         double s = 0.0;
-        for (int k = b; k < e; ++k) s += static_cast<double>(v.at(k, o, i)) + static_cast<double>(v.at(k, K + o, i));
+        for (int k = b; k < e; ++k) {
+            s += static_cast<double>(v.at(k, o, i));
+            if (v.err) s += static_cast<double>(v.at(k, K + o, i));
+        }
         return static_cast<float>(s);
     }
     float s = 0.0f;
@@ -1047,9 +1051,11 @@ CullView cull_view(const DevArrays& a, const SpatialArrays& sp) {
     cv.nbover = nullptr;
     return cv;
 }
-PartView seg_view(const DevArrays& a, int nseg, int KK) { return PartView{a.part, a.n_pad, nseg, nullptr, KK}; }
-PartView item_view(const DevArrays& a, const SpatialArrays& sp, int KK) {
-    return PartView{sp.item_part, a.n_pad, 0, sp.item_start, KK};
+PartView seg_view(const DevArrays& a, int nseg, int KK, bool err) {
+    return PartView{a.part, a.n_pad, nseg, nullptr, KK, err};
+}
+PartView item_view(const DevArrays& a, const SpatialArrays& sp, int KK, bool err) {
+    return PartView{sp.item_part, a.n_pad, 0, sp.item_start, KK, err};
 }
 
 // One block: chunks per item ic = ceil(total near chunks / target) so that items carry equal work,
@@ -1140,7 +1146,7 @@ cudaError_t launch_density(const DevArrays& a, const DevParams& p, const Launch&
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
     const int KK = comp ? 2 : 1;
-    const PartView pv = sp ? item_view(a, *sp, KK) : seg_view(a, L.nseg, KK);
+    const PartView pv = sp ? item_view(a, *sp, KK, comp) : seg_view(a, L.nseg, KK, comp);
     if (comp) k_density_finish<true><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, pv);
     else k_density_finish<false><<<blocks_for(a.n, 256), 256, 0, s>>>(a, p, pv);
     return cudaGetLastError();
@@ -1162,7 +1168,7 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
         // position stages, then per warp the [kNbCap][32] neighbour-index lists
         const size_t smem = pipe_smem_bytes(1, kStageChunks * kChunk) + (kGroup / 32) * kNbCap * 32 * sizeof(int);
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_pairs_items<PASS, SOLIDS, COMP>,
+            cudaError_t e = cudaFuncSetAttribute(k_pairs_items<PASS, SOLIDS, false>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
             if (e != cudaSuccess) return e;
         }
@@ -1173,7 +1179,10 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
             cv.nbcnt = sp->item_nbcnt;
             cv.nbover = sp->item_nbover;
         }
-        k_pairs_items<PASS, SOLIDS, COMP><<<L.item_grid, kGroup, smem, s>>>(a, p, cv);
+        // one work item is one tile of its particles' neighbour sums (a few to tens of terms): its
+        // partials carry no compensation term, and the compensated form folds the items in FP64 in the
+        // finish, so both forms run the plain kernel
+        k_pairs_items<PASS, SOLIDS, false><<<L.item_grid, kGroup, smem, s>>>(a, p, cv);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         GSPH_TIMER_MARK(t, stop);
@@ -1182,7 +1191,7 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
             if (e != cudaSuccess) return e;
         }
         k_pairs_finish<PASS, false, SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(
-            a, p, item_view(a, *sp, COMP ? 2 * K : K), grav_sum(L, PASS == PASS_VGRAD ? 0 : gnseg));
+            a, p, item_view(a, *sp, K, false), grav_sum(L, PASS == PASS_VGRAD ? 0 : gnseg));
         return cudaGetLastError();
     }
     constexpr uint32_t MASK = field_mask<PASS, (GRAV != 0), SOLIDS>();
@@ -1200,7 +1209,7 @@ cudaError_t pairs_t(const DevArrays& a, const DevParams& p, const Launch& L, cud
     if (e != cudaSuccess) return e;
     GSPH_TIMER_MARK(t, stop);
     k_pairs_finish<PASS, (GRAV != 0), SOLIDS, COMP><<<blocks_for(a.n, 256), 256, 0, s>>>(
-        a, p, seg_view(a, L.nseg, COMP ? 2 * K : K), GravSum{});
+        a, p, seg_view(a, L.nseg, COMP ? 2 * K : K, COMP), GravSum{});
     return cudaGetLastError();
 }
 

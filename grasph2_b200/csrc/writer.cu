@@ -85,11 +85,17 @@ void worker_loop(gsph_writer* w) {
         } else {
             gsph_host_particles v{s.host[0], s.host[1], s.host[2], s.host[3], s.host[4], s.host[5],
                                   s.host[6], s.host[7], s.host[8], s.host[9], s.host[10]};
-            try {
-                printTextFile(v, static_cast<size_t>(w->n), s.file, w->mask);
-            } catch (const std::exception& ex) {
-                code = GSPH_E_INVALID;
-                msg = ex.what();
+            const bool h5 = s.file.size() > 3 && s.file.compare(s.file.size() - 3, 3, ".h5") == 0;
+            if (h5) {  // the reference's STORE_HDF5 output (ResultStorageManager.cu:191-227)
+                code = gsph_h5_write(s.file.c_str(), w->n, &v, w->mask);
+                if (code != GSPH_OK) msg = gsph_last_error(nullptr);
+            } else {
+                try {
+                    printTextFile(v, static_cast<size_t>(w->n), s.file, w->mask);
+                } catch (const std::exception& ex) {
+                    code = GSPH_E_INVALID;
+                    msg = ex.what();
+                }
             }
         }
         {

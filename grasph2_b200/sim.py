@@ -414,3 +414,37 @@ def default_options():
 
 __all__ = ["DeviceParticleBuffer", "GsphError", "computeDerivatives", "integrate", "getCurrentTimestep",
            "from_state", "validate_params", "reference_default_params", "default_options", "ALL_ATTRIBS"]
+
+
+# ---- HDF5 snapshots (gsph_h5_*; the system's libhdf5, loaded when first needed) -------------------
+def h5_available():
+    """True when libhdf5 (1.10 or later) could be loaded."""
+    return bool(load_library().gsph_h5_available())
+
+
+def write_h5(filename, state, attributes=("pos", "mass", "vel", "density")):
+    """One float dataset per attribute (POS, MASS, VEL, DENSITY, ... as the reference names them)."""
+    lib = load_library()
+    names = list(attributes)
+    st = {k: np.ascontiguousarray(state[k], dtype=np.float32) for k in names}
+    hp = pointer_struct(st, GsphHostParticles, ctypes.c_float)
+    rc = lib.gsph_h5_write(str(filename).encode(), state_size(st) if "mass" in st else st[names[0]].shape[0],
+                           ctypes.byref(hp), mask_of(names))
+    if rc != 0:
+        raise GsphError(rc, lib.gsph_last_error(None).decode())
+
+
+def read_h5(filename, attributes=("pos", "mass", "vel", "density")):
+    lib = load_library()
+    names = list(attributes)
+    n = ctypes.c_int64(0)
+    rc = lib.gsph_h5_read(str(filename).encode(), 0, None, 0, ctypes.byref(n))
+    if rc != 0:
+        raise GsphError(rc, lib.gsph_last_error(None).decode())
+    full = new_state(n.value, np.float32)
+    st = {k: full[k] for k in names}
+    hp = pointer_struct(st, GsphHostParticles, ctypes.c_float)
+    rc = lib.gsph_h5_read(str(filename).encode(), mask_of(names), ctypes.byref(hp), n.value, ctypes.byref(n))
+    if rc != 0:
+        raise GsphError(rc, lib.gsph_last_error(None).decode())
+    return st

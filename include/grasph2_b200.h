@@ -477,6 +477,18 @@ int gsph_upload_device(gsph_ctx* ctx, uint32_t attr_mask, const gsph_host_partic
  * When every slot is busy, write waits for the oldest. Calls on a writer come from the thread that
  * drives its context; the context must outlive the writer.
  * ------------------------------------------------------------------------------------------- */
+/* HDF5 snapshots (the reference's STORE_HDF5 output, src/ResultStorageManager.cu:191-227, and its
+ * HDF5File particle source, src/initialConditions/particleSources/HDF5File.h:38-150): one float dataset
+ * per attribute in `mask`, named POS, MASS, VEL, ACC, BALSARA, XVEL, DENSITY, DENSITY_DT, DSTRESS,
+ * DSTRESS_DT, MAXVSIG, of shape {n, components}. The system's libhdf5 (1.10 or later) is loaded when
+ * first needed; without it these return GSPH_E_UNSUPPORTED (the reference's HDF5_AVAILABLE check,
+ * CMakeLists.txt:123-130). gsph_h5_read: n = the file's particle count; the arrays of `out` selected by
+ * `mask` (capacity `cap` particles) receive the values; mask 0 only counts. gsph_writer_write writes
+ * HDF5 instead of tsv when the file name ends in ".h5". */
+int gsph_h5_available(void);
+int gsph_h5_write(const char* filename, int64_t n, const gsph_host_particles* h, uint32_t mask);
+int gsph_h5_read(const char* filename, uint32_t mask, gsph_host_particles* out, int64_t cap, int64_t* n);
+
 typedef struct gsph_writer gsph_writer;
 int gsph_writer_create(gsph_ctx* ctx, uint32_t attr_mask, int32_t depth, gsph_writer** out);
 int gsph_writer_write(gsph_writer* w, const char* filename, void* stream);
