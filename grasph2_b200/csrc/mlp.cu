@@ -92,9 +92,10 @@ constexpr int kBias = 3 * kHid + kOutP;
 // shared-memory map (bytes)
 constexpr uint32_t sW1 = 0, sW2 = sW1 + kHid * kIn * 2, sW3 = sW2 + kHid * kHid * 2, sW4 = sW3 + kHid * kHid * 2,
                    sX = sW4 + kOutP * kHid * 2, sH1 = sX + kTileM * kIn * 2;
-// inference: per tile slot one input and one activation buffer
-constexpr int kSlots = 2;
-constexpr uint32_t kSlotBytes = kTileM * kIn * 2 + kTileM * kHid * 2;
+// inference: per tile slot one buffer, holding the tile's inputs until the first layer's MMAs have read
+// them and then its activations
+constexpr int kSlots = 4;
+constexpr uint32_t kSlotBytes = kTileM * kHid * 2;
 constexpr uint32_t sBiasF = sX + kSlots * kSlotBytes, kFwdSmem = sBiasF + kBias * 4;
 static_assert(kFwdSmem <= 227 * 1024, "forward kernel shared memory");
 // training: three activation buffers, the output gradient, the layer gradient, a block of ones
@@ -209,14 +210,13 @@ __device__ __forceinline__ void hidden_out(uint32_t tD, const float* bias, unsig
     }
 }
 
-// Forward over tiles of 128 rows (persistent grid): y[n][13] = MLP(x[n][32]). A CTA runs two
-// independent tile pipelines (slots) of two warpgroups each; a slot has its own input and activation
-// buffers, 128 tensor-memory columns, MMA barrier and named CTA barrier, so while one slot drains an
-// accumulator (bias, SiLU, bf16 pack) the tensor cores run the other slot's layer and its input loads
-// are in flight. Slot s takes tiles 2 b + s, 2 (b + grid) + s, ... of CTA b. In a slot, warp w drains
-// tensor-memory lanes 32 (w % 4) .. + 31 (its rows) and columns 64 (w / 4) .. + 63 of each hidden
-// accumulator; the first warpgroup writes the outputs.
-constexpr int kSlotThreads = 2 * kTileM, kFwdThreads = kSlots * kSlotThreads;
+// Forward over tiles of 128 rows (persistent grid): y[n][13] = MLP(x[n][32]). A CTA runs four
+// independent tile pipelines (slots) of one warpgroup each; a slot has its own buffer (inputs, then
+// activations), 128 tensor-memory columns (all 512 in use), MMA barrier and named CTA barrier, so while
+// one slot drains an accumulator (bias, SiLU, bf16 pack) the tensor cores run other slots' layers and
+// their input loads are in flight. Slot s takes tiles 4 b + s, 4 (b + grid) + s, ... of CTA b. Thread t
+// of a slot owns row t: warp w drains tensor-memory lanes 32 (w % 4) .. + 31, all columns.
+constexpr int kSlotThreads = kTileM, kFwdThreads = kSlots * kSlotThreads;
 
 __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __restrict__ x, float* __restrict__ y,
                                                                int64_t n, const __nv_bfloat16* __restrict__ wq,
@@ -230,16 +230,15 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __r
         for (int k = 0; k < kSlots; ++k) mbar_init(&bar[k], 1);
         fence_barrier_init();
     }
-    if (threadIdx.x < 32) umma::tmem_alloc(&tslot, 256);
+    if (threadIdx.x < 32) umma::tmem_alloc(&tslot, 128 * kSlots);
     umma::fence_before();
     __syncthreads();
     umma::fence_after();
-    const int slot = threadIdx.x / kSlotThreads, t = threadIdx.x % kSlotThreads;
-    const int row = t & (kTileM - 1), half = t / kTileM;
+    const int slot = threadIdx.x / kSlotThreads, row = threadIdx.x % kSlotThreads;
     const int bid = 1 + slot;  // named barrier of the slot (0 is __syncthreads)
     const uint32_t T = tslot + 128 * slot;
     const uint32_t base = smem_u32(sm);
-    const uint32_t xo = sX + slot * kSlotBytes, ho = xo + kTileM * kIn * 2;
+    const uint32_t xo = sX + slot * kSlotBytes, ho = xo;  // the inputs, then the activations
     uint64_t* mbar = &bar[slot];
     uint32_t phase = 0;
     // shared-memory writes and tensor-memory reads of the slot before the MMAs its first thread issues
@@ -258,16 +257,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __r
     };
     auto layer = [&](uint32_t a, uint32_t b, int N, int K) {
         slot_sync();
-        if (t == 0) {
+        if (row == 0) {
             issue(T, base + a, kTileM, false, base + b, N, false, N, K);
             umma::commit(mbar);
         }
         return slot_wait();
     };
-    // hidden epilogue of this thread's row and column half: h = SiLU(D + b)
+    // hidden epilogue of this thread's row: h = SiLU(D + b)
     auto hidden = [&](const float* bias) {
 #pragma unroll 1
-        for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 32) {
+        for (int c0 = 0; c0 < kHid; c0 += 32) {
             float v[32];
             umma::ld32(umma::lane_addr(T, c0), v);
 #pragma unroll
@@ -280,21 +279,21 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __r
     for (int64_t tile = static_cast<int64_t>(blockIdx.x) * kSlots + slot; tile < tiles;
          tile += static_cast<int64_t>(gridDim.x) * kSlots) {
         const int64_t p = tile * kTileM + row;
-        {  // inputs: 16 columns of one row per thread
-            float v[16];
+        {  // inputs: the 32 columns of this thread's row
+            float v[kIn];
             if (p < n) {
-                const float4* src = reinterpret_cast<const float4*>(x + p * kIn + 16 * half);
+                const float4* src = reinterpret_cast<const float4*>(x + p * kIn);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < kIn / 4; ++k) {
                     const float4 q = src[k];
                     v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < 16; ++k) v[k] = 0.0f;
+                for (int k = 0; k < kIn; ++k) v[k] = 0.0f;
             }
-            umma::st8(sm + xo, row, 16 * half, kTileM, v);
-            umma::st8(sm + xo, row, 16 * half + 8, kTileM, v + 8);
+#pragma unroll
+            for (int c = 0; c < kIn; c += 8) umma::st8(sm + xo, row, c, kTileM, v + c);
         }
         if (!layer(xo, sW1, kHid, kIn)) break;
         hidden(sbias);
@@ -303,7 +302,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __r
         if (!layer(ho, sW3, kHid, kHid)) break;
         hidden(sbias + 2 * kHid);
         if (!layer(ho, sW4, kOutP, kHid)) break;
-        if (half == 0) {
+        {
             float v[16];
             umma::ld16(umma::lane_addr(T, 0), v);
             if (p < n) {
@@ -314,7 +313,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __r
     }
     umma::fence_before();
     __syncthreads();
-    if (threadIdx.x < 32) umma::tmem_free(tslot, 256);
+    if (threadIdx.x < 32) umma::tmem_free(tslot, 128 * kSlots);
 }
 
 // ---- training: gradient of L = (1/n) sum_p sum_o w_o (y_po - t_po)^2 --------------------------------
