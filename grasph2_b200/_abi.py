@@ -242,6 +242,7 @@ _SIGNATURES = {
     "gsph_mlp_adam": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                      ctypes.c_void_p]),
     "gsph_mlp_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "gsph_mlp_set_grad_clip": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
     "gsph_gravity_accel_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_void_p]),
     "gsph_gravity_accel_static_status": (ctypes.c_int, [ctypes.c_void_p]),

@@ -531,12 +531,33 @@ __global__ void k_mlp_reduce(const float* __restrict__ part, int ncta, float* __
     }
 }
 
-// Adam (Kingma & Ba 2015) on the FP32 master parameters
+// the squared global norm of the gradient (one block, fixed summation order) for gradient clipping
+constexpr int kNormThreads = 1024;
+__global__ void __launch_bounds__(kNormThreads) k_mlp_grad_norm(const float* __restrict__ grad, double* __restrict__ out) {
+    __shared__ double sh[kNormThreads];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < kParams; i += kNormThreads) s += static_cast<double>(grad[i]) * grad[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = kNormThreads / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master parameters; with clip > 0 the gradient is first scaled by
+// min(1, clip / ||g||_2) (global-norm clipping, Pascanu, Mikolov & Bengio 2013)
 __global__ void k_mlp_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
-                           const float* __restrict__ grad, float lr, float b1, float b2, float eps, float c1, float c2) {
+                           const float* __restrict__ grad, float lr, float b1, float b2, float eps, float c1, float c2,
+                           float clip, const double* __restrict__ norm2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kParams) return;
-    const float gi = grad[i];
+    float gi = grad[i];
+    if (clip > 0.0f) {
+        const double nrm = sqrt(*norm2);
+        if (nrm > static_cast<double>(clip)) gi = static_cast<float>(gi * (static_cast<double>(clip) / nrm));
+    }
     const float mi = b1 * m[i] + (1.0f - b1) * gi;
     const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
     m[i] = mi;
@@ -579,6 +600,8 @@ struct gsph_mlp {
     __nv_bfloat16* wq = nullptr;
     float* bq = nullptr;
     int* status = nullptr;
+    double* norm2 = nullptr;  // squared gradient norm (clipping)
+    float clip = 0.0f;        // global-norm clipping threshold of the Adam step (0: off)
     int grid = 0;
     int64_t step = 0;
     std::string err;
@@ -598,7 +621,7 @@ int mfail(gsph_mlp* m, int code, const std::string& msg) {
     } while (0)
 
 void mlp_release(gsph_mlp* m) {
-    void* ptrs[] = {m->w, m->m, m->v, m->grad, m->part, m->loss_part, m->loss, m->wq, m->bq, m->status};
+    void* ptrs[] = {m->w, m->m, m->v, m->grad, m->part, m->loss_part, m->loss, m->wq, m->bq, m->status, m->norm2};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -640,6 +663,7 @@ int gsph_mlp_create(const float* params, gsph_mlp** out) {
     A(reinterpret_cast<void**>(&m->wq), kPacked * sizeof(__nv_bfloat16));
     A(reinterpret_cast<void**>(&m->bq), kBias * sizeof(float));
     A(reinterpret_cast<void**>(&m->status), sizeof(int));
+    A(reinterpret_cast<void**>(&m->norm2), sizeof(double));
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
     if (e == cudaSuccess && params) e = cudaMemcpy(m->w, params, kParams * sizeof(float), cudaMemcpyHostToDevice);
@@ -721,10 +745,22 @@ int gsph_mlp_adam(gsph_mlp* m, float lr, float beta1, float beta2, float eps, vo
     m->step += 1;
     const float c1 = 1.0f - powf(beta1, static_cast<float>(m->step));
     const float c2 = 1.0f - powf(beta2, static_cast<float>(m->step));
-    k_mlp_adam<<<(kParams + 255) / 256, 256, 0, s>>>(m->w, m->m, m->v, m->grad, lr, beta1, beta2, eps, c1, c2);
+    if (m->clip > 0.0f) {
+        k_mlp_grad_norm<<<1, kNormThreads, 0, s>>>(m->grad, m->norm2);
+        MLP_CK(m, cudaGetLastError(), "gradient norm launch");
+    }
+    k_mlp_adam<<<(kParams + 255) / 256, 256, 0, s>>>(m->w, m->m, m->v, m->grad, lr, beta1, beta2, eps, c1, c2, m->clip,
+                                                     m->norm2);
     MLP_CK(m, cudaGetLastError(), "adam launch");
     k_mlp_pack<<<(kPacked + 255) / 256, 256, 0, s>>>(m->w, m->wq, m->bq);
     MLP_CK(m, cudaGetLastError(), "pack launch");
+    return GSPH_OK;
+}
+
+int gsph_mlp_set_grad_clip(gsph_mlp* m, float max_norm) {
+    if (!m) return GSPH_E_INVALID;
+    if (!(max_norm >= 0.0f)) return mfail(m, GSPH_E_INVALID, "max_norm must be >= 0");
+    m->clip = max_norm;
     return GSPH_OK;
 }
 

@@ -109,6 +109,10 @@ class MLP:
             ctypes.byref(loss) if want else None, _stream_handle(stream)))
         return (grad, loss.value) if want else None
 
+    def set_grad_clip(self, max_norm):
+        """Global-norm clipping of the gradient in the following Adam steps (0: off)."""
+        self._check(self.lib.gsph_mlp_set_grad_clip(self._h, float(max_norm)))
+
     def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
         self._check(self.lib.gsph_mlp_adam(self._h, float(lr), float(beta1), float(beta2), float(eps),
                                            _stream_handle(stream)))

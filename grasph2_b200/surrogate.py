@@ -204,11 +204,12 @@ class Surrogate:
         return c.value
 
 
-def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, clip=0.0, stream=None):
+def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, clip=0.0, grad_clip=0.0,
+        stream=None):
     """Train a Surrogate on (X, Y) with the device kernels (forward + backward on the tensor cores, Adam);
     wout weights the 13 standardised outputs in the loss (default 1); clip > 0 limits the standardised
-    targets to +-clip (the heavy tails of the impact zone otherwise dominate single batches). Returns
-    (surrogate, loss history)."""
+    targets to +-clip (the heavy tails of the impact zone otherwise dominate single batches); grad_clip > 0
+    limits the global gradient norm of each Adam step. Returns (surrogate, loss history)."""
     torch = _torch()
     from .mlp import init_params
     in_mu, in_sig = X.mean(0), X.std(0) + 1e-6
@@ -222,6 +223,8 @@ def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=Non
         Yd.clamp_(-clip, clip)
     w = torch.from_numpy(np.asarray(wout if wout is not None else np.ones(NO), dtype=np.float32)).cuda()
     g = torch.Generator(device="cuda").manual_seed(seed)
+    if grad_clip > 0:
+        sur.net.set_grad_clip(grad_clip)
     m = X.shape[0]
     hist = []
     for step in range(steps):

@@ -35,6 +35,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--clip", type=float, default=0.0, help="limit the standardised targets to +-clip (0: off)")
+    ap.add_argument("--grad-clip", type=float, default=1.0, help="global gradient-norm clipping of Adam (0: off)")
     ap.add_argument("--K", type=int, default=8)
     ap.add_argument("--seed", type=int, default=20261207)
     ap.add_argument("--out", default=DEFAULT_OUT)
@@ -65,12 +66,12 @@ def main(argv=None):
     t_collect = time.time() - t0
     t0 = time.time()
     sur, hist = S.fit(X, Y, a.K, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=max(1, a.steps // 20),
-                      clip=a.clip)
+                      clip=a.clip, grad_clip=a.grad_clip)
     torch.cuda.synchronize()
     t_fit = time.time() - t0
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     meta = dict(n=a.n, trajectories=a.trajectories, windows=a.windows, every=a.every, rows=a.rows, steps=a.steps,
-                batch=a.batch, lr=a.lr, clip=a.clip, seed=a.seed, samples=int(X.shape[0]), collect_s=t_collect, fit_s=t_fit,
+                batch=a.batch, lr=a.lr, clip=a.clip, grad_clip=a.grad_clip, seed=a.seed, samples=int(X.shape[0]), collect_s=t_collect, fit_s=t_fit,
                 loss=[(int(s), float(l)) for s, l in hist])
     sur.save(a.out, meta=json.dumps(meta))
     sur.save(os.path.splitext(a.out)[0] + ".gsur")  # the native model file (gsph_surrogate_load)

@@ -335,6 +335,9 @@ int gsph_mlp_gradient(gsph_mlp* m, const float* x, const float* target, const fl
                       double* loss, void* stream);
 /* one Adam step (Kingma & Ba 2015) with the last gradient */
 int gsph_mlp_adam(gsph_mlp* m, float lr, float beta1, float beta2, float eps, void* stream);
+/* global-norm gradient clipping of the following Adam steps: the gradient is scaled by
+ * min(1, max_norm / ||g||_2) first (0 = off, the default) */
+int gsph_mlp_set_grad_clip(gsph_mlp* m, float max_norm);
 const char* gsph_mlp_last_error(const gsph_mlp* m);
 
 /* Surrogate support on a context (no counterpart in the reference).

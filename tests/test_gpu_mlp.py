@@ -123,6 +123,35 @@ def test_mlp_training_fits_a_teacher():
     assert l1 < 0.1 * l0, (l0, l1)
 
 
+@pytest.mark.parametrize("clip", [0.0, 1e-3, 1e6])
+def test_adam_with_gradient_clipping_matches_host(clip):
+    """Two Adam steps on the device against the host restatement: g scaled by min(1, clip / ||g||_2)
+    (clip 0 = off, a tiny clip always scales, a huge one never does), then Adam with bias correction."""
+    import torch
+    from grasph2_b200.mlp import MLP
+    p, x, t, w = _setup(3000, 17)
+    xd, td, wd = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), torch.from_numpy(w).cuda()
+    lr, b1, b2, eps = 1e-3, 0.9, 0.999, 1e-8
+    with MLP(p) as net:
+        net.set_grad_clip(clip)
+        wh = net.params().astype(np.float64)
+        mh = np.zeros_like(wh)
+        vh = np.zeros_like(wh)
+        for step in (1, 2):
+            g, _ = net.gradient(xd, td, wd, 3000)
+            g = g.astype(np.float64)
+            nrm = np.sqrt((g * g).sum())
+            if clip > 0 and nrm > clip:
+                g = g * (clip / nrm)
+            mh = b1 * mh + (1 - b1) * g
+            vh = b2 * vh + (1 - b2) * g * g
+            wh = wh - lr * (mh / (1 - b1 ** step)) / (np.sqrt(vh / (1 - b2 ** step)) + eps)
+            net.adam(lr=lr, beta1=b1, beta2=b2, eps=eps)
+            got = net.params().astype(np.float64)
+            np.testing.assert_allclose(got, wh, rtol=0, atol=2e-6 * max(1.0, np.abs(wh).max()))
+            wh = got  # continue from the device's FP32 parameters
+
+
 def test_mlp_forward_rejects_misaligned_inputs():
     """The input rows are read as 16-byte vectors: an input pointer off a 16-byte boundary is an error,
     not a fault."""
