@@ -604,7 +604,7 @@ def run_ensemble(args, rank, world, local):
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
     peak_tflops = None if args.no_peak else measure_fp32_peak(0.5)
-    ens = Ensemble(params, sizes, make_options(accum=args.accum))
+    ens = Ensemble(params, sizes, make_options(accum=args.accum, gravity=args.gravity))
     ens.upload(packed, stream=stream)
     shape = {"tile": 512, "ctas_per_sm": 0} if args.no_autotune else ens.autotune(1, stream)
     for _ in range(args.warmup):
@@ -643,7 +643,7 @@ def run_ensemble(args, rank, world, local):
     d2h = sum(a.nbytes for a in pinned_out.values())
     e2e_steps = 0 if args.no_e2e else max(3, min(args.steps, 10))
     e2e_ms = 0.0
-    with Ensemble(params, sizes, make_options(accum=args.accum)) as e2:
+    with Ensemble(params, sizes, make_options(accum=args.accum, gravity=args.gravity)) as e2:
         for k in range(e2e_steps + 2 if e2e_steps else 0):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)

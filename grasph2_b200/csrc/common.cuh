@@ -129,6 +129,41 @@ __device__ __forceinline__ void fold(float& s, float& c, float x) {
     c += e;
 }
 
+// ---- warp butterflies of the symmetric gravity kernels ----------------------------------------
+// NV values per lane (NV = 4 or 8) -> lane l holds the warp's sum of value (l >> (5 - log2 NV)) & (NV - 1):
+// a butterfly that halves the values at each of the first log2 NV levels (fixed order, so the sums are
+// the same on every run)
+__device__ __forceinline__ void reduce_lanes(float (&v)[8], int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const float send = b4 ? v[m] : v[m + 4], keep = b4 ? v[m + 4] : v[m];
+        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const float send = b3 ? v[m] : v[m + 2], keep = b3 ? v[m + 2] : v[m];
+        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const float send = b2 ? v[0] : v[1], keep = b2 ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+__device__ __forceinline__ void reduce_lanes(float (&v)[4], int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const float send = b4 ? v[m] : v[m + 2], keep = b4 ? v[m + 2] : v[m];
+        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    const float send = b3 ? v[0] : v[1], keep = b3 ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 4);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
 // ---- symmetric tensor helpers ----------------------------------------------------------------
 struct Sym {
     float xx, yy, zz, xy, xz, yz;

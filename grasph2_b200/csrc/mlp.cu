@@ -84,6 +84,11 @@ constexpr int kIn = 32, kHid = 128, kOut = 13, kOutP = 16;
 // flat FP32 parameter vector: W1[128][32] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] W4[13][128] b4[13]
 constexpr int oW1 = 0, ob1 = oW1 + kHid * kIn, oW2 = ob1 + kHid, ob2 = oW2 + kHid * kHid, oW3 = ob2 + kHid,
               ob3 = oW3 + kHid * kHid, oW4 = ob3 + kHid, ob4 = oW4 + kOut * kHid, kParams = ob4 + kOut;
+// stride of the per-CTA gradient slices: a multiple of 4 floats, so the weight rows (which start at multiples
+// of 4 within a slice) take 16-byte vector read-modify-writes
+constexpr int kPartStride = (kParams + 3) & ~3;
+static_assert(oW2 % 4 == 0 && oW3 % 4 == 0 && ob1 % 4 == 0 && ob2 % 4 == 0 && ob3 % 4 == 0 && kIn % 4 == 0 &&
+                  kHid % 4 == 0, "vector gradient rows");
 // packed BF16 weights (W4 padded to 16 rows) and FP32 biases (b4 padded to 16)
 constexpr int qW1 = 0, qW2 = qW1 + kHid * kIn, qW3 = qW2 + kHid * kHid, qW4 = qW3 + kHid * kHid,
               kPacked = qW4 + kOutP * kHid;
@@ -318,9 +323,24 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_forward(const float* __r
 
 // ---- training: gradient of L = (1/n) sum_p sum_o w_o (y_po - t_po)^2 --------------------------------
 // Tile k goes to CTA k % grid; each CTA adds its tiles' weight and bias gradients into its own FP32
-// slice part[cta][kParams] (no atomics) and its loss into loss_part[cta]; a second kernel sums the
+// slice part[cta][kPartStride] (no atomics) and its loss into loss_part[cta]; a second kernel sums the
 // slices in CTA order, so the gradient is deterministic.
 __device__ __forceinline__ void rmw(float* a, float v) { *a += v; }
+// a[0..N) += v[0..N), a 16-byte aligned: N/4 vector loads and stores instead of N scalar ones (same sums)
+template <int N>
+__device__ __forceinline__ void rmw_row(float* a, const float* v) {
+    static_assert(N % 4 == 0, "whole vectors");
+    float4* q = reinterpret_cast<float4*>(a);
+#pragma unroll
+    for (int k = 0; k < N / 4; ++k) {
+        float4 r = q[k];
+        r.x += v[4 * k];
+        r.y += v[4 * k + 1];
+        r.z += v[4 * k + 2];
+        r.w += v[4 * k + 3];
+        q[k] = r;
+    }
+}
 
 __global__ void __launch_bounds__(kTileM, 1) k_mlp_train(const float* __restrict__ x, const float* __restrict__ t,
                                                         const float* __restrict__ wout, int64_t n,
@@ -348,7 +368,7 @@ __global__ void __launch_bounds__(kTileM, 1) k_mlp_train(const float* __restrict
     // tensor-memory columns: z1 [0,128) z2 [128,256) z3 / dH [256,384) y / dW [384,512)
     const uint32_t T1 = tslot, T2 = tslot + 128, T3 = tslot + 256, T4 = tslot + 384;
     const uint32_t base = smem_u32(sm);
-    float* g = part + static_cast<int64_t>(blockIdx.x) * kParams;
+    float* g = part + static_cast<int64_t>(blockIdx.x) * kPartStride;
     const float inv_n = 1.0f / static_cast<float>(n);
     uint32_t phase = 0;
     double lsum = 0.0;
@@ -447,13 +467,9 @@ __global__ void __launch_bounds__(kTileM, 1) k_mlp_train(const float* __restrict
             for (int c0 = 0; c0 < kHid; c0 += 32) {
                 float v[32];
                 umma::ld32(umma::lane_addr(T4, c0), v);  // row t = output unit t
-#pragma unroll
-                for (int k = 0; k < 32; ++k) rmw(g + oW + t_id * kHid + c0 + k, v[k]);
+                rmw_row<32>(g + oW + t_id * kHid + c0, v);
                 umma::ld32(umma::lane_addr(T2, c0), v);
-                if (t_id == 0) {
-#pragma unroll
-                    for (int k = 0; k < 32; ++k) rmw(g + ob + c0 + k, v[k]);
-                }
+                if (t_id == 0) rmw_row<32>(g + ob + c0, v);
             }
             if (layer == 2) {  // z1 from its columns
 #pragma unroll
@@ -487,15 +503,11 @@ __global__ void __launch_bounds__(kTileM, 1) k_mlp_train(const float* __restrict
         {
             float v[32];
             umma::ld32(umma::lane_addr(T4, 0), v);
-#pragma unroll
-            for (int k = 0; k < kIn; ++k) rmw(g + oW1 + t_id * kIn + k, v[k]);
+            rmw_row<kIn>(g + oW1 + t_id * kIn, v);
 #pragma unroll 1
             for (int c0 = 0; c0 < kHid; c0 += 32) {
                 umma::ld32(umma::lane_addr(T2, c0), v);
-                if (t_id == 0) {
-#pragma unroll
-                    for (int k = 0; k < 32; ++k) rmw(g + ob1 + c0 + k, v[k]);
-                }
+                if (t_id == 0) rmw_row<32>(g + ob1 + c0, v);
             }
         }
         umma::fence_before();
@@ -521,7 +533,7 @@ __global__ void k_mlp_reduce(const float* __restrict__ part, int ncta, float* __
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < kParams) {
         float s = 0.0f;
-        for (int c = 0; c < ncta; ++c) s += part[static_cast<int64_t>(c) * kParams + i];
+        for (int c = 0; c < ncta; ++c) s += part[static_cast<int64_t>(c) * kPartStride + i];
         grad[i] = s;
     }
     if (i == 0) {
@@ -594,7 +606,7 @@ struct gsph_mlp {
     float* m = nullptr;      // Adam moments
     float* v = nullptr;
     float* grad = nullptr;
-    float* part = nullptr;   // [grid][kParams]
+    float* part = nullptr;   // [grid][kPartStride]
     double* loss_part = nullptr;
     double* loss = nullptr;
     __nv_bfloat16* wq = nullptr;
@@ -657,7 +669,7 @@ int gsph_mlp_create(const float* params, gsph_mlp** out) {
     A(reinterpret_cast<void**>(&m->m), kParams * sizeof(float));
     A(reinterpret_cast<void**>(&m->v), kParams * sizeof(float));
     A(reinterpret_cast<void**>(&m->grad), kParams * sizeof(float));
-    A(reinterpret_cast<void**>(&m->part), static_cast<size_t>(m->grid) * kParams * sizeof(float));
+    A(reinterpret_cast<void**>(&m->part), static_cast<size_t>(m->grid) * kPartStride * sizeof(float));
     A(reinterpret_cast<void**>(&m->loss_part), static_cast<size_t>(m->grid) * sizeof(double));
     A(reinterpret_cast<void**>(&m->loss), sizeof(double));
     A(reinterpret_cast<void**>(&m->wq), kPacked * sizeof(__nv_bfloat16));
@@ -728,7 +740,7 @@ int gsph_mlp_gradient(gsph_mlp* m, const float* x, const float* target, const fl
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int64_t tiles = (n + kTileM - 1) / kTileM;
     const int grid = static_cast<int>(tiles < m->grid ? tiles : m->grid);
-    MLP_CK(m, cudaMemsetAsync(m->part, 0, static_cast<size_t>(grid) * kParams * sizeof(float), s), "clear");
+    MLP_CK(m, cudaMemsetAsync(m->part, 0, static_cast<size_t>(grid) * kPartStride * sizeof(float), s), "clear");
     k_mlp_train<<<grid, kTileM, kTrainSmem, s>>>(x, target, wout, n, m->wq, m->bq, m->part, m->loss_part, m->status);
     MLP_CK(m, cudaGetLastError(), "gradient launch");
     k_mlp_reduce<<<(kParams + 255) / 256, 256, 0, s>>>(m->part, grid, m->grad, m->loss_part, m->loss, n);

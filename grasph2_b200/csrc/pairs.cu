@@ -692,39 +692,6 @@ constexpr int kSymCtas = 3;
 constexpr int kSymJB = 8;  // column particles per butterfly (8: three CTAs per SM; 4 fits four CTAs but its
                            // longer butterflies cost more than the occupancy gains)
 
-// NV values per lane (NV = 4 or 8) -> lane l holds the warp's sum of value (l >> (5 - log2 NV)) & (NV - 1):
-// a butterfly that halves the values at each of the first log2 NV levels (fixed order, so the sums are
-// the same on every run)
-__device__ __forceinline__ void reduce_lanes(float (&v)[8], int lane) {
-    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const float send = b4 ? v[m] : v[m + 4], keep = b4 ? v[m + 4] : v[m];
-        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-        const float send = b3 ? v[m] : v[m + 2], keep = b3 ? v[m + 2] : v[m];
-        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    const float send = b2 ? v[0] : v[1], keep = b2 ? v[1] : v[0];
-    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-}
-__device__ __forceinline__ void reduce_lanes(float (&v)[4], int lane) {
-    const bool b4 = lane & 16, b3 = lane & 8;
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-        const float send = b4 ? v[m] : v[m + 2], keep = b4 ? v[m + 2] : v[m];
-        v[m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    const float send = b3 ? v[0] : v[1], keep = b3 ? v[1] : v[0];
-    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 4);
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-}
 constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
 
 __host__ __device__ __forceinline__ void sym_task(int t, int G, int& ga, int& gb) {

@@ -178,7 +178,10 @@ typedef struct gsph_options {
                                 all-pairs gravity kernel evaluates every ordered pair (i gathers from all j), or
                                 every unordered pair once and applies it to both particles (Newton's third law;
                                 2/3 of the FP32 work, partials of 65 x 3 floats per particle). Auto picks the
-                                symmetric form from 24 blocks of 1024 particles up. Results agree to rounding */
+                                symmetric form from 24 blocks of 1024 particles up. Results agree to rounding.
+                                Ensembles use the one-sided sweep fused with their density pass; SYMMETRIC
+                                gives them a queue stage of group pairs instead (slower on ensembles of
+                                1k..32k-particle simulations) */
     int32_t gravity_groups;  /* symmetric form: particle groups G (tasks G(G+1)/2); 0 = up to 64 */
     int32_t wait_limit_us;   /* batched ensemble: a work item that waits for another item's result (a device-side
                                 spin on a counter) gives up after this many microseconds, sets the timeout bit

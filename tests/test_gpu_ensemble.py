@@ -83,20 +83,25 @@ def oracle_steps(oracle, p, nsteps):
 SIZES = [1, 2, 100, 511, 512, 513, 1500, 3000]
 
 
+@pytest.mark.parametrize("gravity", ["auto", "symmetric"])
 @pytest.mark.parametrize("accum", ["plain", "compensated"])
 @pytest.mark.parametrize("name", list(VARIANTS))
-def test_ensemble_derivatives_vs_oracle(oracle, name, accum):
+def test_ensemble_derivatives_vs_oracle(oracle, name, accum, gravity):
+    """Every simulation against the oracle; with gravity and SPH, `auto` is the one-sided sweep fused with
+    the density pass and `symmetric` the stage of group pairs (512-particle groups, ragged last groups: the
+    sizes straddle 512)."""
     p = VARIANTS[name]()
     rho0 = p.rho0
     states = [sim_state(n, seed=100 + k, rho0=rho0, omega=0.1 * k) for k, n in enumerate(SIZES)]
-    with Ensemble(p, SIZES, make_options(accum=accum)) as ens:
+    with Ensemble(p, SIZES, make_options(accum=accum, gravity=gravity)) as ens:
         ens.upload(pack_states(states))
         ens.compute_derivatives()
         got = ens.split(ens.download())
     for k, st in enumerate(states):
         ref, sens = fp32_sensitivity(oracle_derivs(oracle, p), st, trials=1)
         for f, tol in fields(p).items():
-            check_within(got[k][f], ref[f], sens[f], tol, "%s/%s sim %d (n=%d) %s" % (name, accum, k, SIZES[k], f))
+            check_within(got[k][f], ref[f], sens[f], tol, "%s/%s/%s sim %d (n=%d) %s" % (name, accum, gravity, k,
+                                                                                         SIZES[k], f))
 
 
 @pytest.mark.parametrize("name", ["fluid", "solid", "nbody", "solid_mc"])
