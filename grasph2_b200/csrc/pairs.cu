@@ -677,22 +677,18 @@ __global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ p
 // accumulated per j-tile and then added to the running sum (plain: a sum of 256-term sums, whose
 // rounding error grows with the tile count instead of the pair count; compensated: a two-sum fold whose
 // error terms live in shared memory); the column particle's contribution is summed over the CTA's 1024 row particles -- in the thread, then
-// across the warp by a butterfly that leaves kSymJB column sums spread over the lanes, then over the
-// four warps in shared memory -- and added to its slot in the partials (plain, or two-sum when
-// compensated). The pairs inside a block (the diagonal tile) run one-sided. Each particle has G + 1
+// across the warp by rotation (each lane takes the 32 columns of a block in turn and hands each column's
+// running sum on to its neighbour), then over the four warps in shared memory -- and added to its slot
+// in the partials (plain, or two-sum when compensated). The pairs inside a block (the diagonal tile) run one-sided. Each particle has G + 1
 // slots, each written by one task (its row sums from tasks (g, gb), its column sums from tasks (ga, g),
 // g its group); the finish kernels add a particle's slots in a fixed order, so results do not depend on
 // scheduling. FMA-pipe work per pair interaction: 8 + ~0.4 operations
 // against the one-sided kernel's 12.
 constexpr int kSymT = 128, kSymI = 8, kSymB = kSymT * kSymI, kSymJT = 256;
-// CTAs per SM the register budget is set for. Three: at four (128 registers) the pair loop spills a
-// little and the kernel runs no faster (Plummer N = 2^20: 337.9 vs 339.6 ms plain, 346.8 vs 343.5 ms
-// compensated)
-constexpr int kSymCtas = 3;
-constexpr int kSymJB = 8;  // column particles per butterfly (8: three CTAs per SM; 4 fits four CTAs but its
-                           // longer butterflies cost more than the occupancy gains)
-
-constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
+// CTAs per SM the register budget is set for. Four (128 registers, no spills with the rotating column
+// sums): Plummer N = 2^20, 128 groups, 340.5 ms plain and 340.5 ms compensated, against 338.7 / 350.6 ms
+// for a warp butterfly over batches of 8 columns at three CTAs per SM; five spill and run slower (359.6 ms)
+constexpr int kSymCtas = 4;
 
 __host__ __device__ __forceinline__ void sym_task(int t, int G, int& ga, int& gb) {
     const int noff = G * (G - 1) / 2;
@@ -792,12 +788,17 @@ __global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* _
                     }
                 }
             } else {
+                // column sums by rotation: in round r of a block of 32 columns, lane l pairs its rows
+                // with column (l + r) % 32, adds its share to that column's running sum and hands the sum
+                // to lane l - 1, which takes the column in round r + 1; after 32 rounds lane l holds the
+                // warp's sum for column l (no butterfly, no selects, 3 shuffles per column)
+                const int next = (lane + 1) & 31;
 #pragma unroll 1
-                for (int j0 = 0; j0 < kSymJT; j0 += kSymJB) {
-                    float vx[kSymJB], vy[kSymJB], vz[kSymJB];
-#pragma unroll
-                    for (int jj = 0; jj < kSymJB; ++jj) {
-                        const float4 q = J[j0 + jj];
+                for (int j0 = 0; j0 < kSymJT; j0 += 32) {
+                    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+#pragma unroll 2
+                    for (int r = 0; r < 32; ++r) {
+                        const float4 q = J[j0 + ((lane + r) & 31)];
                         const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y),
                                      qz = make_float2(q.z, q.z), qm = make_float2(q.w, q.w);
                         float2 tx = make_float2(0.0f, 0.0f), ty = tx, tz = tx;
@@ -812,20 +813,13 @@ __global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* _
                             TX[m] = fma2(dx, sj, TX[m]); TY[m] = fma2(dy, sj, TY[m]); TZ[m] = fma2(dz, sj, TZ[m]);
                             tx = fma2(dx, si, tx); ty = fma2(dy, si, ty); tz = fma2(dz, si, tz);
                         }
-                        vx[jj] = tx.x + tx.y;
-                        vy[jj] = ty.x + ty.y;
-                        vz[jj] = tz.x + tz.y;
+                        cx = __shfl_sync(0xffffffffu, cx + (tx.x + tx.y), next);
+                        cy = __shfl_sync(0xffffffffu, cy + (ty.x + ty.y), next);
+                        cz = __shfl_sync(0xffffffffu, cz + (tz.x + tz.y), next);
                     }
-                    reduce_lanes(vx, lane);
-                    reduce_lanes(vy, lane);
-                    reduce_lanes(vz, lane);
-                    constexpr int sh = 5 - log2_c(kSymJB);
-                    if ((lane & ((1 << sh) - 1)) == 0) {
-                        const int j = j0 + ((lane >> sh) & (kSymJB - 1));
-                        js[warp][j][0] = vx[0];
-                        js[warp][j][1] = vy[0];
-                        js[warp][j][2] = vz[0];
-                    }
+                    js[warp][j0 + lane][0] = cx;
+                    js[warp][j0 + lane][1] = cy;
+                    js[warp][j0 + lane][2] = cz;
                 }
             }
             // the tile's row partials into the running sums: a two-sum fold (compensated), or one add
