@@ -205,11 +205,15 @@ class Surrogate:
 
 
 def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=None, clip=0.0, grad_clip=0.0,
-        stream=None):
+        stream=None, eval_rows=65536):
     """Train a Surrogate on (X, Y) with the device kernels (forward + backward on the tensor cores, Adam);
     wout weights the 13 standardised outputs in the loss (default 1); clip > 0 limits the standardised
     targets to +-clip (the heavy tails of the impact zone otherwise dominate single batches); grad_clip > 0
-    limits the global gradient norm of each Adam step. Returns (surrogate, loss history)."""
+    limits the global gradient norm of each Adam step. Returns (surrogate, loss history): every log_every
+    steps (step, loss of that step's batch, loss on a fixed evaluation set of eval_rows samples drawn once
+    with seed + 1). A batch loss follows its batch (a batch holding a few impact-zone samples can read
+    30x the typical loss); the evaluation loss follows the model. The evaluation runs before the step's
+    own gradient, which overwrites it, so training is the same with or without it."""
     torch = _torch()
     from .mlp import init_params
     in_mu, in_sig = X.mean(0), X.std(0) + 1e-6
@@ -227,14 +231,20 @@ def fit(X, Y, K, steps=2000, batch=65536, lr=1e-3, seed=0, log_every=0, wout=Non
         sur.net.set_grad_clip(grad_clip)
     m = X.shape[0]
     hist = []
+    if log_every:
+        ge = torch.Generator(device="cuda").manual_seed(seed + 1)
+        eidx = torch.randint(0, m, (min(eval_rows, m),), device="cuda", generator=ge)
+        xe, ye = Xd[eidx].contiguous(), Yd[eidx].contiguous()
     for step in range(steps):
         idx = torch.randint(0, m, (min(batch, m),), device="cuda", generator=g)
         xb, yb = Xd[idx].contiguous(), Yd[idx].contiguous()
         rate = lr * 0.5 * (1.0 + math.cos(math.pi * step / steps))  # cosine decay
         want = log_every and (step % log_every == 0 or step == steps - 1)
+        if want:
+            le = sur.net.gradient(xe, ye, w, xe.shape[0], stream, want=True)[1]
         r = sur.net.gradient(xb, yb, w, xb.shape[0], stream, want=bool(want))
         if want:
-            hist.append((step, r[1]))
+            hist.append((step, r[1], le))
         sur.net.adam(lr=rate, stream=stream)
     return sur, hist
 

@@ -72,7 +72,7 @@ def main(argv=None):
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     meta = dict(n=a.n, trajectories=a.trajectories, windows=a.windows, every=a.every, rows=a.rows, steps=a.steps,
                 batch=a.batch, lr=a.lr, clip=a.clip, grad_clip=a.grad_clip, seed=a.seed, samples=int(X.shape[0]), collect_s=t_collect, fit_s=t_fit,
-                loss=[(int(s), float(l)) for s, l in hist])
+                loss=[(int(s), float(l)) for s, l, _ in hist], eval_loss=[(int(s), float(e)) for s, _, e in hist])
     sur.save(a.out, meta=json.dumps(meta))
     sur.save(os.path.splitext(a.out)[0] + ".gsur")  # the native model file (gsph_surrogate_load)
     with open(os.path.splitext(a.out)[0] + ".json", "w") as f:
