@@ -402,14 +402,15 @@ __device__ __forceinline__ bool dens_item(const DevArrays& a, const DevParams& p
 // Task (sim, ga, gb), ga <= gb: every pair of a particle of group ga (the rows, four per thread in two
 // f32x2 pairs) and one of group gb (the columns, streamed by the pipe) is evaluated once and its 1/r^3
 // serves both: the rows' sums stay in registers, the columns' are summed over the task's rows (in the
-// thread, over the warp by lane rotation, then over the four warps in shared memory). The diagonal task
+// thread, by a butterfly over the warp, then over the four warps in shared memory). The diagonal task
 // (ga == gb) runs one-sided over the group's own pairs. Every particle of a simulation with G groups has
 // G + 1 slots, [slot][component][particle of the simulation]: its row sums from tasks (g, gb) in slots
 // 0 .. G-1-g, its column sums from tasks (ga, g) in slots G-g .. G, each written by exactly one task (the
 // diagonal task zeroes slot G); the SPH stage folds them in FP64 in slot order, so results are
 // deterministic. Rows past the group's end are inert (zero mass, far away); columns past the simulation's
 // end are never read.
-constexpr int kEnsJC = 128;  // columns per shared-memory reduction round (a multiple of 32)
+constexpr int kEnsJC = 128;  // columns per shared-memory reduction round
+constexpr int kEnsJB = 8;    // columns per warp butterfly
 
 __device__ __forceinline__ float* sim_slots(const EnsView& v, int sim) { return v.gslot + v.slot_base[sim]; }
 
@@ -448,36 +449,12 @@ __device__ __forceinline__ bool gsym_item(const DevArrays& a, const DevParams& p
         for (int k = 0; k < P; ++k) TX[k] = TY[k] = TZ[k] = make_float2(0.0f, 0.0f);
         for (int j0 = 0; j0 < nj; j0 += kEnsJC) {
             const int jn = min(kEnsJC, nj - j0);
-            if (diag) {  // one-sided over the group's own pairs
-#pragma unroll 4
-                for (int u = 0; u < jn; ++u) {
-                    const float4 q = J[j0 + u];
-                    const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y), qz = make_float2(q.z, q.z),
-                                 qm = make_float2(q.w, q.w);
-#pragma unroll
-                    for (int k = 0; k < P; ++k) {
-                        const float2 dx = sub2(qx, X[k]), dy = sub2(qy, Y[k]), dz = sub2(qz, Z[k]);
-                        const float2 r2 = fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, E2)));
-                        float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-                        if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
-                        const float2 sj = mul2(qm, mul2(mul2(inv, inv), inv));
-                        TX[k] = fma2(dx, sj, TX[k]); TY[k] = fma2(dy, sj, TY[k]); TZ[k] = fma2(dz, sj, TZ[k]);
-                    }
-                }
-                continue;
-            }
-            // column sums by rotation: in round r of a block of 32 columns lane l pairs its rows with
-            // column (l + r) % 32, adds its share to that column's running sum and hands the sum to lane
-            // l - 1; after 32 rounds lane l holds the warp's sum for column l of the block (columns past
-            // jn are inert: far away, zero mass, never stored)
-            const int next = (lane + 1) & 31;
 #pragma unroll 1
-            for (int u0 = 0; u0 < jn; u0 += 32) {
-                float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-#pragma unroll 2
-                for (int r = 0; r < 32; ++r) {
-                    const int u = u0 + ((lane + r) & 31);
-                    const float4 q = u < jn ? J[j0 + u] : inert;
+            for (int u0 = 0; u0 < jn; u0 += kEnsJB) {
+                float vx[kEnsJB], vy[kEnsJB], vz[kEnsJB];
+#pragma unroll
+                for (int u = 0; u < kEnsJB; ++u) {
+                    const float4 q = (u0 + u < jn) ? J[j0 + u0 + u] : inert;
                     const float2 qx = make_float2(q.x, q.x), qy = make_float2(q.y, q.y), qz = make_float2(q.z, q.z),
                                  qm = make_float2(q.w, q.w);
                     float2 tx = make_float2(0.0f, 0.0f), ty = tx, tz = tx;
@@ -488,19 +465,30 @@ __device__ __forceinline__ bool gsym_item(const DevArrays& a, const DevParams& p
                         float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
                         if (GRAV == 2) inv = make_float2(fminf(inv.x, 1e12f), fminf(inv.y, 1e12f));
                         const float2 i3 = mul2(mul2(inv, inv), inv);
-                        const float2 sj = mul2(qm, i3), si = mul2(MI[k], i3);
+                        const float2 sj = mul2(qm, i3);
                         TX[k] = fma2(dx, sj, TX[k]); TY[k] = fma2(dy, sj, TY[k]); TZ[k] = fma2(dz, sj, TZ[k]);
-                        tx = fma2(dx, si, tx); ty = fma2(dy, si, ty); tz = fma2(dz, si, tz);
+                        if (!diag) {
+                            const float2 si = mul2(MI[k], i3);
+                            tx = fma2(dx, si, tx); ty = fma2(dy, si, ty); tz = fma2(dz, si, tz);
+                        }
                     }
-                    cx = __shfl_sync(0xffffffffu, cx + (tx.x + tx.y), next);
-                    cy = __shfl_sync(0xffffffffu, cy + (ty.x + ty.y), next);
-                    cz = __shfl_sync(0xffffffffu, cz + (tz.x + tz.y), next);
+                    vx[u] = tx.x + tx.y;
+                    vy[u] = ty.x + ty.y;
+                    vz[u] = tz.x + tz.y;
                 }
-                js[warp][u0 + lane][0] = cx;
-                js[warp][u0 + lane][1] = cy;
-                js[warp][u0 + lane][2] = cz;
+                if (!diag) {
+                    reduce_lanes(vx, lane);
+                    reduce_lanes(vy, lane);
+                    reduce_lanes(vz, lane);
+                    if ((lane & 3) == 0) {
+                        const int u = u0 + ((lane >> 2) & (kEnsJB - 1));
+                        js[warp][u][0] = vx[0];
+                        js[warp][u][1] = vy[0];
+                        js[warp][u][2] = vz[0];
+                    }
+                }
             }
-            {  // this round's column sums over the task's rows, into the column slots
+            if (!diag) {  // this round's column sums over the task's rows, into the column slots
                 __syncthreads();
                 const int lc0 = static_cast<int>(jb - c0) + j0;
                 for (int e = threadIdx.x; e < jn; e += kEnsThreads)
