@@ -55,7 +55,8 @@ FLUSH_BYTES = 256 << 20
 # kernel's traffic is its j-records (16 B per particle, read once from DRAM, then from L2) plus its
 # partial slots ((G + 1) x 12 B per particle, written once), so at fixed G it scales with N.
 MEASURED_TRAFFIC = {
-    ("plummer", "gravity", "symmetric", 128): (682673280.0, 262144),  # ncu, N = 262,144, 2 launches (mean)
+    ("plummer", "gravity", "symmetric", 128): (356643200.0, 262144),  # ncu, N = 262,144, 2 launches (mean)
+    ("impact", "gravity", "symmetric", 64): (2185728.0, 65536),  # ncu, the impact itself, 2 launches (mean)
 }
 FLAG_DEAL_WITH_NO_PARTNERS = 1 << 3  # GSPH_DEAL_WITH_NO_PARTNERS
 
