@@ -685,6 +685,7 @@ __global__ void __launch_bounds__(128) k_gravity_x2(const float4* __restrict__ p
 // scheduling. FMA-pipe work per pair interaction: 8 + ~0.4 operations
 // against the one-sided kernel's 12.
 constexpr int kSymT = 128, kSymI = 8, kSymB = kSymT * kSymI, kSymJT = 256;
+static_assert(kSymB % kSymJT == 0 && kSymJT % kSymT == 0 && kSymJT % 32 == 0, "symmetric gravity tiles");
 // CTAs per SM the register budget is set for. Four (128 registers, no spills with the rotating column
 // sums): Plummer N = 2^20, 128 groups, 340.5 ms plain and 340.5 ms compensated, against 338.7 / 350.6 ms
 // for a warp butterfly over batches of 8 columns at three CTAs per SM; five spill and run slower (359.6 ms)
@@ -754,19 +755,22 @@ __global__ void __launch_bounds__(kSymT, kSymCtas) k_gravity_sym(const float4* _
         const int total = nd + nc;
         const bool first = a == ra0;
         auto src = [&](int k) { return k < nd ? d0 + static_cast<int64_t>(k) * kSymJT : c0 + static_cast<int64_t>(k - nd) * kSymJT; };
-        float4 pf0 = make_float4(0, 0, 0, 0), pf1 = pf0;
+        constexpr int kPf = kSymJT / kSymT;  // j-records each thread stages per tile
+        float4 pf[kPf];
+#pragma unroll
+        for (int h = 0; h < kPf; ++h) pf[h] = make_float4(0, 0, 0, 0);
         if (total > 0) {
-            pf0 = posm[src(0) + tid];
-            pf1 = posm[src(0) + kSymT + tid];
+#pragma unroll
+            for (int h = 0; h < kPf; ++h) pf[h] = posm[src(0) + h * kSymT + tid];
         }
         for (int k = 0; k < total; ++k) {
             __syncthreads();  // the previous tile's reads of J and js are done
-            J[tid] = pf0;
-            J[tid + kSymT] = pf1;
+#pragma unroll
+            for (int h = 0; h < kPf; ++h) J[tid + h * kSymT] = pf[h];
             __syncthreads();
             if (k + 1 < total) {
-                pf0 = posm[src(k + 1) + tid];
-                pf1 = posm[src(k + 1) + kSymT + tid];
+#pragma unroll
+                for (int h = 0; h < kPf; ++h) pf[h] = posm[src(k + 1) + h * kSymT + tid];
             }
             float2 TX[P], TY[P], TZ[P];
 #pragma unroll
