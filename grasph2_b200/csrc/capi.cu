@@ -508,7 +508,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         SpatialArrays& sp = c->sp;
         const int64_t nchunks = n_pad / kChunk, ngroups = n_pad / kGroup;
         L.item_grid = c->sm_count * 5;      // 41 KB of shared memory and at most 102 registers: 5 per SM
-        L.density_grid = c->sm_count * 12;  // 37 registers and 8 KB of shared memory: 12 fit per SM
+        L.density_grid = c->sm_count * 12;  // 40 registers (launch bound) and 8 KB of shared memory: 12 per SM
         sp.item_target = 6 * L.item_grid;
         sp.item_start = static_cast<int*>(dalloc(c, (ngroups + 2) * sizeof(int), ae));
         // worst case fields per item: fused solids pass without gravity, compensated (x2); items are at

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ posm
 // culled density sum over the near-chunk work items (persistent grid); with LISTS every lane also
 // records the indices of its neighbours in this item (for the SPH passes of the same step)
 template <bool COMP, bool LISTS>
-__global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restrict__ posm, DevParams p, CullView cv,
+__global__ void __launch_bounds__(kGroup, 12) k_density_items(const float4* __restrict__ posm, DevParams p, CullView cv,
                                                           int* status) {
     constexpr int SJ = kStageChunks * kChunk;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -110,12 +110,32 @@ __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restri
     pipe.init();
     const uint32_t span = __float_as_uint(p.H2);
     const int total = cv.items();
+    __shared__ float4 wbox[kGroup / 32][2];  // each warp's bounding box for the current item
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
         int g, c0, c1;
         cv.item(w, g, c0, c1);
         const float4 pi = posm[static_cast<int64_t>(g) * kGroup + threadIdx.x];
         float rho_s = 0.0f, rho_c = 0.0f;
         int cnt = 0;
+        // the warp's bounding box: a chunk of the group's list that lies farther than h (1 + kMargin)
+        // from it (the list's own conservative bound) holds no neighbour of the warp's 32 particles, and
+        // the warp skips its tests (same sums, same lists; padding lanes only widen the box)
+        if (LISTS) {
+            float wlo[3] = {pi.x, pi.y, pi.z}, whi[3] = {pi.x, pi.y, pi.z};
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    wlo[c] = fminf(wlo[c], __shfl_xor_sync(0xffffffffu, wlo[c], o));
+                    whi[c] = fmaxf(whi[c], __shfl_xor_sync(0xffffffffu, whi[c], o));
+                }
+            __syncwarp();  // the previous item's reads of this warp's box are done
+            if ((threadIdx.x & 31) == 0) {
+                wbox[threadIdx.x >> 5][0] = make_float4(wlo[0], wlo[1], wlo[2], 0.0f);
+                wbox[threadIdx.x >> 5][1] = make_float4(whi[0], whi[1], whi[2], 0.0f);
+            }
+            __syncwarp();
+        }
         int* lst = LISTS ? cv.nb + static_cast<int64_t>(w) * kItemNb * kGroup + threadIdx.x : nullptr;
         const int* chunks = cv.list + static_cast<int64_t>(g) * cv.nchunks + c0;
         int chunk_base = 0;
@@ -124,7 +144,16 @@ __global__ void __launch_bounds__(kGroup) k_density_items(const float4* __restri
                 if (LISTS) {  // the density_tile sum, recording the neighbours as well (same order)
                     t = 0.0f;
                     for (int s0 = 0; s0 < nj; s0 += kChunk) {
-                        const int jb = chunks[chunk_base + s0 / kChunk] * kChunk;
+                        const int jc = chunks[chunk_base + s0 / kChunk], jb = jc * kChunk;
+                        {
+                            const float4 l = cv.box_lo[jc], u = cv.box_hi[jc];
+                            const float4 wl = wbox[threadIdx.x >> 5][0], wh = wbox[threadIdx.x >> 5][1];
+                            const float gx = fmaxf(0.0f, fmaxf(l.x - wh.x, wl.x - u.x)),
+                                        gy = fmaxf(0.0f, fmaxf(l.y - wh.y, wl.y - u.y)),
+                                        gz = fmaxf(0.0f, fmaxf(l.z - wh.z, wl.z - u.z));
+                            const float hm = p.H * (1.0f + kMargin);
+                            if (gx * gx + gy * gy + gz * gz > hm * hm) continue;  // warp-uniform
+                        }
                         // the chunk's 64 tests into a bit mask without branches, then its set bits in
                         // ascending order (the neighbours, about 2 % of the tests)
                         unsigned m8[8];
@@ -1014,6 +1043,8 @@ CullView cull_view(const DevArrays& a, const SpatialArrays& sp) {
     cv.nb = nullptr;
     cv.nbcnt = nullptr;
     cv.nbover = nullptr;
+    cv.box_lo = sp.box_lo;
+    cv.box_hi = sp.box_hi;
     return cv;
 }
 PartView seg_view(const DevArrays& a, int nseg, int KK, bool err) {

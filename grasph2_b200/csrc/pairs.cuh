@@ -101,6 +101,8 @@ struct CullView {
     int* nb;                // nullable: per item, each lane's neighbour indices [item][kItemNb][kGroup] ...
     int* nbcnt;             // ... and their count [item][kGroup] (kItemNb + 1: the list overflowed) ...
     int* nbover;            // ... and per item whether any lane's list overflowed
+    const float4* box_lo;   // per-chunk bounding boxes (the culled density pass skips, warp by warp, the
+    const float4* box_hi;   // chunks of an item that are farther than h (1 + kMargin) from the warp's box)
     __device__ __forceinline__ int items() const { return item_start[ngroups]; }
     __device__ __forceinline__ void item(int w, int& g, int& c0, int& c1) const {
         int lo = 0, hi = ngroups;  // item_start[lo] <= w < item_start[hi]
