@@ -458,13 +458,14 @@ def total_energy(d):
     return d["e_kin"] + d["e_grav"] + d["e_int"] + d["e_shear"]
 
 
-def energy_drift(params, st, steps, every, stream, forms=("plain", "compensated")):
+def energy_drift(params, st, steps, every, stream, forms=("plain", "compensated"), autotune=True):
     """Total energy along `steps` steps of each FP32 form and of the double-precision form, all from
     the same float32-representable state. Every `every` steps the derivatives are refreshed at the
     current positions and the energy is taken at the synchronous velocity v + a dt/2. Returns, per
     form, max_t |E(t) - E_fp64(t)| / |E_fp64(0)| (the drift against the FP64 trajectory), its own
     max_t |E(t) - E(0)| / |E(0)|, and the simulated time per wall-second of its stepping (CUDA events
-    around the step launches, diagnostics excluded)."""
+    around the step launches, diagnostics excluded). Each FP32 form first takes its own autotuned launch
+    shapes, as the headline runs do (the tuner evaluates derivatives only: the state does not move)."""
     import torch
     from grasph2_b200.params import make_options
     from grasph2_b200.sim import DeviceParticleBuffer
@@ -478,6 +479,8 @@ def energy_drift(params, st, steps, every, stream, forms=("plain", "compensated"
         energies, ms = [], 0.0
         with DeviceParticleBuffer(params, n, opt) as pb:
             pb.upload_f64(st, stream=stream)
+            if form != "fp64" and autotune:
+                pb.autotune(stream=stream)
             done = 0
             while True:
                 pb.compute_derivatives(stream)
@@ -1021,7 +1024,7 @@ def run_context(args, rank, world, local, dist=None):
     if args.drift_steps < 0:
         args.drift_steps = 1000 if args.workload == "impact" else 0
     if args.drift_steps > 0:
-        drift = energy_drift(params, st, args.drift_steps, args.drift_every, stream)
+        drift = energy_drift(params, st, args.drift_steps, args.drift_every, stream, autotune=not args.no_autotune)
 
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
