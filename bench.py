@@ -50,13 +50,17 @@ FLOP_ACC_NB = 60           # pressure acceleration + AV per neighbour (fluid, ac
 FLUSH_BYTES = 256 << 20
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture of the same kernel
-# and launch shape on a smaller case (profiles/ holds the command): key (workload, kernel slot, gravity
-# form, symmetric groups) -> (bytes per launch, particles of the captured case). The symmetric gravity
-# kernel's traffic is its j-records (16 B per particle, read once from DRAM, then from L2) plus its
-# partial slots ((G + 1) x 12 B per particle, written once), so at fixed G it scales with N.
+# and launch shape, on a smaller case where the full one is too large to capture (profiles/ holds the
+# commands): key (workload, kernel slot, gravity form, symmetric groups; for the ensemble its number of
+# simulations) -> (bytes per launch, particles of the captured case). The symmetric gravity kernel's
+# traffic is its j-records (16 B per particle, read once from DRAM, then from L2) plus its partial slots
+# ((G + 1) x 12 B per particle, written once), so at fixed G it scales with N.
 MEASURED_TRAFFIC = {
     ("plummer", "gravity", "symmetric", 128): (356643200.0, 262144),  # ncu, N = 262,144, 2 launches (mean)
     ("impact", "gravity", "symmetric", 64): (2185728.0, 65536),  # ncu, the impact itself, 2 launches (mean)
+    # the 512-simulation ensemble itself (4,630,521 particles, DENS j-tile 512), 2 launches (mean): the
+    # neighbour lists the DENS stage writes and the SPH stage reads dominate it
+    ("ensemble", "k_ensemble", "one-sided", 512): (5093712128.0, 4630521),
 }
 FLAG_DEAL_WITH_NO_PARTNERS = 1 << 3  # GSPH_DEAL_WITH_NO_PARTNERS
 
@@ -711,6 +715,10 @@ def run_ensemble(args, rank, world, local):
                          "diverge at the particle level in any precision, so their energy comparison is not a "
                          "precision measure",
                  "sample": "8 simulations spanning the size range, run as an ensemble (FP32) and one by one in FP64"}
+    form = "symmetric" if args.gravity == "symmetric" else "one-sided"
+    ens_traffic = MEASURED_TRAFFIC.get(("ensemble", "k_ensemble", form, len(sizes)))
+    if ens_traffic is not None:
+        ens_traffic = ens_traffic[0] * n_total / ens_traffic[1]
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -727,8 +735,8 @@ def run_ensemble(args, rank, world, local):
         "sequential_plain_ms_per_step": seq_ms,
         "speedup_vs_sequential": (seq_ms / ms_per_step) if seq_ms else None,
         "roofline": {"bound": "fp32", "kernel": "k_ensemble", "achieved": achieved, "peak": peak_tflops,
-                     "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if peak_tflops else None, "traffic": None,
-                     "flops_per_launch": flops, "neighbour_pairs": nb,
+                     "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if peak_tflops else None,
+                     "traffic": ens_traffic, "flops_per_launch": flops, "neighbour_pairs": nb,
                      "peak_source": "FFMA throughput measured in this run (gsph_measure_fp32_peak)"},
         "cpu_baseline": cpu,
         "clocks": clocks,
