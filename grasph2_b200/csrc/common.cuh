@@ -129,7 +129,7 @@ __device__ __forceinline__ void fold(float& s, float& c, float x) {
     c += e;
 }
 
-// ---- warp butterflies of the symmetric gravity kernels ----------------------------------------
+// ---- warp butterflies (the ensemble's symmetric gravity stage) ----------------------------------
 // NV values per lane (NV = 4 or 8) -> lane l holds the warp's sum of value (l >> (5 - log2 NV)) & (NV - 1):
 // a butterfly that halves the values at each of the first log2 NV levels (fixed order, so the sums are
 // the same on every run)
