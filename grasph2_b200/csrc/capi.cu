@@ -18,6 +18,9 @@
 using namespace gsph;
 
 constexpr int kSnapSlots = 4;
+// floats per particle of the transfer staging buffer: the components of all 11 attributes
+// (pos 3, mass 1, vel 3, acc 3, balsara 1, xvel 3, density 1, density_dt 1, dstress 9, dstress_dt 9, maxvsig 1)
+constexpr int kStagingFloats = 35;
 
 struct gsph_ctx {
     gsph_params params;
@@ -36,7 +39,7 @@ struct gsph_ctx {
     int device = 0;
     int sm_count = 148;
     std::vector<void*> allocations;
-    float* staging = nullptr;     // 9 * n floats
+    float* staging = nullptr;     // kStagingFloats * n floats: every attribute its own region
     double* staging64 = nullptr;  // 9 * n doubles
     double* diag_out = nullptr;   // device, 12 doubles
     size_t part_cap = 0, gpart_cap = 0, item_cap = 0;  // floats allocated for a.part, a.gpart, sp.item_part
@@ -559,7 +562,7 @@ int gsph_create(const gsph_params* p, const gsph_options* opt, int64_t n, gsph_c
         c->dp64 = make_dev_params64(*p, spline_prefactor(p->dimension, p->H), dspline_prefactor(p->dimension, p->H),
                                     wn > 0 ? 1.0 / wn : 0.0);
     }
-    c->staging = static_cast<float*>(dalloc(c, 9 * n * sizeof(float), ae));
+    c->staging = static_cast<float*>(dalloc(c, kStagingFloats * n * sizeof(float), ae));
     c->staging64 = static_cast<double*>(dalloc(c, 9 * n * sizeof(double), ae));
     c->diag_out = static_cast<double*>(dalloc(c, 16 * sizeof(double), ae));
     if (ae != cudaSuccess) {
@@ -623,11 +626,20 @@ int upload_any(gsph_ctx* c, uint32_t mask, const gsph_host_particles* src, void*
     for (int k = 0; k < 11; ++k)
         if ((mask >> k & 1u) && !ptrs[k]) return fail(c, GSPH_E_INVALID, "attribute pointer is NULL for a set mask bit");
     cudaStream_t s = as_stream(stream);
+    // every attribute into its own staging region, all copies first: they run back to back on the copy
+    // engine instead of each waiting for the previous attribute's pack kernel
+    int64_t off[11];
+    int64_t o = 0;
+    for (int k = 0; k < 11; ++k) {
+        off[k] = o;
+        if (!(mask >> k & 1u)) continue;
+        GSPH_CK(c, cudaMemcpyAsync(c->staging + o, ptrs[k], comps[k] * c->a.n * sizeof(float), kind, s), "upload copy");
+        o += comps[k] * c->a.n;
+    }
     for (int k = 0; k < 11; ++k) {
         if (!(mask >> k & 1u)) continue;
-        GSPH_CK(c, cudaMemcpyAsync(c->staging, ptrs[k], comps[k] * c->a.n * sizeof(float), kind, s), "upload copy");
-        if (c->fp64) GSPH_CK(c, launch64_pack(c->a64, k, c->staging, s), "upload pack");
-        else GSPH_CK(c, launch_pack(c->a, k, c->staging, ext_map(c), s), "upload pack");
+        if (c->fp64) GSPH_CK(c, launch64_pack(c->a64, k, c->staging + off[k], s), "upload pack");
+        else GSPH_CK(c, launch_pack(c->a, k, c->staging + off[k], ext_map(c), s), "upload pack");
         c->launches += 1;
     }
     if (mask & GSPH_POS) {
@@ -655,12 +667,21 @@ int gsph_download(gsph_ctx* c, uint32_t mask, gsph_host_particles* dst, void* st
     for (int k = 0; k < 11; ++k)
         if ((mask >> k & 1u) && !ptrs[k]) return fail(c, GSPH_E_INVALID, "attribute pointer is NULL for a set mask bit");
     cudaStream_t s = as_stream(stream);
+    // all unpack kernels into their own staging regions first, then the copies back to back
+    int64_t off[11];
+    int64_t o = 0;
+    for (int k = 0; k < 11; ++k) {
+        off[k] = o;
+        if (!(mask >> k & 1u)) continue;
+        if (c->fp64) GSPH_CK(c, launch64_unpack(c->a64, k, c->staging + o, s), "download unpack");
+        else GSPH_CK(c, launch_unpack(c->a, k, c->staging + o, ext_map(c), s), "download unpack");
+        c->launches += 1;
+        o += comps[k] * c->a.n;
+    }
     for (int k = 0; k < 11; ++k) {
         if (!(mask >> k & 1u)) continue;
-        if (c->fp64) GSPH_CK(c, launch64_unpack(c->a64, k, c->staging, s), "download unpack");
-        else GSPH_CK(c, launch_unpack(c->a, k, c->staging, ext_map(c), s), "download unpack");
-        c->launches += 1;
-        GSPH_CK(c, cudaMemcpyAsync(ptrs[k], c->staging, comps[k] * c->a.n * sizeof(float), cudaMemcpyDeviceToHost, s),
+        GSPH_CK(c, cudaMemcpyAsync(ptrs[k], c->staging + off[k], comps[k] * c->a.n * sizeof(float),
+                                   cudaMemcpyDeviceToHost, s),
                 "download copy");
     }
     return check_status(c, s);
